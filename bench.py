@@ -1,0 +1,381 @@
+#!/usr/bin/env python
+"""SRM throughput benchmark (point*harmonics per second) on B200.
+
+Workload (default): structured 512 x 512 x 512 grid at 25 m, von Karman ACF
+(Hurst 0.5, correlation lengths 3000/3000/1000 m, sigma 0.05), 20 000
+harmonics, seed 1234 -- the precision configuration the tensor-core form is
+specified on. Synthetic by construction (the SRM draws its own harmonics).
+
+One step = one pass of the SRM sum over the whole grid: FP64 per-axis phase
+tables from the harmonic table, then the factorised tcgen05 split-FP16 sum
+(scaled field written to HBM). `value` times K such steps with the harmonic
+table already on the device; `e2e` times K calls of the public C ABI
+(scarf_execute) with a pinned host output buffer: host sampler, H2D of the
+harmonic table, device sum, statistics, D2H of the field.
+
+--impl reference times the CPU restatement of the reference's SRM (the
+reference itself cannot be built here: no Fortran compiler, MPI or TRNG4)
+on all host threads over a bounded slab of the same workload.
+
+Multi-GPU (torchrun, N ranks): each rank computes its own 512^3 z-slab of a
+512 x 512 x 512N global grid with the same seed (weak scaling, no data-path
+collective); the only exchange is the Chan merge of (n, mean, var) in e2e.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "SRM point·harmonics/s, TC split-precision vs FP32 direct sum, ≤1e-5 rel-RMS"
+UNIT = "pt*harm/s"
+WORKLOAD = dict(nx=512, ny=512, nz=512, ds=25.0, acf=0, hurst=0.5, cl=[3000.0, 3000.0, 1000.0], sigma=0.05,
+                nharm=20000, seed=1234)
+FLOP_PER_PTHARM = 12  # 2 real MACs per harmonic and point (complex as real K=2) x 3 split products
+DIRECT_HARM = 2000    # harmonics timed for the direct-sum comparison (throughput is linear in harmonics)
+
+
+def workload_name(w) -> str:
+    return (f"srm_structured_{w['nx']}x{w['ny']}x{w['nz']}_ds{w['ds']:g}m_vk_h{w['hurst']:g}"
+            f"_cl{'/'.join(f'{c:g}' for c in w['cl'])}_nharm{w['nharm']}")
+
+
+def load_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return d.get("bf16_tflops_sustained", d.get("bf16_tflops")), "measured"
+    return 1400.0, "fallback"
+
+
+def profile_traffic():
+    """DRAM bytes per launch of the tensor-core kernel from the committed ncu
+    summary (None until a capture exists)."""
+    p = ROOT / "profiles" / "srm_tc_kernel_traffic.txt"
+    if not p.exists():
+        return None
+    for line in p.read_text().splitlines():
+        if line.startswith("dram_bytes_per_full_launch:"):
+            return float(line.split(":", 1)[1])
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                          "-lms", "200", "-i", str(self.gpu)], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        self.lines = []
+        if self.proc is not None:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except Exception:
+                self.proc.kill()
+                out = ""
+            self.lines = [l for l in out.splitlines() if l.strip()]
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in getattr(self, "lines", []):
+            f = [x.strip() for x in l.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+def run_reference(args, w):
+    """CPU restatement of the reference SRM on all host threads (bounded slab)."""
+    import oracle
+    nth = os.cpu_count() or 1
+    kw = dict(acf=w["acf"], nharm=w["nharm"], seed=w["seed"], hurst=w["hurst"], sigma=w["sigma"], ds=w["ds"],
+              cl=w["cl"])
+    fe = [w["nx"], w["ny"], w["nz"]]
+    op = oracle.structured_params(fs=[1, 1, 1], fe=fe, **kw)
+    so = oracle.setup(op)
+    tab, _ = oracle.sample(op, so)
+    nh = len(tab)
+    # Calibrate on one x-row, then size a slab of rows for ~3 s per step.
+    t0 = time.perf_counter()
+    oracle.sum_structured_mt(so, [1, 1, 1], [w["nx"], 1, 1], w["ds"], tab, nth)
+    rate = w["nx"] * nh / max(time.perf_counter() - t0, 1e-6)
+    rows = int(max(1, min(w["ny"] * w["nz"], 3.0 * rate / (w["nx"] * nh))))
+    n = [w["nx"], min(rows, w["ny"]), max(1, rows // w["ny"]) if rows > w["ny"] else 1]
+    work = n[0] * n[1] * n[2] * nh
+    for _ in range(args.warmup):
+        oracle.sum_structured_mt(so, [1, 1, 1], n, w["ds"], tab, nth)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        oracle.sum_structured_mt(so, [1, 1, 1], n, w["ds"], tab, nth)
+    dt = time.perf_counter() - t0
+    value = work * args.steps / dt
+    sample = f"{n[0]}x{n[1]}x{n[2]} points of the workload x {nh} harmonics per step (FP32 restatement, {nth} threads)"
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (SRM draws its harmonics)",
+            "impl": "reference",
+            "config": {"workload": workload_name(w), "grid": fe, "nharm": w["nharm"], "form": "cpu_fp32_restatement",
+                       "l2": "n/a (host)"},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": nth, "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "note": "reference not buildable here (no gfortran/MPI/TRNG4); its SRM restated in C, op-order FP32"}
+    print(json.dumps(line), flush=True)
+
+
+def cpu_baseline_sample(w):
+    """Rank-0 CPU baseline: FP32 restatement on all host threads, one bounded
+    slab of the workload (~10-20 s of CPU work)."""
+    import oracle
+    nth = os.cpu_count() or 1
+    kw = dict(acf=w["acf"], nharm=w["nharm"], seed=w["seed"], hurst=w["hurst"], sigma=w["sigma"], ds=w["ds"],
+              cl=w["cl"])
+    op = oracle.structured_params(fs=[1, 1, 1], fe=[w["nx"], w["ny"], w["nz"]], **kw)
+    so = oracle.setup(op)
+    tab, _ = oracle.sample(op, so)
+    nh = len(tab)
+    t0 = time.perf_counter()
+    oracle.sum_structured_mt(so, [1, 1, 1], [w["nx"], 1, 1], w["ds"], tab, nth)
+    rate = w["nx"] * nh / max(time.perf_counter() - t0, 1e-6)
+    rows = int(max(1, min(w["ny"], 12.0 * rate / (w["nx"] * nh))))
+    t0 = time.perf_counter()
+    oracle.sum_structured_mt(so, [1, 1, 1], [w["nx"], rows, 1], w["ds"], tab, nth)
+    dt = time.perf_counter() - t0
+    return {"value": w["nx"] * rows * nh / dt, "unit": UNIT, "cores": nth, "kind": "port",
+            "sample": f"{w['nx']}x{rows}x1 points x {nh} harmonics (FP32 restatement of the reference SRM, "
+                      f"{nth} threads, {dt:.1f} s)"}
+
+
+# ---------------------------------------------------------------------------
+def run_b200(args, w):
+    import torch
+    import torch.distributed as dist
+
+    import scarf3d_b200 as sb
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(v: float) -> float:
+        if world == 1:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    nx, ny, nz = w["nx"], w["ny"], w["nz"]
+    ds = w["ds"]
+    fs = [1, 1, 1 + rank * nz]
+    fe = [nx, ny, nz * (rank + 1)]
+    n = [nx, ny, nz]
+    npts = nx * ny * nz
+    # Global extent of the N-slab grid: every rank draws the same harmonics.
+    nc = [0.0, 0.0, 0.0]
+    fc = [float(np.float32(nx - 1) * np.float32(ds)), float(np.float32(ny - 1) * np.float32(ds)),
+          float(np.float32(nz * world - 1) * np.float32(ds))]
+    kw = dict(acf=w["acf"], nharm=w["nharm"], seed=w["seed"], hurst=w["hurst"], sigma=w["sigma"], ds=ds, cl=w["cl"])
+    p = sb.make_params(nc=nc, fc=fc, **kw)
+    s = sb.compute_setup(p)
+    tab, _ = sb.sample(p, s)
+    nh = len(tab)
+    i3 = lambda v: (ctypes.c_int * 3)(*[int(x) for x in v])  # noqa: E731
+
+    d_tab = torch.from_numpy(tab.reshape(-1).copy()).cuda()
+    field = torch.empty(npts, dtype=torch.float32, device="cuda")
+    wbytes = sb.tc_workspace_bytes(3, n, nh)
+    work = torch.empty(wbytes, dtype=torch.uint8, device="cuda")
+    stream = torch.cuda.current_stream()
+    sptr = ctypes.c_void_p(stream.cuda_stream)
+    sb.check(sb.lib.scarf_set_kernel_timing(1))
+
+    def tc_step():
+        sb.check(sb.lib.scarf_srm_tc_structured(ctypes.byref(s), i3(fs), i3(n), ds, ctypes.c_void_p(d_tab.data_ptr()),
+                                                nh, ctypes.c_void_p(field.data_ptr()),
+                                                ctypes.c_void_p(work.data_ptr()), wbytes, sptr))
+        return float(sb.lib.scarf_last_kernel_ms())
+
+    for _ in range(args.warmup):
+        tc_step()
+    torch.cuda.synchronize()
+    kernel_ms = []
+    with ClockSampler(local) as clk:
+        barrier()
+        torch.cuda.synchronize()
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        for _ in range(args.steps):
+            kernel_ms.append(tc_step())
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+    t_local = ev0.elapsed_time(ev1) / 1e3
+    t = max_over_ranks(t_local)
+    work_total = float(npts) * nh * world * args.steps
+    value = work_total / t
+    k_avg_s = float(np.mean(kernel_ms)) / 1e3
+    k_avg_s = max_over_ranks(k_avg_s)
+
+    # Accuracy of the tensor-core field: FP64 oracle and FP32 restatement at
+    # sampled points (rank 0), normalised by the field's standard deviation.
+    acc = None
+    if rank == 0:
+        import oracle
+        op = oracle.params(nc=nc, fc=fc, **kw)
+        so = oracle.setup(op)
+        rng = np.random.default_rng(0)
+        idx = np.sort(rng.choice(npts, size=384, replace=False)).astype(np.int64)
+        f_all = field.double()
+        fstd = float(f_all.std().item())
+        got = field[torch.from_numpy(idx).cuda()].cpu().numpy().astype(np.float64)
+        r64 = oracle.sum_structured(so, fs, n, ds, tab, idx=idx, f64=True)
+        r32 = oracle.sum_structured(so, fs, n, ds, tab, idx=idx)
+        acc = {"points": int(len(idx)), "rel_rms_vs_fp64": float(np.sqrt(np.mean((got - r64) ** 2)) / fstd),
+               "max_abs_vs_fp64": float(np.max(np.abs(got - r64))),
+               "rel_rms_fp32_restatement_vs_fp64": float(np.sqrt(np.mean((r32 - r64) ** 2)) / fstd),
+               "field_std": fstd}
+
+    # FP32 direct sum on the same grid over the first DIRECT_HARM harmonics.
+    dh = min(DIRECT_HARM, nh)
+    d_ms = []
+    for it in range(3):
+        sb.check(sb.lib.scarf_srm_direct_structured(ctypes.byref(s), i3(fs), i3(n), ds,
+                                                    ctypes.c_void_p(d_tab.data_ptr()), dh,
+                                                    ctypes.c_void_p(field.data_ptr()), sptr))
+        if it:
+            d_ms.append(float(sb.lib.scarf_last_kernel_ms()))
+    direct_rate = npts * dh / (np.mean(d_ms) / 1e3)
+
+    # End to end through the public C ABI (scarf_execute), pinned host field.
+    del work
+    host = torch.empty(npts, dtype=torch.float32, pin_memory=True)
+    opt_fc = np.asarray(fc, np.float32)
+    opt_nc = np.asarray(nc, np.float32)
+    sb.set_nharm(w["nharm"])
+    sb.set_form(sb.FORM_AUTO)
+    sb.set_stream(stream.cuda_stream)
+    sb.scarf_initialize(fs=fs, fe=fe, ds=ds, acf=w["acf"], cl=w["cl"], sigma=w["sigma"], method=1,
+                        hurst=w["hurst"], nc=opt_nc, fc=opt_fc)
+    stats = np.zeros(8, np.float32)
+    fptr = ctypes.c_void_p(host.data_ptr())
+    sptr_stats = stats.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+    for _ in range(max(1, args.warmup)):
+        sb.check(sb.lib.scarf_execute_ex(w["seed"], fptr, sptr_stats, 0))
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        sb.check(sb.lib.scarf_execute_ex(w["seed"], fptr, sptr_stats, 0))
+    t_e2e = max_over_ranks(time.perf_counter() - t0)
+    if world > 1:
+        # Chan merge of (n, mean, var) across ranks (scarflib_common.f90:823-875).
+        from scarf3d_b200.distributed import merge_stats_across_ranks
+        merge_stats_across_ranks(float(stats[2]) ** 2, float(stats[3]), npts)
+    e2e_value = work_total / t_e2e
+    sb.scarf_finalize()
+
+    peak, peak_kind = load_peaks()
+    flops_launch = float(npts) * nh * FLOP_PER_PTHARM
+    achieved = flops_launch / k_avg_s / 1e12
+    traffic = profile_traffic()
+    if rank == 0:
+        cpu = cpu_baseline_sample(w) if world == 1 else None
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t / args.steps * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f16x3-split (fp32 accumulate); fp64 phase tables",
+            "data": "synthetic (harmonics drawn by the SRM sampler, seed 1234)",
+            "config": {"workload": workload_name(w), "grid_per_gpu": n, "global_grid": [nx, ny, nz * world],
+                       "nharm": w["nharm"], "harmonics_kept": nh, "form": "tcgen05 FP16 hi/lo 3-product",
+                       "l2": "inputs and output larger than L2 (tables 246 MB, field 537 MB per GPU)",
+                       "parallelism": f"z-slabs x{world}"},
+            "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                         "frac": achieved / peak, "traffic": traffic,
+                         "peak_kind": f"{peak_kind} bf16 dense, sustained (kernel timed inside a long loop)",
+                         "kernel": "srm_tc_kernel", "kernel_ms": k_avg_s * 1e3,
+                         "flop_per_launch": flops_launch},
+            "direct_sum": {"value": direct_rate, "unit": UNIT, "harmonics_timed": dh,
+                           "kernel_ms": float(np.mean(d_ms)), "tc_over_direct": value / direct_rate},
+            "accuracy": acc,
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(nh * 20),
+                    "d2h_bytes_per_step": int(npts * 4 + 8), "ms_per_step": t_e2e / args.steps * 1e3},
+            "gpu_launches": 3 * args.steps,
+            "clocks": clk.summary(),
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--grid", type=int, nargs=3, default=None, help="override the grid (profiling of small cases)")
+    ap.add_argument("--nharm", type=int, default=None)
+    args = ap.parse_args()
+    w = dict(WORKLOAD)
+    if args.grid:
+        w["nx"], w["ny"], w["nz"] = args.grid
+    if args.nharm:
+        w["nharm"] = args.nharm
+    if args.impl == "reference":
+        if int(os.environ.get("RANK", "0")) != 0:
+            return
+        run_reference(args, w)
+    else:
+        run_b200(args, w)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,124 @@
+/*
+ * scarf3d_b200.h -- extended C ABI of the B200 SRM library.
+ *
+ * The reference-compatible entry points (scarf_opt_init, scarf_cart_initialize,
+ * scarf_nocart_initialize, scarf_execute, scarf_finalize, scarf_io_one,
+ * scarf_io_slice) are declared in scarf3d.h. This header adds status-returning
+ * variants, configuration the reference fixes at compile time, and the
+ * building blocks of the SRM path (setup, sampler, device sums, statistics)
+ * with plain pointers and sizes. Device pointers are CUDA device addresses of
+ * the current device; `stream` is a cudaStream_t passed as void* (NULL = the
+ * legacy default stream).
+ *
+ * Every int-returning function returns SCARF_OK (0) or a negative status and
+ * records a message readable with scarf_last_error() (per thread).
+ */
+#ifndef SCARF3D_B200_H_
+#define SCARF3D_B200_H_
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SCARF_OK 0
+#define SCARF_ERR_ARG (-1)         /* invalid argument                          */
+#define SCARF_ERR_STATE (-2)       /* call order (execute before initialize ...) */
+#define SCARF_ERR_CUDA (-3)        /* CUDA runtime error                        */
+#define SCARF_ERR_UNSUPPORTED (-4) /* e.g. method = FIM, acf = user-defined      */
+#define SCARF_ERR_DEVICE (-5)      /* a kernel reported a stalled pipeline       */
+#define SCARF_ERR_NOMEM (-6)       /* host or device allocation failed           */
+
+/* Summation form used by scarf_execute / scarf_execute_ex. */
+#define SCARF_FORM_AUTO 0   /* tensor-core form for structured grids, else direct */
+#define SCARF_FORM_DIRECT 1 /* FP32 direct sum (any point set)                    */
+#define SCARF_FORM_TC 2     /* factorised tcgen05 split-FP16 form (structured)     */
+
+/* Flags for scarf_execute_ex. */
+#define SCARF_FIELD_ON_DEVICE 1    /* `field` is a device pointer (no D2H copy)      */
+#define SCARF_TAPER_UNSTRUCTURED 2 /* apply POI taper on unstructured meshes too    */
+
+/* SRM inputs (scarflib.f90:67-87, SRM fields only). cl[2] <= 0 selects 2D. */
+typedef struct scarf_srm_params {
+  int acf;     /* 0 = von Karman, 1 = Gaussian                        */
+  int nharm;   /* number of harmonics (reference constant: 10000)     */
+  int seed;
+  int rescale; /* 1 = rescale discrete std to sigma                   */
+  float hurst, sigma, ds, dh;
+  float cl[3], nc[3], fc[3];
+  float alpha, beta, gamma; /* rotation angles, degrees           */
+} scarf_srm_params;
+
+/* Derived scalars (scarflib_srm.f90:617-720). m is row-major
+ * (m[3*r+c] = matrix(r+1,c+1)). scaling includes the quadrature ratio. */
+typedef struct scarf_srm_setup {
+  int ndim;
+  float kmin, kmax, kc, nu, cnst, scaling, scaling0;
+  float m[9];
+  float bar[3];
+  float info0, info1;
+  float intg_band, intg_full;
+  int ier_band, ier_full;
+} scarf_srm_setup;
+
+const char *scarf_last_error(void);
+
+/* ---- configuration of the reference-compatible API ---------------------- */
+/* Harmonic count (replaces the constant nharm = 10000, scarflib_srm.f90:90). */
+int scarf_set_nharm(int nharm);
+int scarf_get_nharm(void);
+/* SCARF_FORM_*. */
+int scarf_set_form(int form);
+/* Install the reference's own uniform source (prng.cpp set_seed / srng,
+ * TRNG4 yarn2 + uniform01_dist<float>) so that harmonics are drawn exactly as
+ * the reference draws them. NULL, NULL restores the built-in generator. */
+int scarf_set_uniform_source(void (*set_seed)(int), void (*srng)(float *));
+/* Stream for all device work of the reference-compatible API. */
+int scarf_set_stream(void *stream);
+/* Host threads for the sampler (0 = automatic). */
+int scarf_set_host_threads(int nthreads);
+/* When enabled, the dominant summation kernel of each call is bracketed by
+ * CUDA events on its launch stream; scarf_last_kernel_ms() returns the last
+ * such duration in milliseconds. */
+int scarf_set_kernel_timing(int enable);
+float scarf_last_kernel_ms(void);
+
+/* Status-returning scarf_execute (c_binding.c:138-143); stats[8] as the
+ * reference fills it (stats[4] host seconds, stats[5] device seconds). */
+int scarf_execute_ex(int seed, float *field, float stats[8], int flags);
+
+/* ---- building blocks ----------------------------------------------------- */
+int scarf_srm_compute_setup(const scarf_srm_params *p, scarf_srm_setup *s);
+/* table: nharm rows {v1,v2,v3,a,b} (FP32); *n_kept = rows written. */
+int scarf_srm_sample(const scarf_srm_params *p, const scarf_srm_setup *s, float *table, int *n_kept,
+                     long long *pairs_used);
+
+/* FP32 direct sum, structured block: field[i + n0*(j + n1*k)] for the grid
+ * x = (i + fs[0] - 1) * ds (0-based i), likewise y, z; scaled by s->scaling.
+ * d_table: nh rows of 5 floats on the device. */
+int scarf_srm_direct_structured(const scarf_srm_setup *s, const int fs[3], const int n[3], float ds,
+                                const float *d_table, int nh, float *d_field, void *stream);
+/* FP32 direct sum over npts points (x, y, z device arrays). */
+int scarf_srm_direct_points(const scarf_srm_setup *s, const float *d_x, const float *d_y, const float *d_z,
+                            long long npts, const float *d_table, int nh, float *d_field, void *stream);
+
+/* Factorised tensor-core form (structured only). d_work must hold
+ * scarf_srm_tc_workspace_bytes(...) bytes of device memory (256-B aligned). */
+size_t scarf_srm_tc_workspace_bytes(int ndim, const int n[3], int nh);
+int scarf_srm_tc_structured(const scarf_srm_setup *s, const int fs[3], const int n[3], float ds,
+                            const float *d_table, int nh, float *d_field, void *d_work, size_t work_bytes,
+                            void *stream);
+
+/* Field statistics as the reference computes them (FP64 sums, FP32 results):
+ * mean and unbiased variance (scarflib_common.f90:694-817). d_work must hold
+ * scarf_field_stats_workspace_bytes(n) bytes. Synchronises the stream. */
+size_t scarf_field_stats_workspace_bytes(long long n);
+int scarf_field_stats(const float *d_field, long long n, void *d_work, size_t work_bytes, float *mean,
+                      float *var, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SCARF3D_B200_H_ */

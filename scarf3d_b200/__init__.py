@@ -1,0 +1,307 @@
+"""Python host interface of the B200 SRM library (libscarf3d_b200.so).
+
+Mirrors SCARF3D's initialize / execute / finalize interface (scarflib.f90:48-62,
+c_binding.c:62-150) with the same argument names and meaning, over the library's
+C ABI (include/scarf3d.h, include/scarf3d_b200.h). There is no CPU fallback: if
+the shared library is missing or fails to load, importing this package raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from pathlib import Path
+
+import numpy as np
+
+_HERE = Path(__file__).resolve().parent
+LIB_PATH = Path(os.environ.get("SCARF3D_B200_LIB", _HERE / "libscarf3d_b200.so"))
+
+SCARF_OK = 0
+SCARF_ERR_ARG = -1
+SCARF_ERR_STATE = -2
+SCARF_ERR_CUDA = -3
+SCARF_ERR_UNSUPPORTED = -4
+SCARF_ERR_DEVICE = -5
+SCARF_ERR_NOMEM = -6
+
+FORM_AUTO, FORM_DIRECT, FORM_TC = 0, 1, 2
+FIELD_ON_DEVICE, TAPER_UNSTRUCTURED = 1, 2
+
+EXPORTED_SYMBOLS = (
+    # reference-compatible (include/scarf3d.h)
+    "scarf_opt_init", "scarf_cart_initialize", "scarf_nocart_initialize", "scarf_execute",
+    "scarf_finalize", "scarf_io_one", "scarf_io_slice",
+    # extended (include/scarf3d_b200.h)
+    "scarf_last_error", "scarf_set_nharm", "scarf_get_nharm", "scarf_set_form",
+    "scarf_set_uniform_source", "scarf_set_stream", "scarf_set_host_threads", "scarf_set_kernel_timing",
+    "scarf_last_kernel_ms", "scarf_execute_ex",
+    "scarf_srm_compute_setup", "scarf_srm_sample", "scarf_srm_direct_structured",
+    "scarf_srm_direct_points", "scarf_srm_tc_workspace_bytes", "scarf_srm_tc_structured",
+    "scarf_field_stats_workspace_bytes", "scarf_field_stats",
+)
+
+
+class ScarfError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"scarf3d_b200 error {code}: {msg}")
+        self.code = code
+
+
+class ScarfOpt(ctypes.Structure):
+    """struct scarf_opt (src/scarf3d.h:54-70), byte-for-byte."""
+    _fields_ = [("method", ctypes.c_int), ("hurst", ctypes.c_float), ("dh", ctypes.c_float),
+                ("ds", ctypes.c_float), ("poi", ctypes.POINTER(ctypes.c_float)), ("npoi", ctypes.c_int),
+                ("mute", ctypes.c_float), ("taper", ctypes.c_float), ("rescale", ctypes.c_int),
+                ("pad", ctypes.c_int), ("nc", ctypes.POINTER(ctypes.c_float)),
+                ("fc", ctypes.POINTER(ctypes.c_float)), ("alpha", ctypes.c_float),
+                ("beta", ctypes.c_float), ("gamma", ctypes.c_float)]
+
+
+class SrmParams(ctypes.Structure):
+    _fields_ = [("acf", ctypes.c_int), ("nharm", ctypes.c_int), ("seed", ctypes.c_int),
+                ("rescale", ctypes.c_int), ("hurst", ctypes.c_float), ("sigma", ctypes.c_float),
+                ("ds", ctypes.c_float), ("dh", ctypes.c_float), ("cl", ctypes.c_float * 3),
+                ("nc", ctypes.c_float * 3), ("fc", ctypes.c_float * 3), ("alpha", ctypes.c_float),
+                ("beta", ctypes.c_float), ("gamma", ctypes.c_float)]
+
+
+class SrmSetup(ctypes.Structure):
+    _fields_ = [("ndim", ctypes.c_int), ("kmin", ctypes.c_float), ("kmax", ctypes.c_float),
+                ("kc", ctypes.c_float), ("nu", ctypes.c_float), ("cnst", ctypes.c_float),
+                ("scaling", ctypes.c_float), ("scaling0", ctypes.c_float), ("m", ctypes.c_float * 9),
+                ("bar", ctypes.c_float * 3), ("info0", ctypes.c_float), ("info1", ctypes.c_float),
+                ("intg_band", ctypes.c_float), ("intg_full", ctypes.c_float), ("ier_band", ctypes.c_int),
+                ("ier_full", ctypes.c_int)]
+
+
+def _load() -> ctypes.CDLL:
+    if not LIB_PATH.exists():
+        raise ImportError(f"scarf3d_b200: {LIB_PATH} is missing; build it with "
+                          f"`python -m scarf3d_b200.build` (no CPU fallback exists)")
+    lib = ctypes.CDLL(str(LIB_PATH))
+    c_int, c_float, c_void_p, c_size_t, c_ll = (ctypes.c_int, ctypes.c_float, ctypes.c_void_p,
+                                                ctypes.c_size_t, ctypes.c_longlong)
+    fp = ctypes.POINTER(c_float)
+    ip = ctypes.POINTER(c_int)
+    sig = {
+        "scarf_opt_init": (None, [ctypes.POINTER(ScarfOpt)]),
+        "scarf_cart_initialize": (None, [c_int, ip, ip, c_float, c_int, fp, c_float, ctypes.POINTER(ScarfOpt)]),
+        "scarf_nocart_initialize": (None, [c_int, c_int, fp, fp, fp, c_float, c_int, fp, c_float,
+                                           ctypes.POINTER(ScarfOpt)]),
+        "scarf_execute": (None, [c_int, c_void_p, fp]),
+        "scarf_finalize": (None, []),
+        "scarf_io_one": (None, [c_int, ip, c_void_p, ctypes.c_char_p, ip]),
+        "scarf_io_slice": (None, [ip, ctypes.c_char_p, c_int, c_void_p, ctypes.c_char_p]),
+        "scarf_last_error": (ctypes.c_char_p, []),
+        "scarf_set_nharm": (c_int, [c_int]),
+        "scarf_get_nharm": (c_int, []),
+        "scarf_set_form": (c_int, [c_int]),
+        "scarf_set_uniform_source": (c_int, [c_void_p, c_void_p]),
+        "scarf_set_stream": (c_int, [c_void_p]),
+        "scarf_set_host_threads": (c_int, [c_int]),
+        "scarf_set_kernel_timing": (c_int, [c_int]),
+        "scarf_last_kernel_ms": (c_float, []),
+        "scarf_execute_ex": (c_int, [c_int, c_void_p, fp, c_int]),
+        "scarf_srm_compute_setup": (c_int, [ctypes.POINTER(SrmParams), ctypes.POINTER(SrmSetup)]),
+        "scarf_srm_sample": (c_int, [ctypes.POINTER(SrmParams), ctypes.POINTER(SrmSetup), c_void_p, ip,
+                                     ctypes.POINTER(c_ll)]),
+        "scarf_srm_direct_structured": (c_int, [ctypes.POINTER(SrmSetup), ip, ip, c_float, c_void_p, c_int,
+                                                c_void_p, c_void_p]),
+        "scarf_srm_direct_points": (c_int, [ctypes.POINTER(SrmSetup), c_void_p, c_void_p, c_void_p, c_ll,
+                                            c_void_p, c_int, c_void_p, c_void_p]),
+        "scarf_srm_tc_workspace_bytes": (c_size_t, [c_int, ip, c_int]),
+        "scarf_srm_tc_structured": (c_int, [ctypes.POINTER(SrmSetup), ip, ip, c_float, c_void_p, c_int,
+                                            c_void_p, c_void_p, c_size_t, c_void_p]),
+        "scarf_field_stats_workspace_bytes": (c_size_t, [c_ll]),
+        "scarf_field_stats": (c_int, [c_void_p, c_ll, c_void_p, c_size_t, fp, fp, c_void_p]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    return lib
+
+
+lib = _load()
+
+
+def last_error() -> str:
+    return (lib.scarf_last_error() or b"").decode()
+
+
+def check(rc: int) -> None:
+    if rc != SCARF_OK:
+        raise ScarfError(rc, last_error())
+
+
+def _f32(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+def _iptr(a):
+    arr = (ctypes.c_int * len(a))(*[int(v) for v in a])
+    return arr
+
+
+def _fptr(a):
+    return (ctypes.c_float * len(a))(*[float(v) for v in a])
+
+
+# --------------------------------------------------------------------------
+# Reference-style interface (scarflib.f90 generic procedures)
+# --------------------------------------------------------------------------
+class _State:
+    keep: list = []
+    n: tuple | None = None
+    structured = True
+
+
+def scarf_initialize(*, fs=None, fe=None, ds=None, x=None, y=None, z=None, dh=None, acf, cl, sigma,
+                     method=1, hurst=0.0, poi=None, mute=0.0, taper=0.0, rescale=0, pad=0, nc=None,
+                     fc=None, alpha=0.0, beta=0.0, gamma=0.0):
+    """initialize_structured (fs, fe, ds given) or initialize_unstructured (x, y[, z], dh given).
+
+    Optional arguments follow the C binding's rule: they count as given when
+    > 0 (hurst, dh/ds, mute, taper, npoi), == 1 (method, rescale, pad) or != 0
+    (angles); nc and fc must be given together.
+    """
+    opt = ScarfOpt()
+    lib.scarf_opt_init(ctypes.byref(opt))
+    opt.method = int(method)
+    opt.hurst = float(hurst)
+    opt.mute = float(mute)
+    opt.taper = float(taper)
+    opt.rescale = int(rescale)
+    opt.pad = int(pad)
+    opt.alpha, opt.beta, opt.gamma = float(alpha), float(beta), float(gamma)
+    keep = []
+    if poi is not None:
+        p = _f32(poi)
+        keep.append(p)
+        opt.poi = p.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+        opt.npoi = p.shape[0] if p.ndim == 2 else 1
+    if nc is not None and fc is not None:
+        a, b = _f32(nc), _f32(fc)
+        keep += [a, b]
+        opt.nc = a.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+        opt.fc = b.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+    clv = _f32(cl)
+    keep.append(clv)
+    nd = len(clv)
+    if fs is not None:
+        if dh is not None:
+            opt.dh = float(dh)
+        lib.scarf_cart_initialize(nd, _iptr(fs), _iptr(fe), float(ds), int(acf),
+                                  clv.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), float(sigma),
+                                  ctypes.byref(opt))
+        _State.structured = True
+        _State.n = tuple(int(e) - int(s) + 1 for s, e in zip(fs, fe))
+    else:
+        if ds is not None:
+            opt.ds = float(ds)
+        xs, ys = _f32(x), _f32(y)
+        zs = _f32(z) if z is not None else None
+        keep += [xs, ys] + ([zs] if zs is not None else [])
+        fpz = zs.ctypes.data_as(ctypes.POINTER(ctypes.c_float)) if zs is not None else None
+        lib.scarf_nocart_initialize(nd, len(xs), xs.ctypes.data_as(ctypes.POINTER(ctypes.c_float)),
+                                    ys.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), fpz, float(dh), int(acf),
+                                    clv.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), float(sigma),
+                                    ctypes.byref(opt))
+        _State.structured = False
+        _State.n = (len(xs),)
+    err = last_error()
+    if err:
+        raise ScarfError(SCARF_ERR_ARG, err)
+    _State.keep = keep  # the library borrows these until scarf_finalize
+
+
+def scarf_execute(seed: int, field=None, *, flags: int = 0):
+    """Run the SRM; returns (field, stats[8]). `field` may be a NumPy array
+    (host) or an object exposing a CUDA device pointer via `data_ptr()`
+    (torch tensor), float32, column-major extent n0 x n1 x n2 / npts."""
+    if _State.n is None:
+        raise ScarfError(SCARF_ERR_STATE, "scarf_execute before scarf_initialize")
+    stats = np.zeros(8, np.float32)
+    if field is None:
+        field = np.zeros(int(np.prod(_State.n)), np.float32)
+    if hasattr(field, "data_ptr"):
+        ptr = field.data_ptr()
+        flags |= FIELD_ON_DEVICE if field.is_cuda else 0
+    else:
+        if field.dtype != np.float32 or not field.flags["C_CONTIGUOUS"] and not field.flags["F_CONTIGUOUS"]:
+            raise ValueError("field must be a contiguous float32 array")
+        ptr = field.ctypes.data
+    check(lib.scarf_execute_ex(int(seed), ctypes.c_void_p(ptr),
+                               stats.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), int(flags)))
+    return field, stats
+
+
+def scarf_finalize():
+    lib.scarf_finalize()
+    _State.keep = []
+    _State.n = None
+
+
+def scarf_io(npts, field, filename: str, nwriters=None):
+    nwr = _iptr([nwriters]) if nwriters else None
+    f = _f32(field) if not hasattr(field, "ctypes") else field
+    lib.scarf_io_one(len(npts), _iptr(npts), ctypes.c_void_p(f.ctypes.data), filename.encode(), nwr)
+
+
+def scarf_io_slice(npts, axis: str, plane: int, field, filename: str):
+    lib.scarf_io_slice(_iptr(npts), axis.encode(), int(plane), ctypes.c_void_p(field.ctypes.data),
+                       filename.encode())
+
+
+# --------------------------------------------------------------------------
+# Building blocks
+# --------------------------------------------------------------------------
+def make_params(*, acf, nharm, seed, hurst=0.0, sigma=1.0, ds, dh=None, cl, nc, fc, rescale=0,
+                alpha=0.0, beta=0.0, gamma=0.0) -> SrmParams:
+    p = SrmParams()
+    p.acf, p.nharm, p.seed, p.rescale = int(acf), int(nharm), int(seed), int(rescale)
+    p.hurst, p.sigma, p.ds = float(hurst), float(sigma), float(ds)
+    p.dh = float(dh if dh is not None else ds)
+    cl3 = list(cl) + [0.0] * (3 - len(cl))
+    for c in range(3):
+        p.cl[c] = cl3[c]
+        p.nc[c] = float(nc[c]) if c < len(nc) else 0.0
+        p.fc[c] = float(fc[c]) if c < len(fc) else 0.0
+    p.alpha, p.beta, p.gamma = float(alpha), float(beta), float(gamma)
+    return p
+
+
+def compute_setup(p: SrmParams) -> SrmSetup:
+    s = SrmSetup()
+    check(lib.scarf_srm_compute_setup(ctypes.byref(p), ctypes.byref(s)))
+    return s
+
+
+def sample(p: SrmParams, s: SrmSetup) -> tuple[np.ndarray, int]:
+    """Harmonic table (n_kept x 5: v1, v2, v3, a, b) and the srng pairs used."""
+    tab = np.zeros((max(p.nharm, 1), 5), np.float32)
+    kept = ctypes.c_int()
+    used = ctypes.c_longlong()
+    check(lib.scarf_srm_sample(ctypes.byref(p), ctypes.byref(s), tab.ctypes.data_as(ctypes.c_void_p),
+                               ctypes.byref(kept), ctypes.byref(used)))
+    return tab[: kept.value].copy(), used.value
+
+
+def set_nharm(n: int):
+    check(lib.scarf_set_nharm(int(n)))
+
+
+def set_form(form: int):
+    check(lib.scarf_set_form(int(form)))
+
+
+def set_host_threads(n: int):
+    check(lib.scarf_set_host_threads(int(n)))
+
+
+def set_stream(stream_handle: int | None):
+    check(lib.scarf_set_stream(ctypes.c_void_p(stream_handle or 0)))
+
+
+def tc_workspace_bytes(ndim: int, n, nh: int) -> int:
+    return int(lib.scarf_srm_tc_workspace_bytes(int(ndim), _iptr(n), int(nh)))

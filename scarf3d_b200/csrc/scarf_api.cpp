@@ -1,0 +1,699 @@
+// C ABI of the B200 SRM library: the reference-compatible scarf_* entry
+// points (module-global state, as scarflib.f90:87 and f_binding.f90:44-47
+// keep it) and the extended, status-returning API of scarf3d_b200.h.
+#include <cuda_runtime.h>
+#include <fcntl.h>
+#include <unistd.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "scarf3d.h"
+#include "scarf3d_b200.h"
+#include "srm_host.h"
+#include "srm_kernels.h"
+
+namespace scarf {
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_last_error = buf;
+  return code;
+}
+
+int cuda_fail(cudaError_t e, const char* what) {
+  return fail(SCARF_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+
+#define SCARF_CUDA(call)                                   \
+  do {                                                     \
+    cudaError_t e_ = (call);                               \
+    if (e_ != cudaSuccess) return cuda_fail(e_, #call);    \
+  } while (0)
+
+// ------------------------------------------------------------------ config --
+struct Config {
+  int nharm = 10000;  // scarflib_srm.f90:90
+  int form = SCARF_FORM_AUTO;
+  UniformSource src;
+  cudaStream_t stream = nullptr;
+  int threads = 0;
+  bool kernel_timing = false;
+};
+Config g_cfg;
+float g_last_kernel_ms = 0.0f;
+
+// ------------------------------------------- reference-style global object --
+struct Object {
+  bool ready = false;
+  bool structured = true;
+  int nd = 3;
+  int method = 0;
+  int acf = 0, rescale = 0, pad = 0;
+  int fs[3] = {1, 1, 1}, fe[3] = {1, 1, 1};
+  float ds = 0, dh = 0, sigma = 0, hurst = 0, mute = -999.0f, taper = -999.0f;
+  float alpha = 0, beta = 0, gamma = 0;
+  float cl[3] = {0, 0, 0}, nc[3] = {0, 0, 0}, fc[3] = {0, 0, 0};
+  int npts = 0;
+  const float *x = nullptr, *y = nullptr, *z = nullptr;  // borrowed (scarflib.f90:233-237)
+  std::vector<float> z2d;                                // 2D meshes: z = 0 (:239-240)
+  const float* poi = nullptr;                            // borrowed, [nd x npoi]
+  int npoi = 0;
+};
+Object g_obj;
+std::mutex g_mu;
+
+// --------------------------------------------------- per-device resources --
+struct DeviceBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  cudaError_t ensure(size_t need) {
+    if (need <= bytes) return cudaSuccess;
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+    cudaError_t e = cudaMalloc(&p, need);
+    if (e == cudaSuccess) bytes = need;
+    return e;
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+  }
+};
+
+struct Resources {
+  int device = -1;
+  DeviceBuf status, stats, table, field, coords, work;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr, evk0 = nullptr, evk1 = nullptr;
+  void release() {
+    if (evk0) cudaEventDestroy(evk0);
+    if (evk1) cudaEventDestroy(evk1);
+    evk0 = evk1 = nullptr;
+    status.release();
+    stats.release();
+    table.release();
+    field.release();
+    coords.release();
+    work.release();
+    if (ev0) cudaEventDestroy(ev0);
+    if (ev1) cudaEventDestroy(ev1);
+    ev0 = ev1 = nullptr;
+    device = -1;
+  }
+};
+Resources g_res;
+
+int ensure_resources() {
+  int dev = 0;
+  SCARF_CUDA(cudaGetDevice(&dev));
+  if (g_res.device != dev) {
+    g_res.release();
+    g_res.device = dev;
+  }
+  SCARF_CUDA(g_res.status.ensure(256));
+  SCARF_CUDA(g_res.stats.ensure(stats_partials_bytes(0) + 256));
+  if (!g_res.ev0) SCARF_CUDA(cudaEventCreate(&g_res.ev0));
+  if (!g_res.ev1) SCARF_CUDA(cudaEventCreate(&g_res.ev1));
+  if (!g_res.evk0) SCARF_CUDA(cudaEventCreate(&g_res.evk0));
+  if (!g_res.evk1) SCARF_CUDA(cudaEventCreate(&g_res.evk1));
+  return SCARF_OK;
+}
+
+// Events bracketing the dominant kernel of the next launch, when enabled.
+cudaEvent_t kernel_ev0() { return g_cfg.kernel_timing ? g_res.evk0 : nullptr; }
+cudaEvent_t kernel_ev1() { return g_cfg.kernel_timing ? g_res.evk1 : nullptr; }
+void collect_kernel_time() {
+  if (!g_cfg.kernel_timing) return;
+  float ms = 0.0f;
+  if (cudaEventElapsedTime(&ms, g_res.evk0, g_res.evk1) == cudaSuccess) g_last_kernel_ms = ms;
+  cudaGetLastError();
+}
+
+bool is_device_pointer(const void* p) {
+  cudaPointerAttributes a{};
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+int check_device_status(const int* d_status, cudaStream_t st) {
+  int h = 0;
+  SCARF_CUDA(cudaMemcpyAsync(&h, d_status, sizeof(int), cudaMemcpyDeviceToHost, st));
+  SCARF_CUDA(cudaStreamSynchronize(st));
+  if (h != 0) return fail(SCARF_ERR_DEVICE, "device pipeline reported status %d (bounded wait expired)", h);
+  return SCARF_OK;
+}
+
+double now_s() {
+  return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+scarf_srm_params params_from_object(int seed) {
+  scarf_srm_params p{};
+  p.acf = g_obj.acf;
+  p.nharm = g_cfg.nharm;
+  p.seed = seed;
+  p.rescale = g_obj.rescale;
+  p.hurst = g_obj.hurst;
+  p.sigma = g_obj.sigma;
+  p.ds = g_obj.ds;
+  p.dh = g_obj.dh;
+  for (int c = 0; c < 3; ++c) {
+    p.cl[c] = g_obj.cl[c];
+    p.nc[c] = g_obj.nc[c];
+    p.fc[c] = g_obj.fc[c];
+  }
+  p.alpha = g_obj.alpha;
+  p.beta = g_obj.beta;
+  p.gamma = g_obj.gamma;
+  return p;
+}
+
+// The whole SRM execute (scarflib_srm.f90:505-929 / :105-499) for the global
+// object. field: host or device memory of the local block / point set.
+int execute_impl(int seed, float* field, float stats[8], int flags) {
+  if (!g_obj.ready) return fail(SCARF_ERR_STATE, "scarf_execute called before scarf_*_initialize");
+  if (g_obj.method != 1) return fail(SCARF_ERR_UNSUPPORTED, "only the SRM method (method = 1) is implemented");
+  if (!field || !stats) return fail(SCARF_ERR_ARG, "field and stats must not be NULL");
+  int rc = ensure_resources();
+  if (rc) return rc;
+  cudaStream_t st = g_cfg.stream;
+  for (int i = 0; i < 8; ++i) stats[i] = 0.0f;
+
+  // Host: setup scalars and harmonic table.
+  const double th0 = now_s();
+  const scarf_srm_params p = params_from_object(seed);
+  scarf_srm_setup s{};
+  rc = srm_setup(p, &s);
+  if (rc) return fail(rc, "invalid SRM parameters (acf %d, nharm %d)", p.acf, p.nharm);
+  std::vector<float> table(5 * static_cast<size_t>(p.nharm));
+  const int threads = g_cfg.threads > 0 ? g_cfg.threads : host_threads();
+  long long pairs = 0;
+  const int nh = srm_sample(p, s, &g_cfg.src, threads, table.data(), &pairs);
+  const double t_host = now_s() - th0;
+
+  // Device work.
+  long long npts;
+  int n[3] = {1, 1, 1};
+  if (g_obj.structured) {
+    for (int c = 0; c < 3; ++c) n[c] = g_obj.fe[c] - g_obj.fs[c] + 1;
+    npts = static_cast<long long>(n[0]) * n[1] * n[2];
+  } else {
+    npts = g_obj.npts;
+  }
+  if (npts <= 0) return fail(SCARF_ERR_ARG, "empty point set");
+  const bool on_device = (flags & SCARF_FIELD_ON_DEVICE) || is_device_pointer(field);
+  SCARF_CUDA(g_res.table.ensure(sizeof(float) * 5 * std::max(nh, 1)));
+  float* d_table = static_cast<float*>(g_res.table.p);
+  int* d_status = static_cast<int*>(g_res.status.p);
+  float* d_field = field;
+  if (!on_device) {
+    SCARF_CUDA(g_res.field.ensure(sizeof(float) * npts));
+    d_field = static_cast<float*>(g_res.field.p);
+  }
+  SCARF_CUDA(cudaEventRecord(g_res.ev0, st));
+  SCARF_CUDA(cudaMemsetAsync(d_status, 0, sizeof(int), st));
+  if (nh > 0)
+    SCARF_CUDA(cudaMemcpyAsync(d_table, table.data(), sizeof(float) * 5 * nh, cudaMemcpyHostToDevice, st));
+
+  const float* dx = nullptr;
+  const float* dy = nullptr;
+  const float* dz = nullptr;
+  if (g_obj.structured) {
+    const bool use_tc = (g_cfg.form != SCARF_FORM_DIRECT);
+    TcPlan plan{};
+    if (use_tc && nh > 0 && tc_make_plan(s.ndim, n, nh, &plan)) {
+      SCARF_CUDA(g_res.work.ensure(plan.bytes));
+      SCARF_CUDA(launch_tc_structured(s, g_obj.fs, n, p.ds, d_table, nh, d_field, g_res.work.p, plan, d_status, st,
+                                      kernel_ev0(), kernel_ev1()));
+    } else if (nh > 0) {
+      if (kernel_ev0()) SCARF_CUDA(cudaEventRecord(kernel_ev0(), st));
+      SCARF_CUDA(launch_direct_structured(s, g_obj.fs, n, p.ds, d_table, nh, d_field, d_status, st));
+      if (kernel_ev1()) SCARF_CUDA(cudaEventRecord(kernel_ev1(), st));
+    } else {
+      SCARF_CUDA(cudaMemsetAsync(d_field, 0, sizeof(float) * npts, st));
+    }
+  } else {
+    SCARF_CUDA(g_res.coords.ensure(sizeof(float) * 3 * npts + 64));
+    float* c = static_cast<float*>(g_res.coords.p);
+    const size_t stride = (static_cast<size_t>(npts) + 3) / 4 * 4;  // keep each array 16-B aligned
+    SCARF_CUDA(g_res.coords.ensure(sizeof(float) * 3 * stride));
+    c = static_cast<float*>(g_res.coords.p);
+    SCARF_CUDA(cudaMemcpyAsync(c, g_obj.x, sizeof(float) * npts, cudaMemcpyDefault, st));
+    SCARF_CUDA(cudaMemcpyAsync(c + stride, g_obj.y, sizeof(float) * npts, cudaMemcpyDefault, st));
+    SCARF_CUDA(cudaMemcpyAsync(c + 2 * stride, g_obj.z, sizeof(float) * npts, cudaMemcpyDefault, st));
+    dx = c;
+    dy = c + stride;
+    dz = c + 2 * stride;
+    if (nh > 0) {
+      if (kernel_ev0()) SCARF_CUDA(cudaEventRecord(kernel_ev0(), st));
+      SCARF_CUDA(launch_direct_points(s, dx, dy, dz, npts, d_table, nh, d_field, d_status, st));
+      if (kernel_ev1()) SCARF_CUDA(cudaEventRecord(kernel_ev1(), st));
+    } else {
+      SCARF_CUDA(cudaMemsetAsync(d_field, 0, sizeof(float) * npts, st));
+    }
+  }
+  rc = check_device_status(d_status, st);
+  if (rc) return rc;
+  if (nh > 0) collect_kernel_time();
+
+  // Statistics (scarflib_srm.f90:877-895): single set, so the Chan merge
+  // returns (var, mean) unchanged; std = sqrt(var) in FP32.
+  double* d_part = static_cast<double*>(g_res.stats.p);
+  float* d_out = reinterpret_cast<float*>(static_cast<char*>(g_res.stats.p) + stats_partials_bytes(0));
+  SCARF_CUDA(launch_field_stats(d_field, npts, d_part, d_out, st));
+  float mv[2];
+  SCARF_CUDA(cudaMemcpyAsync(mv, d_out, sizeof(mv), cudaMemcpyDeviceToHost, st));
+  SCARF_CUDA(cudaStreamSynchronize(st));
+  stats[0] = s.info0;
+  stats[1] = s.info1;
+  stats[2] = sqrtf(mv[1]);
+  stats[3] = mv[0];
+
+  // Rescale (:897-912) and taper (:920-925).
+  if (p.rescale == 1) {
+    SCARF_CUDA(launch_rescale(d_field, npts, p.sigma, stats[2], stats[3], st));
+    stats[2] = p.sigma;
+    stats[3] = 0.0f;
+  }
+  const bool taper_ok = g_obj.structured || (flags & SCARF_TAPER_UNSTRUCTURED);
+  if (taper_ok && g_obj.poi && g_obj.npoi > 0) {
+    for (int q = 0; q < g_obj.npoi; ++q) {
+      float pt[3] = {0.0f, 0.0f, 0.0f};
+      for (int c = 0; c < s.ndim; ++c) pt[c] = g_obj.poi[g_obj.nd * q + c];
+      if (g_obj.structured)
+        SCARF_CUDA(launch_taper_structured(d_field, g_obj.fs, n, p.ds, pt, g_obj.mute, g_obj.taper, st));
+      else
+        SCARF_CUDA(launch_taper_points(d_field, dx, dy, dz, npts, pt, g_obj.mute, g_obj.taper, st));
+    }
+  }
+  SCARF_CUDA(cudaEventRecord(g_res.ev1, st));
+  if (!on_device)
+    SCARF_CUDA(cudaMemcpyAsync(field, d_field, sizeof(float) * npts, cudaMemcpyDeviceToHost, st));
+  SCARF_CUDA(cudaStreamSynchronize(st));
+  float ms = 0.0f;
+  cudaEventElapsedTime(&ms, g_res.ev0, g_res.ev1);
+  stats[4] = static_cast<float>(t_host);
+  stats[5] = ms * 1e-3f;
+  return SCARF_OK;
+}
+
+void finalize_impl() {
+  g_obj = Object();
+  g_res.release();
+}
+
+}  // namespace
+}  // namespace scarf
+
+using namespace scarf;
+
+// ======================================================================== //
+// Reference-compatible entry points                                          //
+// ======================================================================== //
+extern "C" {
+
+void scarf_opt_init(struct scarf_opt* var) {
+  if (!var) return;
+  std::memset(var, 0, sizeof(*var));
+}
+
+void scarf_cart_initialize(const int nd, const int fs[], const int fe[], const real ds, const int acf,
+                           const real cl[], const real sigma, struct scarf_opt* var) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  if ((nd != 2 && nd != 3) || !fs || !fe || !cl) {
+    fail(SCARF_ERR_ARG, "scarf_cart_initialize: nd must be 2 or 3 and fs, fe, cl non-NULL");
+    return;
+  }
+  Object& o = g_obj;
+  o = Object();
+  o.structured = true;
+  o.nd = nd;
+  for (int c = 0; c < nd; ++c) {
+    o.fs[c] = fs[c];
+    o.fe[c] = fe[c];
+    o.cl[c] = cl[c];
+  }
+  o.ds = ds;
+  o.dh = ds;  // scarflib.f90:139
+  o.acf = acf;
+  o.sigma = sigma;
+  for (int c = 0; c < 3; ++c) {  // scarflib.f90:157-158
+    o.nc[c] = static_cast<float>(o.fs[c] - 1) * ds;
+    o.fc[c] = static_cast<float>(o.fe[c] - 1) * ds;
+  }
+  if (var) {  // c_binding.c:89-103: a field is given when > 0 / != 0
+    if (var->method == 1) o.method = 1;
+    if (var->hurst > 0) o.hurst = var->hurst;
+    if (var->dh > 0) o.dh = var->dh;
+    if (var->poi && var->npoi > 0) {
+      o.poi = var->poi;
+      o.npoi = var->npoi;
+    }
+    if (var->mute > 0) o.mute = var->mute;
+    if (var->taper > 0) o.taper = var->taper;
+    if (var->rescale == 1) o.rescale = 1;
+    if (var->pad == 1) o.pad = 1;
+    if (var->nc && var->fc)
+      for (int c = 0; c < nd; ++c) {
+        o.nc[c] = var->nc[c];
+        o.fc[c] = var->fc[c];
+      }
+    if (var->alpha != 0) o.alpha = var->alpha;
+    if (var->beta != 0) o.beta = var->beta;
+    if (var->gamma != 0) o.gamma = var->gamma;
+  }
+  o.ready = true;
+  g_last_error.clear();
+}
+
+void scarf_nocart_initialize(const int nd, const int npts, const real* x, const real* y, const real* z,
+                             const real dh, const int acf, const real cl[], const real sigma,
+                             struct scarf_opt* var) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  if ((nd != 2 && nd != 3) || npts <= 0 || !x || !y || !cl || (nd == 3 && !z)) {
+    fail(SCARF_ERR_ARG, "scarf_nocart_initialize: invalid nd/npts or NULL coordinates");
+    return;
+  }
+  Object& o = g_obj;
+  o = Object();
+  o.structured = false;
+  o.nd = nd;
+  o.npts = npts;
+  o.x = x;
+  o.y = y;
+  if (nd == 3) {
+    o.z = z;
+  } else {
+    o.z2d.assign(static_cast<size_t>(npts), 0.0f);
+    o.z = o.z2d.data();
+  }
+  for (int c = 0; c < nd; ++c) o.cl[c] = cl[c];
+  o.dh = dh;
+  o.ds = dh;  // scarflib.f90:249
+  o.acf = acf;
+  o.sigma = sigma;
+  // nc / fc from the coordinate extrema (scarflib.f90:265-271).
+  const float* ax[3] = {x, y, o.z};
+  for (int c = 0; c < 3; ++c) {
+    if (c >= nd) {
+      o.nc[c] = o.fc[c] = 0.0f;
+      continue;
+    }
+    float lo = ax[c][0], hi = ax[c][0];
+    for (int i = 1; i < npts; ++i) {
+      lo = std::min(lo, ax[c][i]);
+      hi = std::max(hi, ax[c][i]);
+    }
+    o.nc[c] = lo;
+    o.fc[c] = hi;
+  }
+  if (var) {
+    if (var->method == 1) o.method = 1;
+    if (var->hurst > 0) o.hurst = var->hurst;
+    if (var->ds > 0) o.ds = var->ds;
+    if (var->poi && var->npoi > 0) {
+      o.poi = var->poi;
+      o.npoi = var->npoi;
+    }
+    if (var->mute > 0) o.mute = var->mute;
+    if (var->taper > 0) o.taper = var->taper;
+    if (var->rescale == 1) o.rescale = 1;
+    if (var->pad == 1) o.pad = 1;
+    if (var->nc && var->fc)
+      for (int c = 0; c < nd; ++c) {
+        o.nc[c] = var->nc[c];
+        o.fc[c] = var->fc[c];
+      }
+    if (var->alpha != 0) o.alpha = var->alpha;
+    if (var->beta != 0) o.beta = var->beta;
+    if (var->gamma != 0) o.gamma = var->gamma;
+  }
+  o.ready = true;
+  g_last_error.clear();
+}
+
+void scarf_execute(const int seed, real* field, real stats[]) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  const int rc = execute_impl(seed, field, stats, 0);
+  if (rc) std::fprintf(stderr, "scarf_execute: %s\n", g_last_error.c_str());
+}
+
+void scarf_finalize(void) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  finalize_impl();
+}
+
+// Raw column-major FP32 output of the local block placed in the global grid
+// `npts` at its fs offset (the subarray view of scarflib_common.f90:363-399).
+void scarf_io_one(const int nd, const int* npts, const real* field, const char fname[], const int* nwriters) {
+  (void)nwriters;
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (!g_obj.ready || !g_obj.structured || !npts || !field || !fname) {
+    fail(SCARF_ERR_STATE, "scarf_io_one: needs an initialized structured mesh");
+    return;
+  }
+  long long gn[3] = {npts[0], nd > 1 ? npts[1] : 1, nd > 2 ? npts[2] : 1};
+  int n[3];
+  for (int c = 0; c < 3; ++c) n[c] = g_obj.fe[c] - g_obj.fs[c] + 1;
+  const int fd = open(fname, O_CREAT | O_WRONLY, 0644);
+  if (fd < 0) {
+    fail(SCARF_ERR_ARG, "scarf_io_one: cannot open %s", fname);
+    return;
+  }
+  for (int k = 0; k < n[2]; ++k)
+    for (int j = 0; j < n[1]; ++j) {
+      const long long gi = (g_obj.fs[0] - 1) + gn[0] * ((g_obj.fs[1] - 1 + j) + gn[1] * (g_obj.fs[2] - 1 + k));
+      const real* src = field + static_cast<long long>(n[0]) * (j + static_cast<long long>(n[1]) * k);
+      if (pwrite(fd, src, sizeof(real) * n[0], static_cast<off_t>(gi * sizeof(real))) < 0) {
+        fail(SCARF_ERR_ARG, "scarf_io_one: write failed");
+        close(fd);
+        return;
+      }
+    }
+  close(fd);
+}
+
+// One plane normal to `axis` ('x','y','z') at global index `plane`
+// (scarflib_common.f90:527-646), written as a 2-D column-major FP32 array.
+void scarf_io_slice(const int* npts, const char axis[], const int plane, const real* field, const char fname[]) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (!g_obj.ready || !g_obj.structured || !npts || !axis || !field || !fname) {
+    fail(SCARF_ERR_STATE, "scarf_io_slice: needs an initialized structured mesh");
+    return;
+  }
+  const int cut = axis[0] == 'x' ? 0 : axis[0] == 'y' ? 1 : axis[0] == 'z' ? 2 : -1;
+  if (cut < 0) return;
+  if (plane < g_obj.fs[cut] || plane > g_obj.fe[cut]) return;
+  int n[3];
+  for (int c = 0; c < 3; ++c) n[c] = g_obj.fe[c] - g_obj.fs[c] + 1;
+  const int d0 = cut == 0 ? 1 : 0, d1 = cut == 2 ? 1 : 2;
+  const int cidx = plane - g_obj.fs[cut];
+  const int fd = open(fname, O_CREAT | O_WRONLY, 0644);
+  if (fd < 0) {
+    fail(SCARF_ERR_ARG, "scarf_io_slice: cannot open %s", fname);
+    return;
+  }
+  std::vector<real> row(n[d0]);
+  for (int b = 0; b < n[d1]; ++b) {
+    for (int a = 0; a < n[d0]; ++a) {
+      int idx[3];
+      idx[cut] = cidx;
+      idx[d0] = a;
+      idx[d1] = b;
+      row[a] = field[idx[0] + static_cast<long long>(n[0]) * (idx[1] + static_cast<long long>(n[1]) * idx[2])];
+    }
+    const long long gi = (g_obj.fs[d0] - 1) + static_cast<long long>(npts[d0]) * (g_obj.fs[d1] - 1 + b);
+    if (pwrite(fd, row.data(), sizeof(real) * n[d0], static_cast<off_t>(gi * sizeof(real))) < 0) break;
+  }
+  close(fd);
+}
+
+// ======================================================================== //
+// Extended API                                                              //
+// ======================================================================== //
+const char* scarf_last_error(void) { return g_last_error.c_str(); }
+
+int scarf_set_nharm(int nharm) {
+  if (nharm <= 0) return fail(SCARF_ERR_ARG, "nharm must be positive");
+  std::lock_guard<std::mutex> lk(g_mu);
+  g_cfg.nharm = nharm;
+  return SCARF_OK;
+}
+
+int scarf_get_nharm(void) { return g_cfg.nharm; }
+
+int scarf_set_form(int form) {
+  if (form < SCARF_FORM_AUTO || form > SCARF_FORM_TC) return fail(SCARF_ERR_ARG, "unknown form %d", form);
+  std::lock_guard<std::mutex> lk(g_mu);
+  g_cfg.form = form;
+  return SCARF_OK;
+}
+
+int scarf_set_uniform_source(void (*set_seed)(int), void (*srng)(float*)) {
+  if ((set_seed == nullptr) != (srng == nullptr))
+    return fail(SCARF_ERR_ARG, "set_seed and srng must both be given or both be NULL");
+  std::lock_guard<std::mutex> lk(g_mu);
+  g_cfg.src.set_seed = set_seed;
+  g_cfg.src.srng = srng;
+  return SCARF_OK;
+}
+
+int scarf_set_stream(void* stream) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  g_cfg.stream = static_cast<cudaStream_t>(stream);
+  return SCARF_OK;
+}
+
+int scarf_set_host_threads(int nthreads) {
+  if (nthreads < 0) return fail(SCARF_ERR_ARG, "nthreads must be >= 0");
+  std::lock_guard<std::mutex> lk(g_mu);
+  g_cfg.threads = nthreads;
+  return SCARF_OK;
+}
+
+int scarf_execute_ex(int seed, float* field, float stats[8], int flags) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  return execute_impl(seed, field, stats, flags);
+}
+
+int scarf_srm_compute_setup(const scarf_srm_params* p, scarf_srm_setup* s) {
+  if (!p || !s) return fail(SCARF_ERR_ARG, "NULL argument");
+  const int rc = srm_setup(*p, s);
+  if (rc) return fail(rc, "invalid SRM parameters");
+  return SCARF_OK;
+}
+
+int scarf_srm_sample(const scarf_srm_params* p, const scarf_srm_setup* s, float* table, int* n_kept,
+                     long long* pairs_used) {
+  if (!p || !s || !table) return fail(SCARF_ERR_ARG, "NULL argument");
+  UniformSource src;
+  {
+    std::lock_guard<std::mutex> lk(g_mu);
+    src = g_cfg.src;
+  }
+  const int threads = g_cfg.threads > 0 ? g_cfg.threads : host_threads();
+  long long used = 0;
+  const int kept = srm_sample(*p, *s, &src, threads, table, &used);
+  if (n_kept) *n_kept = kept;
+  if (pairs_used) *pairs_used = used;
+  return SCARF_OK;
+}
+
+int scarf_srm_direct_structured(const scarf_srm_setup* s, const int fs[3], const int n[3], float ds,
+                                const float* d_table, int nh, float* d_field, void* stream) {
+  if (!s || !fs || !n || !d_field || (nh > 0 && !d_table) || nh < 0) return fail(SCARF_ERR_ARG, "invalid argument");
+  if (n[0] <= 0 || n[1] <= 0 || n[2] <= 0) return fail(SCARF_ERR_ARG, "empty grid");
+  std::lock_guard<std::mutex> lk(g_mu);
+  int rc = ensure_resources();
+  if (rc) return rc;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  int* d_status = static_cast<int*>(g_res.status.p);
+  SCARF_CUDA(cudaMemsetAsync(d_status, 0, sizeof(int), st));
+  if (nh == 0) {
+    SCARF_CUDA(cudaMemsetAsync(d_field, 0, sizeof(float) * n[0] * n[1] * n[2], st));
+    return SCARF_OK;
+  }
+  if (kernel_ev0()) SCARF_CUDA(cudaEventRecord(kernel_ev0(), st));
+  SCARF_CUDA(launch_direct_structured(*s, fs, n, ds, d_table, nh, d_field, d_status, st));
+  if (kernel_ev1()) SCARF_CUDA(cudaEventRecord(kernel_ev1(), st));
+  rc = check_device_status(d_status, st);
+  if (!rc) collect_kernel_time();
+  return rc;
+}
+
+int scarf_srm_direct_points(const scarf_srm_setup* s, const float* d_x, const float* d_y, const float* d_z,
+                            long long npts, const float* d_table, int nh, float* d_field, void* stream) {
+  if (!s || !d_x || !d_y || !d_z || !d_field || npts <= 0 || nh < 0 || (nh > 0 && !d_table))
+    return fail(SCARF_ERR_ARG, "invalid argument");
+  std::lock_guard<std::mutex> lk(g_mu);
+  int rc = ensure_resources();
+  if (rc) return rc;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  int* d_status = static_cast<int*>(g_res.status.p);
+  SCARF_CUDA(cudaMemsetAsync(d_status, 0, sizeof(int), st));
+  if (nh == 0) {
+    SCARF_CUDA(cudaMemsetAsync(d_field, 0, sizeof(float) * npts, st));
+    return SCARF_OK;
+  }
+  if (kernel_ev0()) SCARF_CUDA(cudaEventRecord(kernel_ev0(), st));
+  SCARF_CUDA(launch_direct_points(*s, d_x, d_y, d_z, npts, d_table, nh, d_field, d_status, st));
+  if (kernel_ev1()) SCARF_CUDA(cudaEventRecord(kernel_ev1(), st));
+  rc = check_device_status(d_status, st);
+  if (!rc) collect_kernel_time();
+  return rc;
+}
+
+size_t scarf_srm_tc_workspace_bytes(int ndim, const int n[3], int nh) {
+  TcPlan p{};
+  if (!n || !tc_make_plan(ndim, n, nh, &p)) return 0;
+  return p.bytes;
+}
+
+int scarf_srm_tc_structured(const scarf_srm_setup* s, const int fs[3], const int n[3], float ds, const float* d_table,
+                            int nh, float* d_field, void* d_work, size_t work_bytes, void* stream) {
+  if (!s || !fs || !n || !d_field || !d_table || nh <= 0 || !d_work) return fail(SCARF_ERR_ARG, "invalid argument");
+  TcPlan p{};
+  if (!tc_make_plan(s->ndim, n, nh, &p)) return fail(SCARF_ERR_ARG, "invalid grid for the tensor-core form");
+  if (work_bytes < p.bytes) return fail(SCARF_ERR_ARG, "workspace too small: %zu < %zu", work_bytes, p.bytes);
+  if (reinterpret_cast<uintptr_t>(d_work) & 255u) return fail(SCARF_ERR_ARG, "workspace must be 256-byte aligned");
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (g_cfg.kernel_timing) {
+    const int rc = ensure_resources();
+    if (rc) return rc;
+  }
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  int* d_status = reinterpret_cast<int*>(static_cast<char*>(d_work) + p.off_status);
+  SCARF_CUDA(cudaMemsetAsync(d_status, 0, sizeof(int), st));
+  SCARF_CUDA(launch_tc_structured(*s, fs, n, ds, d_table, nh, d_field, d_work, p, d_status, st, kernel_ev0(),
+                                  kernel_ev1()));
+  const int rc = check_device_status(d_status, st);
+  if (!rc) collect_kernel_time();
+  return rc;
+}
+
+int scarf_set_kernel_timing(int enable) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  g_cfg.kernel_timing = enable != 0;
+  return SCARF_OK;
+}
+
+float scarf_last_kernel_ms(void) { return g_last_kernel_ms; }
+
+size_t scarf_field_stats_workspace_bytes(long long n) { return stats_partials_bytes(n) + 256; }
+
+int scarf_field_stats(const float* d_field, long long n, void* d_work, size_t work_bytes, float* mean, float* var,
+                      void* stream) {
+  if (!d_field || n < 2 || !d_work || !mean || !var) return fail(SCARF_ERR_ARG, "invalid argument");
+  if (work_bytes < scarf_field_stats_workspace_bytes(n)) return fail(SCARF_ERR_ARG, "workspace too small");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  double* d_part = static_cast<double*>(d_work);
+  float* d_out = reinterpret_cast<float*>(static_cast<char*>(d_work) + stats_partials_bytes(n));
+  SCARF_CUDA(launch_field_stats(d_field, n, d_part, d_out, st));
+  float mv[2];
+  SCARF_CUDA(cudaMemcpyAsync(mv, d_out, sizeof(mv), cudaMemcpyDeviceToHost, st));
+  SCARF_CUDA(cudaStreamSynchronize(st));
+  *mean = mv[0];
+  *var = mv[1];
+  return SCARF_OK;
+}
+
+}  // extern "C"

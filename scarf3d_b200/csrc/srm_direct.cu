@@ -1,0 +1,210 @@
+// FP32 direct-sum SRM kernels (the "plain" form): for every point,
+//   field = scaling * sum_h [ a_h sin(arg_h) + b_h cos(arg_h) ],
+//   arg_h = v1*P1 + v2*P2 + v3*P3,  P = M x + bar,
+// evaluated in the reference's operation order without FMA contraction
+// (scarflib_srm.f90:794-809 structured, :397-406 points, :843-851 scaling).
+// The rotated coordinates P are loop invariant in the reference, so they are
+// computed once per point; the harmonic table streams through shared memory
+// in tiles moved by 1-D bulk (TMA) copies, double-buffered on mbarriers.
+#include <cuda_runtime.h>
+
+#include "common.cuh"
+#include "srm_kernels.h"
+
+namespace scarf {
+namespace {
+
+constexpr int kTile = 256;           // harmonics per shared-memory tile
+constexpr int kRow = 5;              // floats per table row {v1,v2,v3,a,b}
+constexpr int kPts = 4;              // points per thread (one float4 store)
+constexpr int kThreads = 128;
+constexpr uint32_t kTileBytes = kTile * kRow * 4;  // 5120, multiple of 16
+
+struct DirectArgs {
+  float m[9];
+  float bar[3];
+  float scaling;
+  int nh;
+  const float* table;  // device, nh x 5
+  float* field;
+  long long npts;
+  int* status;
+  // structured
+  int n0, n1;
+  float ds;
+  int off0, off1, off2;  // fs - 2 (so x = (i1 + off) * ds with 1-based i1)
+  // points
+  const float* x;
+  const float* y;
+  const float* z;
+};
+
+__device__ __forceinline__ void rotate(const DirectArgs& A, float x, float y, float z, float& p1, float& p2,
+                                       float& p3) {
+  // ((m1 x + m2 y) + m3 z) + bar, each operation rounded (no contraction).
+  p1 = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(A.m[0], x), __fmul_rn(A.m[1], y)), __fmul_rn(A.m[2], z)), A.bar[0]);
+  p2 = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(A.m[3], x), __fmul_rn(A.m[4], y)), __fmul_rn(A.m[5], z)), A.bar[1]);
+  p3 = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(A.m[6], x), __fmul_rn(A.m[7], y)), __fmul_rn(A.m[8], z)), A.bar[2]);
+}
+
+template <bool kStructured>
+__global__ void __launch_bounds__(kThreads) srm_direct_kernel(const DirectArgs A) {
+  __shared__ __align__(128) float s_tab[2][kTile * kRow];
+  __shared__ __align__(8) uint64_t s_full[2];
+
+  const int tid = threadIdx.x;
+  const long long p0 = (static_cast<long long>(blockIdx.x) * kThreads + tid) * kPts;
+
+  // Rotated coordinates of this thread's points (loop invariant).
+  float P1[kPts], P2[kPts], P3[kPts], acc[kPts];
+#pragma unroll
+  for (int q = 0; q < kPts; ++q) {
+    const long long p = p0 + q < A.npts ? p0 + q : A.npts - 1;
+    float x, y, z;
+    if constexpr (kStructured) {
+      const long long plane = static_cast<long long>(A.n0) * A.n1;
+      const int k = static_cast<int>(p / plane);
+      const long long rem = p - static_cast<long long>(k) * plane;
+      const int j = static_cast<int>(rem / A.n0);
+      const int i = static_cast<int>(rem - static_cast<long long>(j) * A.n0);
+      // x = (i + fs(1) - 2) * ds with the 1-based index i+1.
+      x = __fmul_rn(static_cast<float>(i + 1 + A.off0), A.ds);
+      y = __fmul_rn(static_cast<float>(j + 1 + A.off1), A.ds);
+      z = __fmul_rn(static_cast<float>(k + 1 + A.off2), A.ds);
+    } else {
+      x = __ldg(A.x + p);
+      y = __ldg(A.y + p);
+      z = __ldg(A.z + p);
+    }
+    rotate(A, x, y, z, P1[q], P2[q], P3[q]);
+    acc[q] = 0.0f;
+  }
+
+  const int nfull = A.nh / kTile;            // tiles moved by bulk copy
+  const int tail = A.nh - nfull * kTile;     // rows of the last tile
+  const int ntiles = nfull + (tail ? 1 : 0);
+  const bool aligned = (reinterpret_cast<uintptr_t>(A.table) & 15u) == 0;
+
+  if (tid == 0) {
+    mbar_init(&s_full[0], 1);
+    mbar_init(&s_full[1], 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  int issued = 0;  // bulk copies issued so far (meaningful in thread 0)
+  if (tid == 0 && aligned) {
+    for (int t = 0; t < 2 && t < nfull; ++t) {
+      mbar_arrive_expect_tx(&s_full[t], kTileBytes);
+      bulk_g2s(s_tab[t], A.table + static_cast<size_t>(t) * kTile * kRow, kTileBytes, &s_full[t]);
+      ++issued;
+    }
+  }
+
+  bool ok = true;
+  int t = 0;
+  for (; t < ntiles; ++t) {
+    const int buf = t & 1;
+    int rows = kTile;
+    if (t < nfull && aligned) {
+      if (!mbar_wait_bounded(&s_full[buf], (t >> 1) & 1, A.status)) ok = false;
+    } else {
+      // Unaligned table or the partial last tile: cooperative plain loads.
+      rows = (t < nfull) ? kTile : tail;
+      const float* src = A.table + static_cast<size_t>(t) * kTile * kRow;
+      for (int e = tid; e < rows * kRow; e += kThreads) s_tab[buf][e] = __ldg(src + e);
+      __syncthreads();
+    }
+    if (!__syncthreads_and(ok)) break;  // all threads agree before consuming
+    const float* tb = s_tab[buf];
+#pragma unroll 2
+    for (int h = 0; h < rows; ++h) {
+      const float v1 = tb[h * kRow + 0], v2 = tb[h * kRow + 1], v3 = tb[h * kRow + 2];
+      const float a = tb[h * kRow + 3], b = tb[h * kRow + 4];
+#pragma unroll
+      for (int q = 0; q < kPts; ++q) {
+        const float arg = __fadd_rn(__fadd_rn(__fmul_rn(v1, P1[q]), __fmul_rn(v2, P2[q])), __fmul_rn(v3, P3[q]));
+        float sn, cs;
+        sincosf(arg, &sn, &cs);
+        acc[q] = __fadd_rn(__fadd_rn(acc[q], __fmul_rn(a, sn)), __fmul_rn(b, cs));
+      }
+    }
+    __syncthreads();  // buffer `buf` fully consumed
+    if (tid == 0 && aligned && t + 2 < nfull) {
+      mbar_arrive_expect_tx(&s_full[buf], kTileBytes);
+      bulk_g2s(s_tab[buf], A.table + static_cast<size_t>(t + 2) * kTile * kRow, kTileBytes, &s_full[buf]);
+      ++issued;
+    }
+  }
+  if (!ok) {
+    // Drain the copies still in flight into this block's shared memory
+    // (tiles t .. issued-1) before the block exits; each wait is bounded.
+    if (tid == 0) {
+      for (int u = t; u < issued; ++u) mbar_wait_drain(&s_full[u & 1], (u >> 1) & 1);
+    }
+    return;
+  }
+
+  // Normalise (field * scaling) and store.
+  float out[kPts];
+#pragma unroll
+  for (int q = 0; q < kPts; ++q) out[q] = __fmul_rn(acc[q], A.scaling);
+  float* dst = A.field + p0;
+  if (p0 + kPts <= A.npts && (reinterpret_cast<uintptr_t>(dst) & 15u) == 0) {
+    *reinterpret_cast<float4*>(dst) = make_float4(out[0], out[1], out[2], out[3]);
+  } else {
+#pragma unroll
+    for (int q = 0; q < kPts; ++q)
+      if (p0 + q < A.npts) dst[q] = out[q];
+  }
+}
+
+}  // namespace
+
+cudaError_t launch_direct_structured(const scarf_srm_setup& s, const int fs[3], const int n[3], float ds,
+                                     const float* d_table, int nh, float* d_field, int* d_status,
+                                     cudaStream_t stream) {
+  DirectArgs A{};
+  for (int i = 0; i < 9; ++i) A.m[i] = s.m[i];
+  for (int i = 0; i < 3; ++i) A.bar[i] = s.bar[i];
+  A.scaling = s.scaling;
+  A.nh = nh;
+  A.table = d_table;
+  A.field = d_field;
+  A.npts = static_cast<long long>(n[0]) * n[1] * n[2];
+  A.status = d_status;
+  A.n0 = n[0];
+  A.n1 = n[1];
+  A.ds = ds;
+  A.off0 = fs[0] - 2;
+  A.off1 = fs[1] - 2;
+  A.off2 = fs[2] - 2;
+  const long long per_block = static_cast<long long>(kThreads) * kPts;
+  const long long blocks = (A.npts + per_block - 1) / per_block;
+  if (blocks <= 0) return cudaSuccess;
+  srm_direct_kernel<true><<<static_cast<unsigned>(blocks), kThreads, 0, stream>>>(A);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_direct_points(const scarf_srm_setup& s, const float* d_x, const float* d_y, const float* d_z,
+                                 long long npts, const float* d_table, int nh, float* d_field, int* d_status,
+                                 cudaStream_t stream) {
+  DirectArgs A{};
+  for (int i = 0; i < 9; ++i) A.m[i] = s.m[i];
+  for (int i = 0; i < 3; ++i) A.bar[i] = s.bar[i];
+  A.scaling = s.scaling;
+  A.nh = nh;
+  A.table = d_table;
+  A.field = d_field;
+  A.npts = npts;
+  A.status = d_status;
+  A.x = d_x;
+  A.y = d_y;
+  A.z = d_z;
+  const long long per_block = static_cast<long long>(kThreads) * kPts;
+  const long long blocks = (npts + per_block - 1) / per_block;
+  if (blocks <= 0) return cudaSuccess;
+  srm_direct_kernel<false><<<static_cast<unsigned>(blocks), kThreads, 0, stream>>>(A);
+  return cudaGetLastError();
+}
+
+}  // namespace scarf

@@ -1,0 +1,386 @@
+// Host side of the SRM path: uniform source, setup scalars and the harmonic
+// sampler. Compiled without FMA contraction so that every single-precision
+// operation rounds exactly as the reference's Fortran statement does.
+#include "srm_host.h"
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <thread>
+#include <vector>
+
+namespace scarf {
+
+// pi as the reference declares it (scarflib_common.f90:94): nearest float.
+constexpr float kPi = 3.14159265358979323846f;
+
+// ------------------------------------------------------------ Yarn2 source --
+uint64_t Yarn2::mulmod(uint64_t a, uint64_t b) {
+  // Mersenne reduction: for p < 2^62, p mod (2^31-1) by folding 31-bit digits.
+  uint64_t p = a * b;
+  p = (p & kMod) + (p >> 31);
+  p = (p & kMod) + (p >> 31);
+  return p >= kMod ? p - kMod : p;
+}
+
+namespace {
+// g^r = g^(r & 0xFFFF) * (g^65536)^(r >> 16): two tables of exact residues.
+struct PowTables {
+  std::vector<uint32_t> lo, hi;
+  PowTables() : lo(1u << 16), hi(1u << 15) {
+    uint64_t v = 1;
+    for (uint32_t k = 0; k < (1u << 16); ++k) {
+      lo[k] = static_cast<uint32_t>(v);
+      v = Yarn2::mulmod(v, Yarn2::kGen);
+    }
+    const uint64_t g16 = v;  // g^65536
+    v = 1;
+    for (uint32_t k = 0; k < (1u << 15); ++k) {
+      hi[k] = static_cast<uint32_t>(v);
+      v = Yarn2::mulmod(v, g16);
+    }
+  }
+};
+const PowTables& pow_tables() {
+  static const PowTables t;
+  return t;
+}
+}  // namespace
+
+uint32_t Yarn2::output(uint64_t r) {
+  if (r == 0) return 0u;
+  const PowTables& t = pow_tables();
+  return static_cast<uint32_t>(mulmod(t.lo[r & 0xFFFFu], t.hi[r >> 16]));
+}
+
+void Yarn2::seed(int s) {
+  // trng seed(unsigned long) with the signed seed converted as prng.cpp:147
+  // does; reduced modulo the prime, second word 1 (state never all-zero).
+  const unsigned long us = static_cast<unsigned long>(static_cast<long>(s));
+  r0 = static_cast<uint64_t>(us % static_cast<unsigned long>(kMod));
+  r1 = 1;
+}
+
+uint32_t Yarn2::next_raw() {
+  uint64_t t = mulmod(kA1, r0) + mulmod(kA2, r1);
+  if (t >= kMod) t -= kMod;
+  r1 = r0;
+  r0 = t;
+  return output(t);
+}
+
+void Yarn2::jump(uint64_t n) {
+  // State transition (r0, r1) -> (a1 r0 + a2 r1, r0) as a 2x2 matrix power.
+  uint64_t m00 = kA1, m01 = kA2, m10 = 1, m11 = 0;  // base matrix
+  uint64_t p00 = 1, p01 = 0, p10 = 0, p11 = 1;      // accumulated power
+  auto addm = [](uint64_t a, uint64_t b) {
+    uint64_t s = a + b;
+    return s >= kMod ? s - kMod : s;
+  };
+  while (n) {
+    if (n & 1) {
+      const uint64_t q00 = addm(mulmod(p00, m00), mulmod(p01, m10));
+      const uint64_t q01 = addm(mulmod(p00, m01), mulmod(p01, m11));
+      const uint64_t q10 = addm(mulmod(p10, m00), mulmod(p11, m10));
+      const uint64_t q11 = addm(mulmod(p10, m01), mulmod(p11, m11));
+      p00 = q00, p01 = q01, p10 = q10, p11 = q11;
+    }
+    const uint64_t s00 = addm(mulmod(m00, m00), mulmod(m01, m10));
+    const uint64_t s01 = addm(mulmod(m00, m01), mulmod(m01, m11));
+    const uint64_t s10 = addm(mulmod(m10, m00), mulmod(m11, m10));
+    const uint64_t s11 = addm(mulmod(m10, m01), mulmod(m11, m11));
+    m00 = s00, m01 = s01, m10 = s10, m11 = s11;
+    n >>= 1;
+  }
+  const uint64_t n0 = addm(mulmod(p00, r0), mulmod(p01, r1));
+  const uint64_t n1 = addm(mulmod(p10, r0), mulmod(p11, r1));
+  r0 = n0;
+  r1 = n1;
+}
+
+// ------------------------------------------------------------- spectra -----
+// psdf.f90:65 (von Karman) and :88 (Gaussian), evaluated in FP32.
+static inline float psd_vk(float x, float nu) { return 1.0f / powf(1.0f + x * x, nu); }
+static inline float psd_gs(float x) { return expf(-0.25f * (x * x)); }
+
+double srm_fn(double x, int ndim, int acf, float nu) {
+  const float xf = static_cast<float>(x);
+  const float fv = (acf == 0) ? psd_vk(xf, nu) : psd_gs(xf);
+  double r = x * static_cast<double>(fv);
+  if (ndim == 3) r = r * x;
+  return r;
+}
+
+// --------------------------------------------------------------- setup -----
+int srm_setup(const scarf_srm_params& p, scarf_srm_setup* s) {
+  std::memset(s, 0, sizeof(*s));
+  if (p.acf != 0 && p.acf != 1) return SCARF_ERR_UNSUPPORTED;
+  if (p.nharm <= 0) return SCARF_ERR_ARG;
+  const int ndim = (p.cl[2] > 0.0f) ? 3 : 2;
+  s->ndim = ndim;
+  float span[3];
+  for (int c = 0; c < 3; ++c) span[c] = p.fc[c] - p.nc[c];
+  for (int c = 0; c < ndim; ++c)
+    if (!(span[c] > 0.0f) || !(p.cl[c] > 0.0f)) return SCARF_ERR_ARG;
+  if (!(p.ds > 0.0f) || !(p.dh > 0.0f)) return SCARF_ERR_ARG;
+  // kmin/kmax/kc (scarflib_srm.f90:647-652): MAXVAL(cl/span), MINVAL(cl).
+  float mx = p.cl[0] / span[0], mn = p.cl[0];
+  for (int c = 1; c < ndim; ++c) {
+    mx = std::max(mx, p.cl[c] / span[c]);
+    mn = std::min(mn, p.cl[c]);
+  }
+  s->kmin = (2.0f * kPi) * mx;
+  s->kmax = (kPi / p.dh) * mn;
+  s->kc = (kPi / p.ds) * mn;
+  // Representation warnings (:660-662).
+  for (int c = 0; c < ndim; ++c) {
+    if ((2.0f * kPi) / span[c] >= 1.0f / p.cl[c]) s->info0 = 1.0f;
+    if (p.ds > p.cl[c] / 2.0f) s->info1 = 1.0f;
+  }
+  s->scaling = p.sigma / sqrtf(static_cast<float>(p.nharm));
+  // Rotation about z (alpha), y (beta), x (gamma) (:678-691), row-major.
+  const float ca = cosf(p.alpha * kPi / 180.0f), sa = sinf(p.alpha * kPi / 180.0f);
+  const float cb = cosf(p.beta * kPi / 180.0f), sb = sinf(p.beta * kPi / 180.0f);
+  const float cg = cosf(p.gamma * kPi / 180.0f), sg = sinf(p.gamma * kPi / 180.0f);
+  float* m = s->m;
+  m[0] = ca * cb;
+  m[3] = sa * cb;
+  m[6] = -sb;
+  m[1] = ca * sb * sg - sa * cg;
+  m[4] = sa * sb * sg + ca * cg;
+  m[7] = cb * sg;
+  m[2] = ca * sb * cg + sa * sg;
+  m[5] = sa * sb * cg - ca * sg;
+  m[8] = cb * cg;
+  // Rotation about the half span (:694-700).
+  float half[3], rot[3];
+  for (int c = 0; c < 3; ++c) half[c] = (p.fc[c] - p.nc[c]) / 2.0f;
+  for (int r = 0; r < 3; ++r) rot[r] = m[3 * r] * half[0] + m[3 * r + 1] * half[1] + m[3 * r + 2] * half[2];
+  for (int c = 0; c < 3; ++c) s->bar[c] = half[c] - rot[c];
+  s->nu = p.hurst + static_cast<float>(ndim) / 2.0f;
+  // Majorant constant (:706-716). The reference leaves it unset for a 2D
+  // Gaussian; 1 bounds k*exp(-k^2/4) there, so 1 is used.
+  s->cnst = (p.acf == 1 && ndim == 3) ? 1.0f / sqrtf(kPi) : 1.0f;
+  // Scaling from the spectral integrals (:720, :935-969).
+  double band = 0, full = 0, err = 0;
+  s->ier_band = quad_dqng(ndim, p.acf, s->nu, static_cast<double>(s->kmin), static_cast<double>(s->kmax), 1.0e-8,
+                          1.0e-5, &band, &err);
+  s->ier_full = quad_dqagi(ndim, p.acf, s->nu, 0.0, 1.0e-8, 1.0e-5, 500, &full, &err);
+  s->intg_band = static_cast<float>(band);
+  s->intg_full = static_cast<float>(full);
+  s->scaling0 = s->scaling;
+  s->scaling = s->scaling * sqrtf(s->intg_band / s->intg_full);
+  return SCARF_OK;
+}
+
+int host_threads() {
+  if (const char* e = std::getenv("SCARF_HOST_THREADS")) {
+    const int v = std::atoi(e);
+    if (v > 0) return v;
+  }
+  const unsigned hc = std::thread::hardware_concurrency();
+  return static_cast<int>(std::max(1u, std::min(hc, 64u)));
+}
+
+// ------------------------------------------------------------- sampler -----
+namespace {
+
+// Everything the per-harmonic math needs from the draws of one harmonic.
+struct Draws {
+  float u;
+  float ang[2], ra[2], rb[2];
+  bool skip;
+};
+
+// Per-harmonic arithmetic (scarflib_srm.f90:754-778) in statement order.
+inline void harmonic_row(const Draws& d, int ndim, const float cl[3], float* row) {
+  const float phi = d.ang[0] * 2.0f * kPi;
+  float v1, v2, v3;
+  if (ndim == 3) {
+    const float theta = acosf(1.0f - 2.0f * d.ang[1]);
+    v1 = d.u * sinf(phi) * sinf(theta) / cl[0];
+    v2 = d.u * cosf(phi) * sinf(theta) / cl[1];
+    v3 = d.u * cosf(theta) / cl[2];
+  } else {
+    v1 = d.u * cosf(phi) / cl[0];
+    v2 = d.u * sinf(phi) / cl[1];
+    v3 = 0.0f;
+  }
+  row[0] = v1;
+  row[1] = v2;
+  row[2] = v3;
+  row[3] = sqrtf(-2.0f * logf(d.ra[0])) * cosf(2.0f * kPi * d.ra[1]);
+  row[4] = sqrtf(-2.0f * logf(d.rb[0])) * cosf(2.0f * kPi * d.rb[1]);
+}
+
+inline bool accept(float r1, float r2, const scarf_srm_setup& s, int acf, float* u_out) {
+  const float u = r1 * (s.kmax - s.kmin) + s.kmin;
+  const float d = static_cast<float>(srm_fn(static_cast<double>(u), s.ndim, acf, s.nu) * static_cast<double>(s.cnst));
+  *u_out = u;
+  return r2 < d;
+}
+
+// Serial walk over an arbitrary pair source (the reference's own loop).
+template <class NextPair>
+int walk_serial(const scarf_srm_params& p, const scarf_srm_setup& s, NextPair next, float* table, long long* used) {
+  int kept = 0;
+  long long np = 0;
+  float r[2];
+  for (int l = 0; l < p.nharm; ++l) {
+    Draws d{};
+    for (;;) {
+      next(r);
+      ++np;
+      if (accept(r[0], r[1], s, p.acf, &d.u)) break;
+    }
+    next(r);
+    ++np;
+    if (d.u > s.kc) continue;
+    d.ang[0] = r[0];
+    d.ang[1] = r[1];
+    next(r);
+    ++np;
+    d.ra[0] = r[0];
+    d.ra[1] = r[1];
+    next(r);
+    ++np;
+    d.rb[0] = r[0];
+    d.rb[1] = r[1];
+    harmonic_row(d, s.ndim, p.cl, table + 5 * static_cast<size_t>(kept));
+    ++kept;
+  }
+  if (used) *used = np;
+  return kept;
+}
+
+// Parallel form for the built-in generator. The pair stream is cut into
+// rounds; in each round `threads` workers evaluate the rejection test for
+// consecutive chunks of pairs from jumped copies of the generator, and one
+// walker then consumes the round in stream order exactly as the serial loop
+// would. Decisions and values are those of the serial loop by construction.
+int walk_parallel(const scarf_srm_params& p, const scarf_srm_setup& s, int threads, float* table, long long* used) {
+  // Round size from the expected number of pairs: a pair is accepted with
+  // probability int_{kmin}^{kmax} d(k) dk / (kmax - kmin), and every kept
+  // harmonic consumes three more pairs.
+  double acc_rate = static_cast<double>(s.intg_band) * s.cnst / std::max(1e-30, double(s.kmax) - double(s.kmin));
+  acc_rate = std::min(1.0, std::max(acc_rate, 1e-6));
+  const double expect = p.nharm * (1.0 / acc_rate + 3.0) * 1.05 + 64.0;
+  const int64_t chunk = std::min<int64_t>(1 << 18, std::max<int64_t>(4096, static_cast<int64_t>(expect / threads) + 1));
+  const int64_t round_pairs = chunk * threads;
+  std::vector<float> cur(2 * round_pairs), nxt(2 * round_pairs);
+  std::vector<uint8_t> acc_cur(round_pairs), acc_nxt(round_pairs);
+  std::vector<float> u_cur(round_pairs), u_nxt(round_pairs);
+  Yarn2 base;
+  base.seed(p.seed);
+
+  auto fill = [&](int64_t first_pair, std::vector<float>& r, std::vector<uint8_t>& acc, std::vector<float>& uu) {
+    std::vector<std::thread> pool;
+    pool.reserve(threads);
+    for (int t = 0; t < threads; ++t) {
+      pool.emplace_back([&, t]() {
+        Yarn2 g = base;
+        g.jump(2ull * static_cast<uint64_t>(first_pair + t * chunk));
+        for (int64_t q = t * chunk; q < (t + 1) * chunk; ++q) {
+          const float r1 = g.next_u01(), r2 = g.next_u01();
+          r[2 * q] = r1;
+          r[2 * q + 1] = r2;
+          float u;
+          acc[q] = accept(r1, r2, s, p.acf, &u) ? 1 : 0;
+          uu[q] = u;
+        }
+      });
+    }
+    for (auto& th : pool) th.join();
+  };
+
+  int64_t cur_first = 0;
+  fill(0, cur, acc_cur, u_cur);
+  bool have_next = false;
+  auto ensure_next = [&]() {
+    if (!have_next) {
+      fill(cur_first + round_pairs, nxt, acc_nxt, u_nxt);
+      have_next = true;
+    }
+  };
+  auto advance_round = [&]() {
+    ensure_next();
+    std::swap(cur, nxt);
+    std::swap(acc_cur, acc_nxt);
+    std::swap(u_cur, u_nxt);
+    cur_first += round_pairs;
+    have_next = false;
+  };
+  // Pair q (global index) values; q may reach into the next round.
+  auto pair_at = [&](int64_t q, float out[2]) {
+    int64_t k = q - cur_first;
+    if (k < round_pairs) {
+      out[0] = cur[2 * k];
+      out[1] = cur[2 * k + 1];
+    } else {
+      ensure_next();
+      k -= round_pairs;
+      out[0] = nxt[2 * k];
+      out[1] = nxt[2 * k + 1];
+    }
+  };
+
+  int kept = 0;
+  int64_t pos = 0;  // next unconsumed pair
+  for (int l = 0; l < p.nharm; ++l) {
+    // First accepted pair at or after pos.
+    float u = 0.0f;
+    for (;;) {
+      while (pos - cur_first >= round_pairs) advance_round();
+      const int64_t k = pos - cur_first;
+      const int64_t end = round_pairs;
+      int64_t j = k;
+      while (j < end && !acc_cur[j]) ++j;
+      if (j < end) {
+        u = u_cur[j];
+        pos = cur_first + j + 1;
+        break;
+      }
+      pos = cur_first + end;
+    }
+    Draws d{};
+    d.u = u;
+    pair_at(pos, d.ang);
+    ++pos;
+    if (u > s.kc) continue;
+    pair_at(pos, d.ra);
+    ++pos;
+    pair_at(pos, d.rb);
+    ++pos;
+    harmonic_row(d, s.ndim, p.cl, table + 5 * static_cast<size_t>(kept));
+    ++kept;
+  }
+  if (used) *used = pos;
+  return kept;
+}
+
+}  // namespace
+
+int srm_sample(const scarf_srm_params& p, const scarf_srm_setup& s, const UniformSource* src, int threads,
+               float* table, long long* pairs_used) {
+  if (src && src->srng) {
+    if (src->set_seed) src->set_seed(p.seed);
+    return walk_serial(p, s, [&](float r[2]) { src->srng(r); }, table, pairs_used);
+  }
+  if (threads <= 1 || p.nharm < 64) {
+    Yarn2 g;
+    g.seed(p.seed);
+    return walk_serial(
+        p, s,
+        [&](float r[2]) {
+          r[0] = g.next_u01();
+          r[1] = g.next_u01();
+        },
+        table, pairs_used);
+  }
+  return walk_parallel(p, s, threads, table, pairs_used);
+}
+
+}  // namespace scarf

@@ -1,0 +1,66 @@
+// Host-side pieces of the SRM path: parameters, derived setup, uniform
+// source, quadrature and the harmonic sampler. Pure C++ (no CUDA types).
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <vector>
+
+#include "scarf3d_b200.h"
+
+namespace scarf {
+
+// YARN2-type uniform source: order-2 multiple recursive generator modulo the
+// Mersenne prime 2^31-1 (multipliers 1498809829, 1160990996) whose output is
+// the power g^r mod (2^31-1), g = 123567893 -- the parameters TRNG publishes
+// for trng::yarn2, which prng.cpp:60 instantiates. Draws map to floats in the
+// open interval (0,1) as ((y >> 8) + 0.5) * 2^-23.
+class Yarn2 {
+ public:
+  static constexpr uint64_t kMod = 2147483647ull;
+  static constexpr uint64_t kA1 = 1498809829ull;
+  static constexpr uint64_t kA2 = 1160990996ull;
+  static constexpr uint64_t kGen = 123567893ull;
+
+  void seed(int s);
+  uint32_t next_raw();
+  float next_u01() { return to_u01(next_raw()); }
+  // Advance the state by n raw draws in O(log n).
+  void jump(uint64_t n);
+
+  static float to_u01(uint32_t y) { return (static_cast<float>(y >> 8) + 0.5f) * (1.0f / 8388608.0f); }
+  static uint32_t output(uint64_t r);  // g^r mod m (0 for r == 0)
+  static uint64_t mulmod(uint64_t a, uint64_t b);
+
+  uint64_t r0 = 0, r1 = 1;  // r0 = newest state word
+};
+
+// Spectral integrand of the SRM (scarflib_srm.f90:975-995 with
+// psdf.f90:50-90): x * psd(float(x)) [* x in 3D], FP32 spectrum, FP64 rest.
+double srm_fn(double x, int ndim, int acf, float nu);
+
+// QUADPACK restatements (quadpack.f90): DQNG (:8137) over [a,b] and DQAGI
+// (:1177, via DQAGIE :712) over [bound, +inf). Return the QUADPACK ier.
+int quad_dqng(int ndim, int acf, float nu, double a, double b, double epsabs, double epsrel, double* result,
+              double* abserr);
+int quad_dqagi(int ndim, int acf, float nu, double bound, double epsabs, double epsrel, int limit,
+               double* result, double* abserr);
+
+// Derived scalars (scarflib_srm.f90:617-720).
+int srm_setup(const scarf_srm_params& p, scarf_srm_setup* s);
+
+// Harmonic sampler (scarflib_srm.f90:731-778). Fills table rows
+// {v1,v2,v3,a,b} for kept harmonics; returns the count kept. Uses the
+// caller-supplied uniform source when one is installed, else Yarn2; with
+// Yarn2 the rejection tests run on `threads` host threads over jumped
+// sub-streams and the result is identical to the serial walk.
+struct UniformSource {
+  void (*set_seed)(int) = nullptr;
+  void (*srng)(float*) = nullptr;
+};
+int srm_sample(const scarf_srm_params& p, const scarf_srm_setup& s, const UniformSource* src, int threads,
+               float* table, long long* pairs_used);
+
+int host_threads();
+
+}  // namespace scarf

@@ -1,0 +1,56 @@
+// Launchers of the SRM device kernels (host-callable, no allocation inside).
+#pragma once
+
+#include <cstddef>
+#include <cuda_runtime.h>
+
+#include "scarf3d_b200.h"
+
+namespace scarf {
+
+// ---- direct sum (srm_direct.cu) ----
+cudaError_t launch_direct_structured(const scarf_srm_setup& s, const int fs[3], const int n[3], float ds,
+                                     const float* d_table, int nh, float* d_field, int* d_status,
+                                     cudaStream_t stream);
+cudaError_t launch_direct_points(const scarf_srm_setup& s, const float* d_x, const float* d_y, const float* d_z,
+                                 long long npts, const float* d_table, int nh, float* d_field, int* d_status,
+                                 cudaStream_t stream);
+
+// ---- factorised tensor-core form (srm_tc.cu) ----
+// Geometry of one structured field in the factorised form:
+//   out[i + n1*(j + n2*k)] = scale * Re sum_h R_h(i) S_h(j) C_h(k)
+// with (n1,n2,n3) = (nx,ny,nz) in 3D and (nx,1,ny) in 2D.
+struct TcPlan {
+  int n1, n2, n3;        // logical extents
+  int ti, tj;            // row tile = ti x tj = 128 rows over (i, j)
+  int bi, bj;            // number of row blocks along i and j
+  int ntile_n;           // column tile width (multiple of 16, <= 256)
+  int bn;                // number of column blocks
+  int nh;                // harmonics
+  int nh_pad;            // padded to a multiple of the stage size
+  int stages;            // nh_pad / kStageHarm
+  size_t off_r, off_s, off_c, off_status, bytes;  // workspace layout
+};
+
+bool tc_make_plan(int ndim, const int n[3], int nh, TcPlan* plan);
+cudaError_t launch_tc_structured(const scarf_srm_setup& s, const int fs[3], const int n[3], float ds,
+                                 const float* d_table, int nh, float* d_field, void* d_work, const TcPlan& plan,
+                                 int* d_status, cudaStream_t stream, cudaEvent_t ev_main0 = nullptr,
+                                 cudaEvent_t ev_main1 = nullptr);
+
+// ---- statistics and post-processing (srm_stats.cu) ----
+size_t stats_partials_bytes(long long n);
+// Two passes (mean, then centred sums) in FP64; writes mean/var (FP32
+// results as the reference returns them) to d_out[0..1] (float).
+cudaError_t launch_field_stats(const float* d_field, long long n, double* d_partials, float* d_out,
+                               cudaStream_t stream);
+// field = field * (sigma / std) - mean (scarflib_srm.f90:897-912).
+cudaError_t launch_rescale(float* d_field, long long n, float sigma, float std_, float mean, cudaStream_t stream);
+// Structured / point taper for one point of interest
+// (scarflib_common.f90:881-994).
+cudaError_t launch_taper_structured(float* d_field, const int fs[3], const int n[3], float dh, const float poi[3],
+                                    float mute, float taper, cudaStream_t stream);
+cudaError_t launch_taper_points(float* d_field, const float* d_x, const float* d_y, const float* d_z, long long n,
+                                const float poi[3], float mute, float taper, cudaStream_t stream);
+
+}  // namespace scarf

@@ -1,0 +1,510 @@
+// Factorised tensor-core SRM for structured grids.
+//
+// The phase of harmonic h at grid point (x, y, z) is linear in the
+// coordinates (scarflib_srm.f90:802-804): arg = kx x + ky y + kz z + c with
+// k' = M^T v and c = v . bar. Hence
+//   a sin(arg) + b cos(arg) = Re[(b - i a) e^{i c} e^{i kx x} e^{i ky y} e^{i kz z}]
+// and the field over an (i,j) x k block is a real contraction
+//   F[(i,j), k] = sum_h  Re(P_h(i,j)) cos(kz z_k) - Im(P_h(i,j)) sin(kz z_k),
+//   P_h(i,j) = R_h(i) S_h(j),  R_h(i) = (b - i a) e^{i (kx x_i + c)},  S_h(j) = e^{i ky y_j}.
+// Per-axis factors are computed in FP64 (phases reach ~1e4 rad) and rounded to
+// FP32. The A operand [128 rows x 2 nh] is generated in shared memory from the
+// R and S factor tiles (complex multiply, FP16 hi/lo split); the B operand
+// [cos; sin](kz z) is pre-split into FP16 hi/lo images in global memory and
+// staged by 1-D bulk copies. Three tcgen05 kind::f16 products (hi*hi, hi*lo,
+// lo*hi) accumulate in FP32 in tensor memory.
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+
+#include "common.cuh"
+#include "srm_kernels.h"
+
+namespace scarf {
+namespace {
+
+constexpr int kStageHarm = 16;            // harmonics per pipeline stage (K = 32)
+constexpr int kRows = 128;                // M of one tile (one CTA)
+constexpr int kRowBytes = 64;             // 32 fp16 along K = one 64-B swizzle row
+constexpr int kATileBytes = kRows * kRowBytes;  // 8 KB per hi or lo
+constexpr int kThreads = 512;             // 16 warps
+constexpr int kGenWarp0 = 8;              // warps 8..15 generate A
+constexpr int kEpiWarp0 = 4;              // warps 4..7 drain the accumulators
+constexpr uint32_t kSwizzle64 = 4;        // tcgen05 descriptor: 64-B swizzle
+
+__host__ __device__ constexpr uint32_t swz64(uint32_t row, uint32_t chunk) {
+  return (row >> 3) * 512u + (row & 7u) * 64u + ((chunk ^ ((row & 7u) >> 1)) << 4);
+}
+
+struct TcArgs {
+  // geometry
+  int n1, n2, n3, ti, tj, bi, bj, ntile_n, bn, stages, num_items;
+  int ti_shift;
+  float scaling;
+  uint32_t idesc;
+  // workspace images
+  const float2* rimg;   // [bi][stages][16][ti]
+  const float2* simg;   // [bj][stages][16][tj]
+  const uint8_t* cimg;  // [bn][stages][hi,lo][ntile_n * 64 B]
+  float* field;
+  int* status;
+  // shared-memory carve-up (bytes from the 1024-aligned base)
+  int nstage_buf;
+  uint32_t stage_bytes, off_b, off_a, off_r, off_s, bars_off;
+};
+
+// ------------------------------------------------------------------ tables --
+struct TableArgs {
+  const float* table;  // nh x {v1,v2,v3,a,b}
+  int nh, stages;
+  double m[9], bar[3];
+  double ds;
+  int off[3];          // coordinate of 0-based index t on axis a: (t + off[a]) * ds
+  int ax_r, ax_s, ax_c;  // physical axis of the row-fast, row-slow and column factors
+  int n1, n2, n3, ti, tj, bi, bj, ntile_n, bn;
+  float2* rimg;
+  float2* simg;
+  uint8_t* cimg;
+};
+
+__device__ __forceinline__ void harmonic_k(const TableArgs& T, int h, double k[3], double& c, double& a,
+                                           double& b) {
+  const float* r = T.table + 5 * static_cast<size_t>(h);
+  const double v1 = r[0], v2 = r[1], v3 = r[2];
+  // k'_col = sum_r v_r M[r][col]; c = sum_r v_r bar_r.
+  for (int col = 0; col < 3; ++col) k[col] = v1 * T.m[col] + v2 * T.m[3 + col] + v3 * T.m[6 + col];
+  c = v1 * T.bar[0] + v2 * T.bar[1] + v3 * T.bar[2];
+  a = r[3];
+  b = r[4];
+}
+
+// R image (with the harmonic's complex amplitude and constant phase folded in)
+// and S image. One thread per entry.
+__global__ void tc_build_rs(const TableArgs T) {
+  const long long nr = static_cast<long long>(T.bi) * T.stages * kStageHarm * T.ti;
+  const long long ns = static_cast<long long>(T.bj) * T.stages * kStageHarm * T.tj;
+  for (long long e = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; e < nr + ns;
+       e += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const bool is_r = e < nr;
+    const long long q = is_r ? e : e - nr;
+    const int tw = is_r ? T.ti : T.tj;
+    const int t = static_cast<int>(q % tw);
+    const long long q2 = q / tw;
+    const int hp = static_cast<int>(q2 % kStageHarm);
+    const long long q3 = q2 / kStageHarm;
+    const int k = static_cast<int>(q3 % T.stages);
+    const int blk = static_cast<int>(q3 / T.stages);
+    const int h = k * kStageHarm + hp;
+    const int idx = blk * tw + t;
+    const int nlim = is_r ? T.n1 : T.n2;
+    float2 out = make_float2(0.0f, 0.0f);
+    if (h < T.nh && idx < nlim) {
+      double kv[3], c, a, b;
+      harmonic_k(T, h, kv, c, a, b);
+      const int ax = is_r ? T.ax_r : T.ax_s;
+      const double coord = static_cast<double>(idx + T.off[ax]) * T.ds;
+      double sn, cs;
+      if (is_r) {
+        sincos(kv[ax] * coord + c, &sn, &cs);
+        // (b - i a)(cos + i sin)
+        out = make_float2(static_cast<float>(b * cs + a * sn), static_cast<float>(b * sn - a * cs));
+      } else {
+        sincos(kv[ax] * coord, &sn, &cs);
+        out = make_float2(static_cast<float>(cs), static_cast<float>(sn));
+      }
+    }
+    (is_r ? T.rimg : T.simg)[q] = out;
+  }
+}
+
+// Column image: per (column block, stage) a 64-B-swizzled K-major tile of
+// ntile_n rows x 32 fp16 ([cos, sin] of 16 harmonics), hi then lo.
+__global__ void tc_build_c(const TableArgs T) {
+  const long long nchunks = static_cast<long long>(T.bn) * T.stages * T.ntile_n * 4;
+  for (long long e = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; e < nchunks;
+       e += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const int chunk = static_cast<int>(e & 3);
+    const long long q = e >> 2;
+    const int row = static_cast<int>(q % T.ntile_n);
+    const long long q2 = q / T.ntile_n;
+    const int k = static_cast<int>(q2 % T.stages);
+    const int nb = static_cast<int>(q2 / T.stages);
+    const int col = nb * T.ntile_n + row;
+    __half2 hi[4], lo[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int h = k * kStageHarm + chunk * 4 + u;
+      float cs32 = 0.0f, sn32 = 0.0f;
+      if (h < T.nh && col < T.n3) {
+        double kv[3], c, a, b;
+        harmonic_k(T, h, kv, c, a, b);
+        const double coord = static_cast<double>(col + T.off[T.ax_c]) * T.ds;
+        double sn, cs;
+        sincos(kv[T.ax_c] * coord, &sn, &cs);
+        cs32 = static_cast<float>(cs);
+        sn32 = static_cast<float>(sn);
+      }
+      hi[u] = __floats2half2_rn(cs32, sn32);
+      const float2 hf = __half22float2(hi[u]);
+      lo[u] = __floats2half2_rn(cs32 - hf.x, sn32 - hf.y);
+    }
+    uint8_t* base = T.cimg + (static_cast<size_t>(nb) * T.stages + k) * (2u * T.ntile_n * kRowBytes);
+    const uint32_t off = swz64(static_cast<uint32_t>(row), static_cast<uint32_t>(chunk));
+    *reinterpret_cast<uint4*>(base + off) = *reinterpret_cast<const uint4*>(hi);
+    *reinterpret_cast<uint4*>(base + static_cast<size_t>(T.ntile_n) * kRowBytes + off) =
+        *reinterpret_cast<const uint4*>(lo);
+  }
+}
+
+// ------------------------------------------------------------- main kernel --
+__global__ void __launch_bounds__(kThreads, 1) srm_tc_kernel(const TcArgs A) {
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  const int S = A.nstage_buf;
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + A.bars_off);  // bulk copies landed
+  uint64_t* agen = full + S;                                         // A tile generated
+  uint64_t* empty = agen + S;                                        // stage consumed by MMA
+  uint64_t* accf = empty + S;                                        // accumulator ready [2]
+  uint64_t* acce = accf + 2;                                         // accumulator drained [2]
+  uint64_t* fin = acce + 2;                                          // MMA drain at exit
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(fin + 1);
+
+  const int warp = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < S; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&agen[s], kThreads / 32 - kGenWarp0);
+      mbar_init(&empty[s], 1);
+    }
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(&accf[b], 1);
+      mbar_init(&acce[b], 4);
+    }
+    mbar_init(fin, 1);
+    fence_mbar_init();
+  }
+  if (warp == 2) {
+    tmem_alloc(tmem_slot, 512);
+    tmem_relinquish();
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem_base = *tmem_slot;
+
+  const int tiles_m = A.bi * A.bj;
+  bool ok = true;
+
+  if (warp == 0) {
+    // ------------------------------------------------------ producer -------
+    uint32_t cnt = 0;
+    uint32_t last_cnt[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    bool used[8] = {false, false, false, false, false, false, false, false};
+    for (int item = blockIdx.x; item < A.num_items && ok; item += gridDim.x) {
+      const int nt = item / tiles_m;
+      const int mt = item - nt * tiles_m;
+      const int ib = mt % A.bi;
+      const int jb = mt / A.bi;
+      for (int k = 0; k < A.stages; ++k, ++cnt) {
+        const int s = cnt % S;
+        const uint32_t ph = (cnt / S) & 1;
+        if (!mbar_wait_bounded(&empty[s], ph ^ 1, A.status)) {
+          ok = false;
+          break;
+        }
+        if (lane == 0) {
+          uint8_t* st = smem + s * A.stage_bytes;
+          const uint32_t bbytes = 2u * A.ntile_n * kRowBytes;
+          const uint32_t rbytes = kStageHarm * A.ti * 8u;
+          const uint32_t sbytes = kStageHarm * A.tj * 8u;
+          mbar_arrive_expect_tx(&full[s], bbytes + rbytes + sbytes);
+          bulk_g2s(st + A.off_b, A.cimg + (static_cast<size_t>(nt) * A.stages + k) * bbytes, bbytes, &full[s]);
+          bulk_g2s(st + A.off_r, A.rimg + (static_cast<size_t>(ib) * A.stages + k) * kStageHarm * A.ti, rbytes,
+                   &full[s]);
+          bulk_g2s(st + A.off_s, A.simg + (static_cast<size_t>(jb) * A.stages + k) * kStageHarm * A.tj, sbytes,
+                   &full[s]);
+        }
+        last_cnt[s] = cnt;
+        used[s] = true;
+        __syncwarp();
+      }
+    }
+    if (!ok) {
+      // Let every issued copy land before shared memory is released.
+      for (int s = 0; s < S; ++s)
+        if (used[s]) mbar_wait_drain(&full[s], (last_cnt[s] / S) & 1);
+    }
+  } else if (warp == 1) {
+    // ------------------------------------------------------- MMA issuer ----
+    uint32_t cnt = 0, acc_cnt = 0;
+    bool issued_any = false;
+    for (int item = blockIdx.x; item < A.num_items && ok; item += gridDim.x, ++acc_cnt) {
+      const int buf = acc_cnt & 1;
+      const uint32_t aph = (acc_cnt >> 1) & 1;
+      if (!mbar_wait_bounded(&acce[buf], aph ^ 1, A.status)) {
+        ok = false;
+        break;
+      }
+      tc_fence_after();
+      const uint32_t d_tmem = tmem_base + static_cast<uint32_t>(buf * 256);
+      for (int k = 0; k < A.stages; ++k, ++cnt) {
+        const int s = cnt % S;
+        const uint32_t ph = (cnt / S) & 1;
+        if (!mbar_wait_bounded(&full[s], ph, A.status) || !mbar_wait_bounded(&agen[s], ph, A.status)) {
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        if (lane == 0) {
+          const uint32_t st = smem_u32(smem + s * A.stage_bytes);
+          const uint32_t a_hi = st + A.off_a, a_lo = a_hi + kATileBytes;
+          const uint32_t b_hi = st + A.off_b, b_lo = b_hi + A.ntile_n * kRowBytes;
+#pragma unroll
+          for (int kk = 0; kk < 2; ++kk) {
+            const uint64_t dah = umma_smem_desc(a_hi + 32 * kk, 16, 512, kSwizzle64);
+            const uint64_t dal = umma_smem_desc(a_lo + 32 * kk, 16, 512, kSwizzle64);
+            const uint64_t dbh = umma_smem_desc(b_hi + 32 * kk, 16, 512, kSwizzle64);
+            const uint64_t dbl = umma_smem_desc(b_lo + 32 * kk, 16, 512, kSwizzle64);
+            umma_f16(d_tmem, dah, dbh, A.idesc, (k > 0 || kk > 0) ? 1u : 0u);
+            umma_f16(d_tmem, dah, dbl, A.idesc, 1u);
+            umma_f16(d_tmem, dal, dbh, A.idesc, 1u);
+          }
+          umma_commit(&empty[s]);
+          issued_any = true;
+        }
+        __syncwarp();
+      }
+      if (!ok) break;
+      if (lane == 0) umma_commit(&accf[buf]);
+      __syncwarp();
+    }
+    if (lane == 0 && issued_any) {
+      // All MMAs of this CTA complete before tensor memory is released.
+      umma_commit(fin);
+      mbar_wait_drain(fin, 0);
+    }
+    __syncwarp();
+  } else if (warp >= kEpiWarp0 && warp < kEpiWarp0 + 4) {
+    // --------------------------------------------------------- epilogue ----
+    const int q = warp & 3;
+    const int r = q * 32 + lane;
+    const int ii = r & (A.ti - 1);
+    const int jj = r >> A.ti_shift;
+    uint32_t acc_cnt = 0;
+    for (int item = blockIdx.x; item < A.num_items && ok; item += gridDim.x, ++acc_cnt) {
+      const int buf = acc_cnt & 1;
+      const uint32_t aph = (acc_cnt >> 1) & 1;
+      if (!mbar_wait_bounded(&accf[buf], aph, A.status)) {
+        ok = false;
+        break;
+      }
+      tc_fence_after();
+      const int nt = item / tiles_m;
+      const int mt = item - nt * tiles_m;
+      const int i = (mt % A.bi) * A.ti + ii;
+      const int j = (mt / A.bi) * A.tj + jj;
+      const bool row_ok = (i < A.n1) && (j < A.n2);
+      const long long plane = static_cast<long long>(A.n1) * A.n2;
+      float* dst = A.field + i + static_cast<long long>(A.n1) * j;
+      const int k0 = nt * A.ntile_n;
+      for (int c0 = 0; c0 < A.ntile_n; c0 += 32) {
+        uint32_t v[32];
+        tmem_ld_32x32b_x32(tmem_base + (static_cast<uint32_t>(q * 32) << 16) + buf * 256 + c0, v);
+        tmem_wait_ld();
+        if (row_ok) {
+#pragma unroll
+          for (int c = 0; c < 32; ++c) {
+            const int kcol = k0 + c0 + c;
+            if (c0 + c < A.ntile_n && kcol < A.n3)
+              dst[plane * kcol] = __fmul_rn(__uint_as_float(v[c]), A.scaling);
+          }
+        }
+      }
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&acce[buf]);
+    }
+  } else if (warp >= kGenWarp0) {
+    // -------------------------------------------------------- generators ---
+    const int g = threadIdx.x - kGenWarp0 * 32;  // 0..255
+    const int r = g & (kRows - 1);
+    const int half = g >> 7;                     // harmonics [8*half, 8*half+8)
+    const int ii = r & (A.ti - 1);
+    const int jj = r >> A.ti_shift;
+    uint32_t cnt = 0;
+    for (int item = blockIdx.x; item < A.num_items && ok; item += gridDim.x) {
+      for (int k = 0; k < A.stages; ++k, ++cnt) {
+        const int s = cnt % S;
+        const uint32_t ph = (cnt / S) & 1;
+        if (!mbar_wait_bounded(&full[s], ph, A.status)) {
+          ok = false;
+          break;
+        }
+        uint8_t* st = smem + s * A.stage_bytes;
+        const float2* rt = reinterpret_cast<const float2*>(st + A.off_r);
+        const float2* stt = reinterpret_cast<const float2*>(st + A.off_s);
+        uint8_t* a_hi = st + A.off_a;
+        uint8_t* a_lo = a_hi + kATileBytes;
+#pragma unroll
+        for (int cc = 0; cc < 2; ++cc) {
+          const int chunk = half * 2 + cc;
+          __half2 hv[4], lv[4];
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            const int hp = chunk * 4 + u;
+            const float2 x = rt[hp * A.ti + ii];
+            const float2 y = stt[hp * A.tj + jj];
+            const float re = x.x * y.x - x.y * y.y;
+            const float nim = -(x.x * y.y + x.y * y.x);
+            hv[u] = __floats2half2_rn(re, nim);
+            const float2 hf = __half22float2(hv[u]);
+            lv[u] = __floats2half2_rn(re - hf.x, nim - hf.y);
+          }
+          const uint32_t off = swz64(static_cast<uint32_t>(r), static_cast<uint32_t>(chunk));
+          *reinterpret_cast<uint4*>(a_hi + off) = *reinterpret_cast<const uint4*>(hv);
+          *reinterpret_cast<uint4*>(a_lo + off) = *reinterpret_cast<const uint4*>(lv);
+        }
+        fence_proxy_async_smem();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&agen[s]);
+      }
+    }
+  }
+
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 2) {
+    tc_fence_after();
+    tmem_dealloc(tmem_base, 512);
+  }
+}
+
+int ilog2(int v) {
+  int s = 0;
+  while ((1 << s) < v) ++s;
+  return s;
+}
+
+}  // namespace
+
+bool tc_make_plan(int ndim, const int n[3], int nh, TcPlan* P) {
+  if (nh <= 0 || n[0] <= 0 || n[1] <= 0 || n[2] <= 0) return false;
+  TcPlan p{};
+  p.n1 = n[0];
+  if (ndim == 3) {
+    p.n2 = n[1];
+    p.n3 = n[2];
+  } else {
+    p.n2 = n[2];  // the single z plane
+    p.n3 = n[1];
+  }
+  p.tj = 1;
+  while (p.tj < 8 && p.tj * 2 <= p.n2) p.tj *= 2;
+  p.ti = kRows / p.tj;
+  p.bi = (p.n1 + p.ti - 1) / p.ti;
+  p.bj = (p.n2 + p.tj - 1) / p.tj;
+  const int n3_16 = (p.n3 + 15) / 16 * 16;
+  p.bn = (n3_16 + 255) / 256;
+  p.ntile_n = ((p.n3 + p.bn - 1) / p.bn + 15) / 16 * 16;
+  p.nh = nh;
+  p.nh_pad = (nh + kStageHarm - 1) / kStageHarm * kStageHarm;
+  p.stages = p.nh_pad / kStageHarm;
+  auto align = [](size_t v) { return (v + 255) / 256 * 256; };
+  size_t off = 0;
+  p.off_r = off;
+  off = align(off + static_cast<size_t>(p.bi) * p.stages * kStageHarm * p.ti * sizeof(float2));
+  p.off_s = off;
+  off = align(off + static_cast<size_t>(p.bj) * p.stages * kStageHarm * p.tj * sizeof(float2));
+  p.off_c = off;
+  off = align(off + static_cast<size_t>(p.bn) * p.stages * 2 * p.ntile_n * kRowBytes);
+  p.off_status = off;
+  off = align(off + 256);
+  p.bytes = off;
+  *P = p;
+  return true;
+}
+
+cudaError_t launch_tc_structured(const scarf_srm_setup& s, const int fs[3], const int n[3], float ds,
+                                 const float* d_table, int nh, float* d_field, void* d_work, const TcPlan& p,
+                                 int* d_status, cudaStream_t stream, cudaEvent_t ev_main0, cudaEvent_t ev_main1) {
+  uint8_t* work = static_cast<uint8_t*>(d_work);
+  TableArgs T{};
+  T.table = d_table;
+  T.nh = nh;
+  T.stages = p.stages;
+  for (int i = 0; i < 9; ++i) T.m[i] = s.m[i];
+  for (int i = 0; i < 3; ++i) T.bar[i] = s.bar[i];
+  T.ds = ds;
+  for (int a = 0; a < 3; ++a) T.off[a] = fs[a] - 1;  // 0-based t -> (t + fs - 1) * ds
+  T.ax_r = 0;
+  T.ax_s = (s.ndim == 3) ? 1 : 2;
+  T.ax_c = (s.ndim == 3) ? 2 : 1;
+  T.n1 = p.n1;
+  T.n2 = p.n2;
+  T.n3 = p.n3;
+  T.ti = p.ti;
+  T.tj = p.tj;
+  T.bi = p.bi;
+  T.bj = p.bj;
+  T.ntile_n = p.ntile_n;
+  T.bn = p.bn;
+  T.rimg = reinterpret_cast<float2*>(work + p.off_r);
+  T.simg = reinterpret_cast<float2*>(work + p.off_s);
+  T.cimg = work + p.off_c;
+
+  int dev = 0, nsm = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  tc_build_rs<<<nsm * 8, 256, 0, stream>>>(T);
+  tc_build_c<<<nsm * 8, 256, 0, stream>>>(T);
+  cudaError_t le = cudaGetLastError();
+  if (le != cudaSuccess) return le;
+  if (ev_main0) cudaEventRecord(ev_main0, stream);
+
+  TcArgs A{};
+  A.n1 = p.n1;
+  A.n2 = p.n2;
+  A.n3 = p.n3;
+  A.ti = p.ti;
+  A.tj = p.tj;
+  A.bi = p.bi;
+  A.bj = p.bj;
+  A.ntile_n = p.ntile_n;
+  A.bn = p.bn;
+  A.stages = p.stages;
+  A.num_items = p.bi * p.bj * p.bn;
+  A.ti_shift = ilog2(p.ti);
+  A.scaling = s.scaling;
+  A.idesc = umma_idesc_f16_f32(kRows, static_cast<uint32_t>(p.ntile_n));
+  A.rimg = T.rimg;
+  A.simg = T.simg;
+  A.cimg = T.cimg;
+  A.field = d_field;
+  A.status = d_status;
+  // Shared memory per stage: B hi+lo, A hi+lo (1024-aligned), R and S tiles.
+  const uint32_t b_bytes = 2u * p.ntile_n * kRowBytes;
+  A.off_b = 0;
+  A.off_a = (b_bytes + 1023u) & ~1023u;
+  A.off_r = A.off_a + 2u * kATileBytes;
+  A.off_s = A.off_r + kStageHarm * p.ti * 8u;
+  A.stage_bytes = (A.off_s + kStageHarm * p.tj * 8u + 1023u) & ~1023u;
+  const uint32_t budget = 227u * 1024u - 1024u - 256u;
+  int nbuf = static_cast<int>(budget / A.stage_bytes);
+  nbuf = std::min(nbuf, 8);
+  if (nbuf < 2) return cudaErrorInvalidConfiguration;
+  A.nstage_buf = nbuf;
+  A.bars_off = nbuf * A.stage_bytes;
+  const size_t smem = 1024 + A.bars_off + (3 * nbuf + 5) * 8 + 16;
+  cudaError_t e = cudaFuncSetAttribute(srm_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       static_cast<int>(smem));
+  if (e != cudaSuccess) return e;
+  const int grid = std::min(A.num_items, nsm);
+  srm_tc_kernel<<<grid, kThreads, smem, stream>>>(A);
+  if (ev_main1) cudaEventRecord(ev_main1, stream);
+  return cudaGetLastError();
+}
+
+}  // namespace scarf
