@@ -83,6 +83,10 @@ int scarf_set_host_threads(int nthreads);
  * such duration in milliseconds. */
 int scarf_set_kernel_timing(int enable);
 float scarf_last_kernel_ms(void);
+/* Harmonics accumulated in tensor memory before each FP32 drain of the
+ * tensor-core form (0 = default, 512). The tensor core's FP32 accumulation
+ * does not round to nearest, so its error grows with this length. */
+int scarf_set_tc_chunk(int harmonics);
 
 /* Status-returning scarf_execute (c_binding.c:138-143); stats[8] as the
  * reference fills it (stats[4] host seconds, stats[5] device seconds). */

@@ -34,7 +34,7 @@ EXPORTED_SYMBOLS = (
     # extended (include/scarf3d_b200.h)
     "scarf_last_error", "scarf_set_nharm", "scarf_get_nharm", "scarf_set_form",
     "scarf_set_uniform_source", "scarf_set_stream", "scarf_set_host_threads", "scarf_set_kernel_timing",
-    "scarf_last_kernel_ms", "scarf_execute_ex",
+    "scarf_last_kernel_ms", "scarf_set_tc_chunk", "scarf_execute_ex",
     "scarf_srm_compute_setup", "scarf_srm_sample", "scarf_srm_direct_structured",
     "scarf_srm_direct_points", "scarf_srm_tc_workspace_bytes", "scarf_srm_tc_structured",
     "scarf_field_stats_workspace_bytes", "scarf_field_stats",
@@ -101,6 +101,7 @@ def _load() -> ctypes.CDLL:
         "scarf_set_host_threads": (c_int, [c_int]),
         "scarf_set_kernel_timing": (c_int, [c_int]),
         "scarf_last_kernel_ms": (c_float, []),
+        "scarf_set_tc_chunk": (c_int, [c_int]),
         "scarf_execute_ex": (c_int, [c_int, c_void_p, fp, c_int]),
         "scarf_srm_compute_setup": (c_int, [ctypes.POINTER(SrmParams), ctypes.POINTER(SrmSetup)]),
         "scarf_srm_sample": (c_int, [ctypes.POINTER(SrmParams), ctypes.POINTER(SrmSetup), c_void_p, ip,

@@ -678,6 +678,13 @@ int scarf_set_kernel_timing(int enable) {
 
 float scarf_last_kernel_ms(void) { return g_last_kernel_ms; }
 
+int scarf_set_tc_chunk(int harmonics) {
+  if (harmonics < 0) return fail(SCARF_ERR_ARG, "chunk must be >= 0");
+  std::lock_guard<std::mutex> lk(g_mu);
+  tc_set_chunk_harmonics(harmonics);
+  return SCARF_OK;
+}
+
 size_t scarf_field_stats_workspace_bytes(long long n) { return stats_partials_bytes(n) + 256; }
 
 int scarf_field_stats(const float* d_field, long long n, void* d_work, size_t work_bytes, float* mean, float* var,

@@ -29,10 +29,14 @@ struct TcPlan {
   int nh;                // harmonics
   int nh_pad;            // padded to a multiple of the stage size
   int stages;            // nh_pad / kStageHarm
+  int chunk_stages;      // stages per TMEM accumulation chunk (FP32 sum of chunks)
   size_t off_r, off_s, off_c, off_status, bytes;  // workspace layout
 };
 
 bool tc_make_plan(int ndim, const int n[3], int nh, TcPlan* plan);
+// Harmonics accumulated in tensor memory before each FP32 drain (rounded up
+// to whole pipeline stages); 0 restores the default.
+void tc_set_chunk_harmonics(int harmonics);
 cudaError_t launch_tc_structured(const scarf_srm_setup& s, const int fs[3], const int n[3], float ds,
                                  const float* d_table, int nh, float* d_field, void* d_work, const TcPlan& plan,
                                  int* d_status, cudaStream_t stream, cudaEvent_t ev_main0 = nullptr,
