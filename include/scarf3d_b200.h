@@ -114,6 +114,19 @@ int scarf_srm_tc_structured(const scarf_srm_setup *s, const int fs[3], const int
                             const float *d_table, int nh, float *d_field, void *d_work, size_t work_bytes,
                             void *stream);
 
+/* Same tensor-core sum as scarf_srm_tc_structured, for callers that cannot
+ * allocate device memory (their memory belongs to another allocator, or a
+ * per-step cudaMalloc/cudaFree synchronisation is unacceptable). No
+ * counterpart in the reference. Scratch lives in a fixed device array of
+ * scarf_srm_tc_noalloc_capacity_bytes() (64 MiB) that every GPU loading the
+ * library holds until exit; larger grids/harmonic counts return
+ * SCARF_ERR_ARG. The first call on a device looks up the array's device
+ * address, so make it before any stream capture. All calls on a device share
+ * the array: calls that overlap on the GPU race and must be serialised. */
+size_t scarf_srm_tc_noalloc_capacity_bytes(void);
+int scarf_srm_tc_structured_noalloc(const scarf_srm_setup *s, const int fs[3], const int n[3], float ds,
+                                    const float *d_table, int nh, float *d_field, void *stream);
+
 /* Field statistics as the reference computes them (FP64 sums, FP32 results):
  * mean and unbiased variance (scarflib_common.f90:694-817). d_work must hold
  * scarf_field_stats_workspace_bytes(n) bytes. Synchronises the stream. */

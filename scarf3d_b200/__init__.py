@@ -37,6 +37,7 @@ EXPORTED_SYMBOLS = (
     "scarf_last_kernel_ms", "scarf_set_tc_chunk", "scarf_execute_ex",
     "scarf_srm_compute_setup", "scarf_srm_sample", "scarf_srm_direct_structured",
     "scarf_srm_direct_points", "scarf_srm_tc_workspace_bytes", "scarf_srm_tc_structured",
+    "scarf_srm_tc_noalloc_capacity_bytes", "scarf_srm_tc_structured_noalloc",
     "scarf_field_stats_workspace_bytes", "scarf_field_stats",
 )
 
@@ -113,6 +114,9 @@ def _load() -> ctypes.CDLL:
         "scarf_srm_tc_workspace_bytes": (c_size_t, [c_int, ip, c_int]),
         "scarf_srm_tc_structured": (c_int, [ctypes.POINTER(SrmSetup), ip, ip, c_float, c_void_p, c_int,
                                             c_void_p, c_void_p, c_size_t, c_void_p]),
+        "scarf_srm_tc_noalloc_capacity_bytes": (c_size_t, []),
+        "scarf_srm_tc_structured_noalloc": (c_int, [ctypes.POINTER(SrmSetup), ip, ip, c_float, c_void_p, c_int,
+                                                    c_void_p, c_void_p]),
         "scarf_field_stats_workspace_bytes": (c_size_t, [c_ll]),
         "scarf_field_stats": (c_int, [c_void_p, c_ll, c_void_p, c_size_t, fp, fp, c_void_p]),
     }

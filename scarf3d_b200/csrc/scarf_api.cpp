@@ -322,6 +322,10 @@ void finalize_impl() {
 }
 
 }  // namespace
+
+// Error recording for entry points defined in other translation units.
+int record_error(int code, const char* msg) { return fail(code, "%s", msg); }
+
 }  // namespace scarf
 
 using namespace scarf;
