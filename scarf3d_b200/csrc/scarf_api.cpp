@@ -208,6 +208,11 @@ int execute_impl(int seed, float* field, float stats[8], int flags) {
   const int threads = g_cfg.threads > 0 ? g_cfg.threads : host_threads();
   long long pairs = 0;
   const int nh = srm_sample(p, s, &g_cfg.src, threads, table.data(), &pairs);
+  if (nh < 0)
+    return fail(SCARF_ERR_ARG,
+                "rejection sampling infeasible: acceptance rate %.3g < %.1g (domain too small for the correlation "
+                "lengths; stats[0] would flag it)",
+                acceptance_rate(s), kMinAcceptance);
   const double t_host = now_s() - th0;
 
   // Device work.
@@ -597,6 +602,9 @@ int scarf_srm_sample(const scarf_srm_params* p, const scarf_srm_setup* s, float*
   const int threads = g_cfg.threads > 0 ? g_cfg.threads : host_threads();
   long long used = 0;
   const int kept = srm_sample(*p, *s, &src, threads, table, &used);
+  if (kept < 0)
+    return fail(SCARF_ERR_ARG, "rejection sampling infeasible: acceptance rate %.3g < %.1g", acceptance_rate(*s),
+                kMinAcceptance);
   if (n_kept) *n_kept = kept;
   if (pairs_used) *pairs_used = used;
   return SCARF_OK;

@@ -363,8 +363,19 @@ int walk_parallel(const scarf_srm_params& p, const scarf_srm_setup& s, int threa
 
 }  // namespace
 
+double acceptance_rate(const scarf_srm_setup& s) {
+  const double width = static_cast<double>(s.kmax) - static_cast<double>(s.kmin);
+  if (!(width > 0.0)) return 0.0;
+  return static_cast<double>(s.intg_band) * s.cnst / width;
+}
+
 int srm_sample(const scarf_srm_params& p, const scarf_srm_setup& s, const UniformSource* src, int threads,
                float* table, long long* pairs_used) {
+  // The rejection loop (scarflib_srm.f90:731-745) draws until r2 < d(u); its
+  // success probability is the spectral mass in [kmin, kmax] over the
+  // interval width. Below kMinAcceptance a field would take hours of host
+  // time (the reference spins the same way), so such inputs are refused.
+  if (acceptance_rate(s) < kMinAcceptance) return -1;
   if (src && src->srng) {
     if (src->set_seed) src->set_seed(p.seed);
     return walk_serial(p, s, [&](float r[2]) { src->srng(r); }, table, pairs_used);

@@ -61,6 +61,14 @@ struct UniformSource {
 int srm_sample(const scarf_srm_params& p, const scarf_srm_setup& s, const UniformSource* src, int threads,
                float* table, long long* pairs_used);
 
+// Success probability of one rejection trial: spectral mass in [kmin, kmax]
+// times the majorant constant over the interval width. srm_sample returns -1
+// without drawing when it is below kMinAcceptance (the domain is too small
+// for the correlation lengths, e.g. a Gaussian spectrum whose bulk lies below
+// kmin).
+constexpr double kMinAcceptance = 1e-6;
+double acceptance_rate(const scarf_srm_setup& s);
+
 int host_threads();
 
 }  // namespace scarf
