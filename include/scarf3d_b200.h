@@ -114,6 +114,36 @@ int scarf_srm_tc_structured(const scarf_srm_setup *s, const int fs[3], const int
                             const float *d_table, int nh, float *d_field, void *d_work, size_t work_bytes,
                             void *stream);
 
+/* Batched tensor-core form: many structured fields (uneven sizes, spectra,
+ * harmonic counts) in one persistent launch that pulls 128-row output tiles
+ * from a device work queue, longest first. All fields of a batch must share
+ * one row-tile shape (3-D fields with n[1] >= 8 do by default; 2-D fields
+ * form their own batches). No counterpart in the reference, whose SRM
+ * produces one field per call (scarflib_srm.f90:505). */
+typedef struct scarf_tc_field {
+  const scarf_srm_setup *setup; /* read during create only          */
+  int fs[3];
+  int n[3];
+  float ds;
+  const float *d_table; /* nh rows of 5 floats, device            */
+  int nh;
+  float *d_field; /* n[0]*n[1]*n[2] floats, device            */
+  int tile_j;     /* row tile (128/tile_j) x tile_j; 0 = auto   */
+} scarf_tc_field;
+typedef struct scarf_tc_batch scarf_tc_batch;
+size_t scarf_srm_tc_batch_workspace_bytes(const scarf_tc_field *fields, int nfields);
+/* Plans the batch and uploads its descriptors into d_work (synchronous; call
+ * outside stream capture). Tables and outputs must stay valid while the
+ * batch is launched. */
+int scarf_srm_tc_batch_create(const scarf_tc_field *fields, int nfields, void *d_work, size_t work_bytes,
+                              scarf_tc_batch **batch);
+/* Enqueues the batch on `stream` (table builds + one persistent kernel);
+ * makes no synchronising or allocating call. */
+int scarf_srm_tc_batch_launch(const scarf_tc_batch *batch, void *stream);
+/* Synchronises `stream` and reports a kernel-side pipeline failure. */
+int scarf_srm_tc_batch_wait(const scarf_tc_batch *batch, void *stream);
+void scarf_srm_tc_batch_destroy(scarf_tc_batch *batch);
+
 /* Same tensor-core sum as scarf_srm_tc_structured, for callers that cannot
  * allocate device memory (their memory belongs to another allocator, or a
  * per-step cudaMalloc/cudaFree synchronisation is unacceptable). No

@@ -38,6 +38,8 @@ EXPORTED_SYMBOLS = (
     "scarf_srm_compute_setup", "scarf_srm_sample", "scarf_srm_direct_structured",
     "scarf_srm_direct_points", "scarf_srm_tc_workspace_bytes", "scarf_srm_tc_structured",
     "scarf_srm_tc_noalloc_capacity_bytes", "scarf_srm_tc_structured_noalloc",
+    "scarf_srm_tc_batch_workspace_bytes", "scarf_srm_tc_batch_create", "scarf_srm_tc_batch_launch",
+    "scarf_srm_tc_batch_wait", "scarf_srm_tc_batch_destroy",
     "scarf_field_stats_workspace_bytes", "scarf_field_stats",
 )
 
@@ -73,6 +75,13 @@ class SrmSetup(ctypes.Structure):
                 ("bar", ctypes.c_float * 3), ("info0", ctypes.c_float), ("info1", ctypes.c_float),
                 ("intg_band", ctypes.c_float), ("intg_full", ctypes.c_float), ("ier_band", ctypes.c_int),
                 ("ier_full", ctypes.c_int)]
+
+
+class TcField(ctypes.Structure):
+    """scarf_tc_field: one structured field of a batched tensor-core launch."""
+    _fields_ = [("setup", ctypes.POINTER(SrmSetup)), ("fs", ctypes.c_int * 3), ("n", ctypes.c_int * 3),
+                ("ds", ctypes.c_float), ("d_table", ctypes.c_void_p), ("nh", ctypes.c_int),
+                ("d_field", ctypes.c_void_p), ("tile_j", ctypes.c_int)]
 
 
 def _load() -> ctypes.CDLL:
@@ -114,6 +123,12 @@ def _load() -> ctypes.CDLL:
         "scarf_srm_tc_workspace_bytes": (c_size_t, [c_int, ip, c_int]),
         "scarf_srm_tc_structured": (c_int, [ctypes.POINTER(SrmSetup), ip, ip, c_float, c_void_p, c_int,
                                             c_void_p, c_void_p, c_size_t, c_void_p]),
+        "scarf_srm_tc_batch_workspace_bytes": (c_size_t, [ctypes.POINTER(TcField), c_int]),
+        "scarf_srm_tc_batch_create": (c_int, [ctypes.POINTER(TcField), c_int, c_void_p, c_size_t,
+                                              ctypes.POINTER(c_void_p)]),
+        "scarf_srm_tc_batch_launch": (c_int, [c_void_p, c_void_p]),
+        "scarf_srm_tc_batch_wait": (c_int, [c_void_p, c_void_p]),
+        "scarf_srm_tc_batch_destroy": (None, [c_void_p]),
         "scarf_srm_tc_noalloc_capacity_bytes": (c_size_t, []),
         "scarf_srm_tc_structured_noalloc": (c_int, [ctypes.POINTER(SrmSetup), ip, ip, c_float, c_void_p, c_int,
                                                     c_void_p, c_void_p]),
@@ -310,3 +325,48 @@ def set_stream(stream_handle: int | None):
 
 def tc_workspace_bytes(ndim: int, n, nh: int) -> int:
     return int(lib.scarf_srm_tc_workspace_bytes(int(ndim), _iptr(n), int(nh)))
+
+
+class TcBatch:
+    """Batched tensor-core launch over many structured fields.
+
+    `entries` is a list of dicts with keys setup (SrmSetup), fs, n, ds,
+    d_table (device pointer), nh, d_field (device pointer) and optional tile_j.
+    `alloc(nbytes)` returns a device buffer object exposing data_ptr() (e.g. a
+    torch.uint8 CUDA tensor) that stays alive with the batch.
+    """
+
+    def __init__(self, entries, alloc):
+        self._setups = [e["setup"] for e in entries]
+        arr = (TcField * len(entries))()
+        for k, e in enumerate(entries):
+            f = arr[k]
+            f.setup = ctypes.pointer(self._setups[k])
+            for c in range(3):
+                f.fs[c] = int(e["fs"][c])
+                f.n[c] = int(e["n"][c])
+            f.ds = float(e["ds"])
+            f.d_table = ctypes.c_void_p(int(e["d_table"]))
+            f.nh = int(e["nh"])
+            f.d_field = ctypes.c_void_p(int(e["d_field"]))
+            f.tile_j = int(e.get("tile_j", 0))
+        self._arr = arr
+        self.bytes = int(lib.scarf_srm_tc_batch_workspace_bytes(arr, len(entries)))
+        if self.bytes == 0:
+            raise ScarfError(SCARF_ERR_ARG, "fields cannot share one batched launch")
+        self.work = alloc(self.bytes)
+        self._h = ctypes.c_void_p()
+        check(lib.scarf_srm_tc_batch_create(arr, len(entries), ctypes.c_void_p(self.work.data_ptr()), self.bytes,
+                                            ctypes.byref(self._h)))
+
+    def launch(self, stream_handle: int | None = None):
+        check(lib.scarf_srm_tc_batch_launch(self._h, ctypes.c_void_p(stream_handle or 0)))
+
+    def wait(self, stream_handle: int | None = None):
+        check(lib.scarf_srm_tc_batch_wait(self._h, ctypes.c_void_p(stream_handle or 0)))
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            lib.scarf_srm_tc_batch_destroy(h)
+            self._h = None

@@ -12,6 +12,7 @@
 #include <cstdio>
 #include <cstring>
 #include <mutex>
+#include <new>
 #include <string>
 #include <vector>
 
@@ -681,6 +682,94 @@ int scarf_srm_tc_structured(const scarf_srm_setup* s, const int fs[3], const int
   if (!rc) collect_kernel_time();
   return rc;
 }
+
+}  // extern "C"
+
+struct scarf_tc_batch {
+  scarf::TcBatchPlan plan;
+  void* d_work = nullptr;
+};
+
+namespace {
+std::vector<scarf::TcBatchInput> batch_inputs(const scarf_tc_field* fields, int nfields) {
+  std::vector<scarf::TcBatchInput> in(nfields);
+  for (int f = 0; f < nfields; ++f) {
+    in[f].s = fields[f].setup;
+    for (int c = 0; c < 3; ++c) {
+      in[f].fs[c] = fields[f].fs[c];
+      in[f].n[c] = fields[f].n[c];
+    }
+    in[f].ds = fields[f].ds;
+    in[f].d_table = fields[f].d_table;
+    in[f].nh = fields[f].nh;
+    in[f].d_field = fields[f].d_field;
+    in[f].tj = fields[f].tile_j;
+  }
+  return in;
+}
+
+bool batch_fields_valid(const scarf_tc_field* fields, int nfields) {
+  if (!fields || nfields <= 0) return false;
+  for (int f = 0; f < nfields; ++f)
+    if (!fields[f].setup || !fields[f].d_table || !fields[f].d_field || fields[f].nh <= 0) return false;
+  return true;
+}
+}  // namespace
+
+extern "C" {
+
+size_t scarf_srm_tc_batch_workspace_bytes(const scarf_tc_field* fields, int nfields) {
+  if (!batch_fields_valid(fields, nfields)) return 0;
+  const auto in = batch_inputs(fields, nfields);
+  return tc_batch_plan(in.data(), nfields, nullptr);
+}
+
+int scarf_srm_tc_batch_create(const scarf_tc_field* fields, int nfields, void* d_work, size_t work_bytes,
+                              scarf_tc_batch** batch) {
+  if (!batch || !d_work || !batch_fields_valid(fields, nfields)) return fail(SCARF_ERR_ARG, "invalid argument");
+  if (reinterpret_cast<uintptr_t>(d_work) & 255u) return fail(SCARF_ERR_ARG, "workspace must be 256-byte aligned");
+  const auto in = batch_inputs(fields, nfields);
+  auto* b = new (std::nothrow) scarf_tc_batch();
+  if (!b) return fail(SCARF_ERR_NOMEM, "out of host memory");
+  if (!tc_batch_plan(in.data(), nfields, &b->plan)) {
+    delete b;
+    return fail(SCARF_ERR_ARG, "fields cannot share one launch (row-tile shapes differ or a grid is empty)");
+  }
+  if (work_bytes < b->plan.bytes) {
+    const size_t need = b->plan.bytes;
+    delete b;
+    return fail(SCARF_ERR_ARG, "workspace too small: %zu < %zu", work_bytes, need);
+  }
+  b->d_work = d_work;
+  const cudaError_t e = tc_batch_upload(in.data(), b->plan, d_work);
+  if (e != cudaSuccess) {
+    delete b;
+    return cuda_fail(e, "tc_batch_upload");
+  }
+  *batch = b;
+  return SCARF_OK;
+}
+
+int scarf_srm_tc_batch_launch(const scarf_tc_batch* batch, void* stream) {
+  if (!batch) return fail(SCARF_ERR_ARG, "NULL batch");
+  if (g_cfg.kernel_timing) {
+    const int rc = ensure_resources();
+    if (rc) return rc;
+  }
+  SCARF_CUDA(tc_batch_launch(batch->plan, batch->d_work, static_cast<cudaStream_t>(stream), kernel_ev0(),
+                             kernel_ev1()));
+  return SCARF_OK;
+}
+
+int scarf_srm_tc_batch_wait(const scarf_tc_batch* batch, void* stream) {
+  if (!batch) return fail(SCARF_ERR_ARG, "NULL batch");
+  const int* d_status = reinterpret_cast<const int*>(static_cast<const char*>(batch->d_work) + batch->plan.off_status);
+  const int rc = check_device_status(d_status, static_cast<cudaStream_t>(stream));
+  if (!rc) collect_kernel_time();
+  return rc;
+}
+
+void scarf_srm_tc_batch_destroy(scarf_tc_batch* batch) { delete batch; }
 
 int scarf_set_kernel_timing(int enable) {
   std::lock_guard<std::mutex> lk(g_mu);

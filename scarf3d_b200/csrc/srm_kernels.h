@@ -2,6 +2,8 @@
 #pragma once
 
 #include <cstddef>
+#include <vector>
+
 #include <cuda_runtime.h>
 
 #include "scarf3d_b200.h"
@@ -33,14 +35,42 @@ struct TcPlan {
   size_t off_r, off_s, off_c, off_status, bytes;  // workspace layout
 };
 
-bool tc_make_plan(int ndim, const int n[3], int nh, TcPlan* plan);
+// tj_force > 0 fixes the row tile to (128 / tj_force) x tj_force.
+bool tc_make_plan(int ndim, const int n[3], int nh, TcPlan* plan, int tj_force = 0);
 // Harmonics accumulated in tensor memory before each FP32 drain (rounded up
 // to whole pipeline stages); 0 restores the default.
 void tc_set_chunk_harmonics(int harmonics);
+// Status word at d_status[0]; d_status[1] is used as the work-queue counter.
 cudaError_t launch_tc_structured(const scarf_srm_setup& s, const int fs[3], const int n[3], float ds,
                                  const float* d_table, int nh, float* d_field, void* d_work, const TcPlan& plan,
                                  int* d_status, cudaStream_t stream, cudaEvent_t ev_main0 = nullptr,
                                  cudaEvent_t ev_main1 = nullptr);
+
+// Batched form: many fields in one persistent launch fed by a device work
+// queue. All fields of a batch share one row-tile shape.
+struct TcBatchInput {
+  const scarf_srm_setup* s;
+  int fs[3], n[3];
+  float ds;
+  const float* d_table;
+  int nh;
+  float* d_field;
+  int tj;  // row-tile shape (0 = automatic)
+};
+struct TcBatchPlan {
+  int nfields = 0, num_items = 0, ti = 0, tj = 0, ntile_max = 0;
+  size_t off_fields = 0, off_jobs = 0, off_items = 0, off_status = 0, bytes = 0;
+  std::vector<TcPlan> plans;
+  std::vector<size_t> field_off;
+};
+// Workspace bytes (0 if the fields cannot share one launch).
+size_t tc_batch_plan(const TcBatchInput* in, int nfields, TcBatchPlan* out);
+// Host -> device upload of descriptors, table jobs and the work list
+// (synchronous; not for use inside stream capture).
+cudaError_t tc_batch_upload(const TcBatchInput* in, const TcBatchPlan& plan, void* d_work);
+// Enqueue only: status/queue reset, table builds, persistent kernel.
+cudaError_t tc_batch_launch(const TcBatchPlan& plan, void* d_work, cudaStream_t stream,
+                            cudaEvent_t ev_main0 = nullptr, cudaEvent_t ev_main1 = nullptr);
 
 // ---- statistics and post-processing (srm_stats.cu) ----
 size_t stats_partials_bytes(long long n);

@@ -1,4 +1,5 @@
-// Factorised tensor-core SRM for structured grids.
+// Factorised tensor-core SRM for structured grids, single field or a batch of
+// fields in one persistent launch.
 //
 // The phase of harmonic h at grid point (x, y, z) is linear in the
 // coordinates (scarflib_srm.f90:802-804): arg = kx x + ky y + kz z + c with
@@ -13,10 +14,18 @@
 // [cos; sin](kz z) is pre-split into FP16 hi/lo images in global memory and
 // staged by 1-D bulk copies. Three tcgen05 kind::f16 products (hi*hi, hi*lo,
 // lo*hi) accumulate in FP32 in tensor memory.
+//
+// Work distribution: one persistent CTA per SM pulls work items (one 128-row
+// x <=256-column output tile of one field) from a device work queue (an
+// atomic counter over an item list sorted longest first); the producer warp
+// fetches each item and broadcasts it to the other warp roles through a small
+// shared-memory ring.
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <numeric>
+#include <vector>
 
 #include "common.cuh"
 #include "srm_kernels.h"
@@ -24,44 +33,53 @@
 namespace scarf {
 namespace {
 
-constexpr int kStageHarm = 16;            // harmonics per pipeline stage (K = 32)
-constexpr int kRows = 128;                // M of one tile (one CTA)
-constexpr int kRowBytes = 64;             // 32 fp16 along K = one 64-B swizzle row
+constexpr int kStageHarm = 16;                  // harmonics per pipeline stage (K = 32)
+constexpr int kRows = 128;                      // M of one tile (one CTA)
+constexpr int kRowBytes = 64;                   // 32 fp16 along K = one 64-B swizzle row
 constexpr int kATileBytes = kRows * kRowBytes;  // 8 KB per hi or lo
-constexpr int kThreads = 512;             // 16 warps
-constexpr int kGenWarp0 = 8;              // warps 8..15 generate A
-constexpr int kEpiWarp0 = 4;              // warps 4..7 drain the accumulators
-constexpr uint32_t kSwizzle64 = 4;        // tcgen05 descriptor: 64-B swizzle
+constexpr int kThreads = 512;                   // 16 warps
+constexpr int kGenWarp0 = 8;                    // warps 8..15 generate A
+constexpr int kEpiWarp0 = 4;                    // warps 4..7 drain the accumulators
+constexpr int kGenWarps = kThreads / 32 - kGenWarp0;
+constexpr int kItemRing = 4;                    // work items in flight between roles
+constexpr int kItemConsumers = 1 + 4 + kGenWarps;  // MMA warp, epilogue warps, generator warps
+constexpr uint32_t kSwizzle64 = 4;              // tcgen05 descriptor: 64-B swizzle
 
 __host__ __device__ constexpr uint32_t swz64(uint32_t row, uint32_t chunk) {
   return (row >> 3) * 512u + (row & 7u) * 64u + ((chunk ^ ((row & 7u) >> 1)) << 4);
 }
 
-struct TcArgs {
-  // geometry
-  int n1, n2, n3, ti, tj, bi, bj, ntile_n, bn, stages, num_items;
-  int ti_shift;
-  int chunk_stages;     // stages accumulated per TMEM buffer before a drain
-  float scaling;
+// Geometry and table images of one field in the factorised form.
+struct TcField {
+  int n1, n2, n3;
+  int bi, bj, ntile_n, stages, chunk_stages;
   uint32_t idesc;
-  // workspace images
+  float scaling;
   const float2* rimg;   // [bi][stages][16][ti]
   const float2* simg;   // [bj][stages][16][tj]
   const uint8_t* cimg;  // [bn][stages][hi,lo][ntile_n * 64 B]
   float* field;
+};
+
+struct TcKernelArgs {
+  TcField f0;             // the field when `fields` is null
+  const TcField* fields;  // per-field descriptors of a batch
+  const int2* items;      // {field, local item}, longest first; null: field 0 in natural order
+  int num_items;
+  int* queue;             // work-queue counter, zero at launch
   int* status;
-  // shared-memory carve-up (bytes from the 1024-aligned base)
+  int ti, tj, ti_shift;   // row-tile shape (uniform over a launch)
   int nstage_buf;
   uint32_t stage_bytes, off_b, off_a, off_r, off_s, bars_off;
 };
 
-// ------------------------------------------------------------------ tables --
-struct TableArgs {
+// Per-field inputs of the table builders.
+struct TableJob {
   const float* table;  // nh x {v1,v2,v3,a,b}
   int nh, stages;
   double m[9], bar[3];
   double ds;
-  int off[3];          // coordinate of 0-based index t on axis a: (t + off[a]) * ds
+  int off[3];            // coordinate of 0-based index t on axis a: (t + off[a]) * ds
   int ax_r, ax_s, ax_c;  // physical axis of the row-fast, row-slow and column factors
   int n1, n2, n3, ti, tj, bi, bj, ntile_n, bn;
   float2* rimg;
@@ -69,7 +87,7 @@ struct TableArgs {
   uint8_t* cimg;
 };
 
-__device__ __forceinline__ void harmonic_k(const TableArgs& T, int h, double k[3], double& c, double& a,
+__device__ __forceinline__ void harmonic_k(const TableJob& T, int h, double k[3], double& c, double& a,
                                            double& b) {
   const float* r = T.table + 5 * static_cast<size_t>(h);
   const double v1 = r[0], v2 = r[1], v3 = r[2];
@@ -80,9 +98,10 @@ __device__ __forceinline__ void harmonic_k(const TableArgs& T, int h, double k[3
   b = r[4];
 }
 
-// R image (with the harmonic's complex amplitude and constant phase folded in)
-// and S image. One thread per entry.
-__global__ void tc_build_rs(const TableArgs T) {
+// R image (the harmonic's complex amplitude and constant phase folded in) and
+// S image; one thread per entry. blockIdx.y selects the field of a batch.
+__global__ void tc_build_rs(const TableJob j0, const TableJob* jobs) {
+  const TableJob& T = jobs ? jobs[blockIdx.y] : j0;
   const long long nr = static_cast<long long>(T.bi) * T.stages * kStageHarm * T.ti;
   const long long ns = static_cast<long long>(T.bj) * T.stages * kStageHarm * T.tj;
   for (long long e = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; e < nr + ns;
@@ -121,7 +140,8 @@ __global__ void tc_build_rs(const TableArgs T) {
 
 // Column image: per (column block, stage) a 64-B-swizzled K-major tile of
 // ntile_n rows x 32 fp16 ([cos, sin] of 16 harmonics), hi then lo.
-__global__ void tc_build_c(const TableArgs T) {
+__global__ void tc_build_c(const TableJob j0, const TableJob* jobs) {
+  const TableJob& T = jobs ? jobs[blockIdx.y] : j0;
   const long long nchunks = static_cast<long long>(T.bn) * T.stages * T.ntile_n * 4;
   for (long long e = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; e < nchunks;
        e += static_cast<long long>(gridDim.x) * blockDim.x) {
@@ -158,18 +178,44 @@ __global__ void tc_build_c(const TableArgs T) {
   }
 }
 
+// One work item: field descriptor and the tile's block coordinates.
+struct Item {
+  TcField f;
+  int ib, jb, nt;
+};
+
+__device__ __forceinline__ Item decode_item(const TcKernelArgs& A, int idx) {
+  Item it;
+  int fid = 0, local = idx;
+  if (A.items) {
+    const int2 e = A.items[idx];
+    fid = e.x;
+    local = e.y;
+  }
+  it.f = A.fields ? A.fields[fid] : A.f0;
+  const int tiles_m = it.f.bi * it.f.bj;
+  it.nt = local / tiles_m;
+  const int mt = local - it.nt * tiles_m;
+  it.ib = mt % it.f.bi;
+  it.jb = mt / it.f.bi;
+  return it;
+}
+
 // ------------------------------------------------------------- main kernel --
-__global__ void __launch_bounds__(kThreads, 1) srm_tc_kernel(const TcArgs A) {
+__global__ void __launch_bounds__(kThreads, 1) srm_tc_kernel(const TcKernelArgs A) {
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   const int S = A.nstage_buf;
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + A.bars_off);  // bulk copies landed
   uint64_t* agen = full + S;                                         // A tile generated
   uint64_t* empty = agen + S;                                        // stage consumed by MMA
-  uint64_t* accf = empty + S;                                        // accumulator ready [2]
-  uint64_t* acce = accf + 2;                                         // accumulator drained [2]
-  uint64_t* fin = acce + 2;                                          // MMA drain at exit
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(fin + 1);
+  uint64_t* accf = empty + S;                                        // chunk accumulated
+  uint64_t* acce = accf + 1;                                         // chunk drained
+  uint64_t* fin = acce + 1;                                          // MMA drain at exit
+  uint64_t* item_full = fin + 1;                                     // item slot written [kItemRing]
+  uint64_t* item_empty = item_full + kItemRing;                      // item slot read [kItemRing]
+  int* item_slot = reinterpret_cast<int*>(item_empty + kItemRing);   // [kItemRing]
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(item_slot + kItemRing);
 
   const int warp = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
@@ -177,14 +223,16 @@ __global__ void __launch_bounds__(kThreads, 1) srm_tc_kernel(const TcArgs A) {
   if (threadIdx.x == 0) {
     for (int s = 0; s < S; ++s) {
       mbar_init(&full[s], 1);
-      mbar_init(&agen[s], kThreads / 32 - kGenWarp0);
+      mbar_init(&agen[s], kGenWarps);
       mbar_init(&empty[s], 1);
     }
-    for (int b = 0; b < 2; ++b) {
-      mbar_init(&accf[b], 1);
-      mbar_init(&acce[b], 4);
-    }
+    mbar_init(accf, 1);
+    mbar_init(acce, 4);
     mbar_init(fin, 1);
+    for (int q = 0; q < kItemRing; ++q) {
+      mbar_init(&item_full[q], 1);
+      mbar_init(&item_empty[q], kItemConsumers);
+    }
     fence_mbar_init();
   }
   if (warp == 2) {
@@ -195,21 +243,44 @@ __global__ void __launch_bounds__(kThreads, 1) srm_tc_kernel(const TcArgs A) {
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem_base = *tmem_slot;
-
-  const int tiles_m = A.bi * A.bj;
   bool ok = true;
+
+  // Consumer side of the item ring: the next item index (or -1 when the
+  // queue is exhausted). Lane 0 of each consumer warp acknowledges the slot.
+  auto next_item = [&](uint32_t it, int& idx) -> bool {
+    const int q = it % kItemRing;
+    if (!mbar_wait_bounded(&item_full[q], (it / kItemRing) & 1, A.status)) return false;
+    idx = *reinterpret_cast<volatile int*>(&item_slot[q]);
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&item_empty[q]);
+    return true;
+  };
 
   if (warp == 0) {
     // ------------------------------------------------------ producer -------
     uint32_t cnt = 0;
     uint32_t last_cnt[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     bool used[8] = {false, false, false, false, false, false, false, false};
-    for (int item = blockIdx.x; item < A.num_items && ok; item += gridDim.x) {
-      const int nt = item / tiles_m;
-      const int mt = item - nt * tiles_m;
-      const int ib = mt % A.bi;
-      const int jb = mt / A.bi;
-      for (int k = 0; k < A.stages; ++k, ++cnt) {
+    for (uint32_t it = 0; ok; ++it) {
+      const int q = it % kItemRing;
+      if (!mbar_wait_bounded(&item_empty[q], ((it / kItemRing) & 1) ^ 1, A.status)) {
+        ok = false;
+        break;
+      }
+      int idx = 0;
+      if (lane == 0) {
+        idx = atomicAdd(A.queue, 1);
+        if (idx >= A.num_items) idx = -1;
+        item_slot[q] = idx;
+        mbar_arrive(&item_full[q]);  // release: the slot write is visible to waiters
+      }
+      idx = __shfl_sync(0xffffffffu, idx, 0);
+      if (idx < 0) break;
+      const Item w = decode_item(A, idx);
+      const uint32_t bbytes = 2u * w.f.ntile_n * kRowBytes;
+      const uint32_t rbytes = kStageHarm * A.ti * 8u;
+      const uint32_t sbytes = kStageHarm * A.tj * 8u;
+      for (int k = 0; k < w.f.stages; ++k, ++cnt) {
         const int s = cnt % S;
         const uint32_t ph = (cnt / S) & 1;
         if (!mbar_wait_bounded(&empty[s], ph ^ 1, A.status)) {
@@ -218,14 +289,12 @@ __global__ void __launch_bounds__(kThreads, 1) srm_tc_kernel(const TcArgs A) {
         }
         if (lane == 0) {
           uint8_t* st = smem + s * A.stage_bytes;
-          const uint32_t bbytes = 2u * A.ntile_n * kRowBytes;
-          const uint32_t rbytes = kStageHarm * A.ti * 8u;
-          const uint32_t sbytes = kStageHarm * A.tj * 8u;
           mbar_arrive_expect_tx(&full[s], bbytes + rbytes + sbytes);
-          bulk_g2s(st + A.off_b, A.cimg + (static_cast<size_t>(nt) * A.stages + k) * bbytes, bbytes, &full[s]);
-          bulk_g2s(st + A.off_r, A.rimg + (static_cast<size_t>(ib) * A.stages + k) * kStageHarm * A.ti, rbytes,
+          bulk_g2s(st + A.off_b, w.f.cimg + (static_cast<size_t>(w.nt) * w.f.stages + k) * bbytes, bbytes,
                    &full[s]);
-          bulk_g2s(st + A.off_s, A.simg + (static_cast<size_t>(jb) * A.stages + k) * kStageHarm * A.tj, sbytes,
+          bulk_g2s(st + A.off_r, w.f.rimg + (static_cast<size_t>(w.ib) * w.f.stages + k) * kStageHarm * A.ti, rbytes,
+                   &full[s]);
+          bulk_g2s(st + A.off_s, w.f.simg + (static_cast<size_t>(w.jb) * w.f.stages + k) * kStageHarm * A.tj, sbytes,
                    &full[s]);
         }
         last_cnt[s] = cnt;
@@ -240,7 +309,7 @@ __global__ void __launch_bounds__(kThreads, 1) srm_tc_kernel(const TcArgs A) {
     }
   } else if (warp == 1) {
     // ------------------------------------------------------- MMA issuer ----
-    // The K loop of an item runs in chunks of A.chunk_stages stages, each
+    // The K loop of an item runs in chunks of chunk_stages stages, each
     // accumulated from zero in the TMEM chunk buffer (columns 0..255). At the
     // end of a chunk the epilogue adds the buffer into an FP32 master
     // accumulator held in TMEM columns 256..511 (round to nearest), or, for
@@ -249,16 +318,22 @@ __global__ void __launch_bounds__(kThreads, 1) srm_tc_kernel(const TcArgs A) {
     // the number of accumulation steps into one buffer; chunking bounds it.
     uint32_t cnt = 0, chunk = 0;
     bool issued_any = false;
-    for (int item = blockIdx.x; item < A.num_items && ok; item += gridDim.x) {
-      for (int c0 = 0; c0 < A.stages && ok; c0 += A.chunk_stages, ++chunk) {
-        const int c1 = min(A.stages, c0 + A.chunk_stages);
+    for (uint32_t it = 0; ok; ++it) {
+      int idx;
+      if (!next_item(it, idx)) {
+        ok = false;
+        break;
+      }
+      if (idx < 0) break;
+      const Item w = decode_item(A, idx);
+      for (int c0 = 0; c0 < w.f.stages && ok; c0 += w.f.chunk_stages, ++chunk) {
+        const int c1 = min(w.f.stages, c0 + w.f.chunk_stages);
         // The previous chunk must be drained before the buffer restarts.
         if (chunk > 0 && !mbar_wait_bounded(acce, (chunk - 1) & 1, A.status)) {
           ok = false;
           break;
         }
         tc_fence_after();
-        const uint32_t d_tmem = tmem_base;
         for (int k = c0; k < c1; ++k, ++cnt) {
           const int s = cnt % S;
           const uint32_t ph = (cnt / S) & 1;
@@ -270,16 +345,16 @@ __global__ void __launch_bounds__(kThreads, 1) srm_tc_kernel(const TcArgs A) {
           if (lane == 0) {
             const uint32_t st = smem_u32(smem + s * A.stage_bytes);
             const uint32_t a_hi = st + A.off_a, a_lo = a_hi + kATileBytes;
-            const uint32_t b_hi = st + A.off_b, b_lo = b_hi + A.ntile_n * kRowBytes;
+            const uint32_t b_hi = st + A.off_b, b_lo = b_hi + w.f.ntile_n * kRowBytes;
 #pragma unroll
             for (int kk = 0; kk < 2; ++kk) {
               const uint64_t dah = umma_smem_desc(a_hi + 32 * kk, 16, 512, kSwizzle64);
               const uint64_t dal = umma_smem_desc(a_lo + 32 * kk, 16, 512, kSwizzle64);
               const uint64_t dbh = umma_smem_desc(b_hi + 32 * kk, 16, 512, kSwizzle64);
               const uint64_t dbl = umma_smem_desc(b_lo + 32 * kk, 16, 512, kSwizzle64);
-              umma_f16(d_tmem, dah, dbh, A.idesc, (k > c0 || kk > 0) ? 1u : 0u);
-              umma_f16(d_tmem, dah, dbl, A.idesc, 1u);
-              umma_f16(d_tmem, dal, dbh, A.idesc, 1u);
+              umma_f16(tmem_base, dah, dbh, w.f.idesc, (k > c0 || kk > 0) ? 1u : 0u);
+              umma_f16(tmem_base, dah, dbl, w.f.idesc, 1u);
+              umma_f16(tmem_base, dal, dbh, w.f.idesc, 1u);
             }
             umma_commit(&empty[s]);
             issued_any = true;
@@ -305,24 +380,29 @@ __global__ void __launch_bounds__(kThreads, 1) srm_tc_kernel(const TcArgs A) {
     const int jj = r >> A.ti_shift;
     const uint32_t lane_base = tmem_base + (static_cast<uint32_t>(q * 32) << 16);
     uint32_t chunk = 0;
-    for (int item = blockIdx.x; item < A.num_items && ok; item += gridDim.x) {
-      const int nt = item / tiles_m;
-      const int mt = item - nt * tiles_m;
-      const int i = (mt % A.bi) * A.ti + ii;
-      const int j = (mt / A.bi) * A.tj + jj;
-      const bool row_ok = (i < A.n1) && (j < A.n2);
-      const long long plane = static_cast<long long>(A.n1) * A.n2;
-      float* dst = A.field + i + static_cast<long long>(A.n1) * j;
-      const int k0 = nt * A.ntile_n;
-      for (int s0 = 0; s0 < A.stages; s0 += A.chunk_stages, ++chunk) {
+    for (uint32_t it = 0; ok; ++it) {
+      int idx;
+      if (!next_item(it, idx)) {
+        ok = false;
+        break;
+      }
+      if (idx < 0) break;
+      const Item w = decode_item(A, idx);
+      const int i = w.ib * A.ti + ii;
+      const int j = w.jb * A.tj + jj;
+      const bool row_ok = (i < w.f.n1) && (j < w.f.n2);
+      const long long plane = static_cast<long long>(w.f.n1) * w.f.n2;
+      float* dst = w.f.field + i + static_cast<long long>(w.f.n1) * j;
+      const int k0 = w.nt * w.f.ntile_n;
+      for (int s0 = 0; s0 < w.f.stages; s0 += w.f.chunk_stages, ++chunk) {
         const bool first = (s0 == 0);
-        const bool last = (s0 + A.chunk_stages >= A.stages);
+        const bool last = (s0 + w.f.chunk_stages >= w.f.stages);
         if (!mbar_wait_bounded(accf, chunk & 1, A.status)) {
           ok = false;
           break;
         }
         tc_fence_after();
-        for (int c0 = 0; c0 < A.ntile_n; c0 += 32) {
+        for (int c0 = 0; c0 < w.f.ntile_n; c0 += 32) {
           uint32_t v[32];
           tmem_ld_32x32b_x32(lane_base + c0, v);
           if (!first) {
@@ -331,7 +411,8 @@ __global__ void __launch_bounds__(kThreads, 1) srm_tc_kernel(const TcArgs A) {
             tmem_ld_32x32b_x32(lane_base + 256 + c0, m);
             tmem_wait_ld();
 #pragma unroll
-            for (int c = 0; c < 32; ++c) v[c] = __float_as_uint(__fadd_rn(__uint_as_float(m[c]), __uint_as_float(v[c])));
+            for (int c = 0; c < 32; ++c)
+              v[c] = __float_as_uint(__fadd_rn(__uint_as_float(m[c]), __uint_as_float(v[c])));
           } else {
             tmem_wait_ld();
           }
@@ -342,7 +423,8 @@ __global__ void __launch_bounds__(kThreads, 1) srm_tc_kernel(const TcArgs A) {
 #pragma unroll
             for (int c = 0; c < 32; ++c) {
               const int kcol = k0 + c0 + c;
-              if (c0 + c < A.ntile_n && kcol < A.n3) dst[plane * kcol] = __fmul_rn(__uint_as_float(v[c]), A.scaling);
+              if (c0 + c < w.f.ntile_n && kcol < w.f.n3)
+                dst[plane * kcol] = __fmul_rn(__uint_as_float(v[c]), w.f.scaling);
             }
           }
         }
@@ -360,8 +442,15 @@ __global__ void __launch_bounds__(kThreads, 1) srm_tc_kernel(const TcArgs A) {
     const int ii = r & (A.ti - 1);
     const int jj = r >> A.ti_shift;
     uint32_t cnt = 0;
-    for (int item = blockIdx.x; item < A.num_items && ok; item += gridDim.x) {
-      for (int k = 0; k < A.stages; ++k, ++cnt) {
+    for (uint32_t it = 0; ok; ++it) {
+      int idx;
+      if (!next_item(it, idx)) {
+        ok = false;
+        break;
+      }
+      if (idx < 0) break;
+      const int stages = (A.fields ? A.fields[A.items ? A.items[idx].x : 0] : A.f0).stages;
+      for (int k = 0; k < stages; ++k, ++cnt) {
         const int s = cnt % S;
         const uint32_t ph = (cnt / S) & 1;
         if (!mbar_wait_bounded(&full[s], ph, A.status)) {
@@ -418,55 +507,10 @@ int ilog2(int v) {
 constexpr int kDefaultChunkStages = 32;
 int g_chunk_stages = kDefaultChunkStages;
 
-}  // namespace
-
-void tc_set_chunk_harmonics(int harmonics) {
-  g_chunk_stages = harmonics > 0 ? (harmonics + kStageHarm - 1) / kStageHarm : kDefaultChunkStages;
-}
-
-bool tc_make_plan(int ndim, const int n[3], int nh, TcPlan* P) {
-  if (nh <= 0 || n[0] <= 0 || n[1] <= 0 || n[2] <= 0) return false;
-  TcPlan p{};
-  p.n1 = n[0];
-  if (ndim == 3) {
-    p.n2 = n[1];
-    p.n3 = n[2];
-  } else {
-    p.n2 = n[2];  // the single z plane
-    p.n3 = n[1];
-  }
-  p.tj = 1;
-  while (p.tj < 8 && p.tj * 2 <= p.n2) p.tj *= 2;
-  p.ti = kRows / p.tj;
-  p.bi = (p.n1 + p.ti - 1) / p.ti;
-  p.bj = (p.n2 + p.tj - 1) / p.tj;
-  const int n3_16 = (p.n3 + 15) / 16 * 16;
-  p.bn = (n3_16 + 255) / 256;
-  p.ntile_n = ((p.n3 + p.bn - 1) / p.bn + 15) / 16 * 16;
-  p.nh = nh;
-  p.nh_pad = (nh + kStageHarm - 1) / kStageHarm * kStageHarm;
-  p.stages = p.nh_pad / kStageHarm;
-  p.chunk_stages = g_chunk_stages;
-  auto align = [](size_t v) { return (v + 255) / 256 * 256; };
-  size_t off = 0;
-  p.off_r = off;
-  off = align(off + static_cast<size_t>(p.bi) * p.stages * kStageHarm * p.ti * sizeof(float2));
-  p.off_s = off;
-  off = align(off + static_cast<size_t>(p.bj) * p.stages * kStageHarm * p.tj * sizeof(float2));
-  p.off_c = off;
-  off = align(off + static_cast<size_t>(p.bn) * p.stages * 2 * p.ntile_n * kRowBytes);
-  p.off_status = off;
-  off = align(off + 256);
-  p.bytes = off;
-  *P = p;
-  return true;
-}
-
-cudaError_t launch_tc_structured(const scarf_srm_setup& s, const int fs[3], const int n[3], float ds,
-                                 const float* d_table, int nh, float* d_field, void* d_work, const TcPlan& p,
-                                 int* d_status, cudaStream_t stream, cudaEvent_t ev_main0, cudaEvent_t ev_main1) {
+TableJob make_job(const scarf_srm_setup& s, const int fs[3], float ds, const float* d_table, int nh,
+                  const TcPlan& p, void* d_work) {
   uint8_t* work = static_cast<uint8_t*>(d_work);
-  TableArgs T{};
+  TableJob T{};
   T.table = d_table;
   T.nh = nh;
   T.stages = p.stages;
@@ -489,56 +533,239 @@ cudaError_t launch_tc_structured(const scarf_srm_setup& s, const int fs[3], cons
   T.rimg = reinterpret_cast<float2*>(work + p.off_r);
   T.simg = reinterpret_cast<float2*>(work + p.off_s);
   T.cimg = work + p.off_c;
+  return T;
+}
 
-  int dev = 0, nsm = 148;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-  tc_build_rs<<<nsm * 8, 256, 0, stream>>>(T);
-  tc_build_c<<<nsm * 8, 256, 0, stream>>>(T);
-  cudaError_t le = cudaGetLastError();
-  if (le != cudaSuccess) return le;
-  if (ev_main0) cudaEventRecord(ev_main0, stream);
+TcField make_field(const scarf_srm_setup& s, const TcPlan& p, const TableJob& T, float* d_field) {
+  TcField f{};
+  f.n1 = p.n1;
+  f.n2 = p.n2;
+  f.n3 = p.n3;
+  f.bi = p.bi;
+  f.bj = p.bj;
+  f.ntile_n = p.ntile_n;
+  f.stages = p.stages;
+  f.chunk_stages = std::max(1, p.chunk_stages);
+  f.idesc = umma_idesc_f16_f32(kRows, static_cast<uint32_t>(p.ntile_n));
+  f.scaling = s.scaling;
+  f.rimg = T.rimg;
+  f.simg = T.simg;
+  f.cimg = T.cimg;
+  f.field = d_field;
+  return f;
+}
 
-  TcArgs A{};
-  A.n1 = p.n1;
-  A.n2 = p.n2;
-  A.n3 = p.n3;
-  A.ti = p.ti;
-  A.tj = p.tj;
-  A.bi = p.bi;
-  A.bj = p.bj;
-  A.ntile_n = p.ntile_n;
-  A.bn = p.bn;
-  A.stages = p.stages;
-  A.num_items = p.bi * p.bj * p.bn;
-  A.ti_shift = ilog2(p.ti);
-  A.chunk_stages = std::max(1, p.chunk_stages);
-  A.scaling = s.scaling;
-  A.idesc = umma_idesc_f16_f32(kRows, static_cast<uint32_t>(p.ntile_n));
-  A.rimg = T.rimg;
-  A.simg = T.simg;
-  A.cimg = T.cimg;
-  A.field = d_field;
-  A.status = d_status;
-  // Shared memory per stage: B hi+lo, A hi+lo (1024-aligned), R and S tiles.
-  const uint32_t b_bytes = 2u * p.ntile_n * kRowBytes;
+constexpr int kMaxDynSmem = 227 * 1024;
+
+// Shared-memory carve-up for a launch with row tiles ti x tj and column
+// tiles up to ntile_max; returns the dynamic shared-memory size (0 if the
+// ring cannot hold two stages).
+size_t compute_layout(TcKernelArgs& A, int ti, int tj, int ntile_max) {
+  A.ti = ti;
+  A.tj = tj;
+  A.ti_shift = ilog2(ti);
+  const uint32_t b_bytes = 2u * ntile_max * kRowBytes;
   A.off_b = 0;
   A.off_a = (b_bytes + 1023u) & ~1023u;
   A.off_r = A.off_a + 2u * kATileBytes;
-  A.off_s = A.off_r + kStageHarm * p.ti * 8u;
-  A.stage_bytes = (A.off_s + kStageHarm * p.tj * 8u + 1023u) & ~1023u;
-  const uint32_t budget = 227u * 1024u - 1024u - 256u;
-  int nbuf = static_cast<int>(budget / A.stage_bytes);
-  nbuf = std::min(nbuf, 8);
-  if (nbuf < 2) return cudaErrorInvalidConfiguration;
+  A.off_s = A.off_r + kStageHarm * ti * 8u;
+  A.stage_bytes = (A.off_s + kStageHarm * tj * 8u + 1023u) & ~1023u;
+  const uint32_t budget = kMaxDynSmem - 1024u - 512u;
+  const int nbuf = std::min(8, static_cast<int>(budget / A.stage_bytes));
+  if (nbuf < 2) return 0;
   A.nstage_buf = nbuf;
   A.bars_off = nbuf * A.stage_bytes;
-  const size_t smem = 1024 + A.bars_off + (3 * nbuf + 5) * 8 + 16;
-  cudaError_t e = cudaFuncSetAttribute(srm_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       static_cast<int>(smem));
+  return 1024 + A.bars_off + (3 * nbuf + 3 + 2 * kItemRing) * 8 + kItemRing * 4 + 16;
+}
+
+// The kernel's dynamic shared-memory limit, raised once per device so that
+// launches themselves make no attribute calls.
+cudaError_t ensure_smem_attribute() {
+  static bool done[64] = {};
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
-  const int grid = std::min(A.num_items, nsm);
-  srm_tc_kernel<<<grid, kThreads, smem, stream>>>(A);
+  if (dev >= 0 && dev < 64 && done[dev]) return cudaSuccess;
+  e = cudaFuncSetAttribute(srm_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
+  if (e == cudaSuccess && dev >= 0 && dev < 64) done[dev] = true;
+  return e;
+}
+
+int device_sms() {
+  int dev = 0, nsm = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  return nsm;
+}
+
+}  // namespace
+
+void tc_set_chunk_harmonics(int harmonics) {
+  g_chunk_stages = harmonics > 0 ? (harmonics + kStageHarm - 1) / kStageHarm : kDefaultChunkStages;
+}
+
+bool tc_make_plan(int ndim, const int n[3], int nh, TcPlan* P, int tj_force) {
+  if (nh <= 0 || n[0] <= 0 || n[1] <= 0 || n[2] <= 0) return false;
+  TcPlan p{};
+  p.n1 = n[0];
+  if (ndim == 3) {
+    p.n2 = n[1];
+    p.n3 = n[2];
+  } else {
+    p.n2 = n[2];  // the single z plane
+    p.n3 = n[1];
+  }
+  if (tj_force > 0) {
+    if (tj_force > kRows || (tj_force & (tj_force - 1))) return false;
+    p.tj = tj_force;
+  } else {
+    p.tj = 1;
+    while (p.tj < 8 && p.tj * 2 <= p.n2) p.tj *= 2;
+  }
+  p.ti = kRows / p.tj;
+  p.bi = (p.n1 + p.ti - 1) / p.ti;
+  p.bj = (p.n2 + p.tj - 1) / p.tj;
+  const int n3_16 = (p.n3 + 15) / 16 * 16;
+  p.bn = (n3_16 + 255) / 256;
+  p.ntile_n = ((p.n3 + p.bn - 1) / p.bn + 15) / 16 * 16;
+  p.nh = nh;
+  p.nh_pad = (nh + kStageHarm - 1) / kStageHarm * kStageHarm;
+  p.stages = p.nh_pad / kStageHarm;
+  p.chunk_stages = g_chunk_stages;
+  auto align = [](size_t v) { return (v + 255) / 256 * 256; };
+  size_t off = 0;
+  p.off_r = off;
+  off = align(off + static_cast<size_t>(p.bi) * p.stages * kStageHarm * p.ti * sizeof(float2));
+  p.off_s = off;
+  off = align(off + static_cast<size_t>(p.bj) * p.stages * kStageHarm * p.tj * sizeof(float2));
+  p.off_c = off;
+  off = align(off + static_cast<size_t>(p.bn) * p.stages * 2 * p.ntile_n * kRowBytes);
+  p.off_status = off;  // status word, then the work-queue counter
+  off = align(off + 256);
+  p.bytes = off;
+  *P = p;
+  return true;
+}
+
+cudaError_t launch_tc_structured(const scarf_srm_setup& s, const int fs[3], const int n[3], float ds,
+                                 const float* d_table, int nh, float* d_field, void* d_work, const TcPlan& p,
+                                 int* d_status, cudaStream_t stream, cudaEvent_t ev_main0, cudaEvent_t ev_main1) {
+  const TableJob T = make_job(s, fs, ds, d_table, nh, p, d_work);
+  const int nsm = device_sms();
+  tc_build_rs<<<nsm * 8, 256, 0, stream>>>(T, nullptr);
+  tc_build_c<<<nsm * 8, 256, 0, stream>>>(T, nullptr);
+  cudaError_t le = cudaGetLastError();
+  if (le != cudaSuccess) return le;
+
+  TcKernelArgs A{};
+  A.f0 = make_field(s, p, T, d_field);
+  A.fields = nullptr;
+  A.items = nullptr;
+  A.num_items = p.bi * p.bj * p.bn;
+  A.status = d_status;
+  A.queue = d_status + 1;
+  const size_t smem = compute_layout(A, p.ti, p.tj, p.ntile_n);
+  if (!smem) return cudaErrorInvalidConfiguration;
+  cudaError_t e = ensure_smem_attribute();
+  if (e != cudaSuccess) return e;
+  e = cudaMemsetAsync(A.queue, 0, sizeof(int), stream);
+  if (e != cudaSuccess) return e;
+  if (ev_main0) cudaEventRecord(ev_main0, stream);
+  srm_tc_kernel<<<std::min(A.num_items, nsm), kThreads, smem, stream>>>(A);
+  if (ev_main1) cudaEventRecord(ev_main1, stream);
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------- batches --
+size_t tc_batch_plan(const TcBatchInput* in, int nfields, TcBatchPlan* out) {
+  TcBatchPlan bp;
+  bp.nfields = nfields;
+  auto align = [](size_t v) { return (v + 255) / 256 * 256; };
+  size_t off = 0;
+  bp.off_fields = off;
+  off = align(off + sizeof(TcField) * nfields);
+  bp.off_jobs = off;
+  off = align(off + sizeof(TableJob) * nfields);
+  long long items = 0;
+  int ti = 0, tj = 0, ntile_max = 16;
+  for (int f = 0; f < nfields; ++f) {
+    TcPlan p{};
+    if (!tc_make_plan(in[f].s->ndim, in[f].n, in[f].nh, &p, in[f].tj)) return 0;
+    if (f == 0) {
+      ti = p.ti;
+      tj = p.tj;
+    } else if (p.ti != ti || p.tj != tj) {
+      return 0;  // one row-tile shape per launch
+    }
+    ntile_max = std::max(ntile_max, p.ntile_n);
+    items += static_cast<long long>(p.bi) * p.bj * p.bn;
+    bp.field_off.push_back(off);
+    bp.plans.push_back(p);
+    off = align(off + p.bytes);
+  }
+  bp.ti = ti;
+  bp.tj = tj;
+  bp.ntile_max = ntile_max;
+  bp.num_items = static_cast<int>(items);
+  bp.off_items = off;
+  off = align(off + sizeof(int2) * static_cast<size_t>(items));
+  bp.off_status = off;
+  off = align(off + 256);
+  bp.bytes = off;
+  if (out) *out = bp;
+  return bp.bytes;
+}
+
+cudaError_t tc_batch_upload(const TcBatchInput* in, const TcBatchPlan& bp, void* d_work) {
+  uint8_t* work = static_cast<uint8_t*>(d_work);
+  std::vector<TcField> fields(bp.nfields);
+  std::vector<TableJob> jobs(bp.nfields);
+  std::vector<int2> items;
+  items.reserve(bp.num_items);
+  for (int f = 0; f < bp.nfields; ++f) {
+    jobs[f] = make_job(*in[f].s, in[f].fs, in[f].ds, in[f].d_table, in[f].nh, bp.plans[f], work + bp.field_off[f]);
+    fields[f] = make_field(*in[f].s, bp.plans[f], jobs[f], in[f].d_field);
+    const int nit = bp.plans[f].bi * bp.plans[f].bj * bp.plans[f].bn;
+    for (int l = 0; l < nit; ++l) items.push_back(make_int2(f, l));
+  }
+  // Longest items first (the dynamic queue then balances the tail).
+  std::stable_sort(items.begin(), items.end(),
+                   [&](const int2& a, const int2& b) { return bp.plans[a.x].stages > bp.plans[b.x].stages; });
+  cudaError_t e = cudaMemcpy(work + bp.off_fields, fields.data(), sizeof(TcField) * bp.nfields,
+                             cudaMemcpyHostToDevice);
+  if (e == cudaSuccess)
+    e = cudaMemcpy(work + bp.off_jobs, jobs.data(), sizeof(TableJob) * bp.nfields, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess)
+    e = cudaMemcpy(work + bp.off_items, items.data(), sizeof(int2) * items.size(), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = ensure_smem_attribute();
+  return e;
+}
+
+cudaError_t tc_batch_launch(const TcBatchPlan& bp, void* d_work, cudaStream_t stream, cudaEvent_t ev_main0,
+                            cudaEvent_t ev_main1) {
+  uint8_t* work = static_cast<uint8_t*>(d_work);
+  const int nsm = device_sms();
+  const TableJob* jobs = reinterpret_cast<const TableJob*>(work + bp.off_jobs);
+  const int gx = std::max(1, std::min(64, nsm * 8 / std::max(1, bp.nfields)));
+  dim3 grid(gx, bp.nfields);
+  TableJob none{};
+  int* status = reinterpret_cast<int*>(work + bp.off_status);
+  cudaError_t e = cudaMemsetAsync(status, 0, 2 * sizeof(int), stream);
+  if (e != cudaSuccess) return e;
+  tc_build_rs<<<grid, 256, 0, stream>>>(none, jobs);
+  tc_build_c<<<grid, 256, 0, stream>>>(none, jobs);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  TcKernelArgs A{};
+  A.fields = reinterpret_cast<const TcField*>(work + bp.off_fields);
+  A.items = reinterpret_cast<const int2*>(work + bp.off_items);
+  A.num_items = bp.num_items;
+  A.status = status;
+  A.queue = status + 1;
+  const size_t smem = compute_layout(A, bp.ti, bp.tj, bp.ntile_max);
+  if (!smem) return cudaErrorInvalidConfiguration;
+  if (ev_main0) cudaEventRecord(ev_main0, stream);
+  srm_tc_kernel<<<std::min(bp.num_items, nsm), kThreads, smem, stream>>>(A);
   if (ev_main1) cudaEventRecord(ev_main1, stream);
   return cudaGetLastError();
 }
