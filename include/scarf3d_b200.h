@@ -98,6 +98,24 @@ int scarf_srm_compute_setup(const scarf_srm_params *p, scarf_srm_setup *s);
 int scarf_srm_sample(const scarf_srm_params *p, const scarf_srm_setup *s, float *table, int *n_kept,
                      long long *pairs_used);
 
+/* The same table as scarf_srm_sample (built-in generator), with the rejection
+ * tests of the sampling loop (scarflib_srm.f90:731-745) evaluated on the
+ * current GPU; the host walks the accepted pairs and decides the pairs whose
+ * test lies within float rounding of its threshold, so the table is bit-
+ * identical to the host loop's. *host_decided receives that pair count. */
+int scarf_srm_sample_device(const scarf_srm_params *p, const scarf_srm_setup *s, float *table, int *n_kept,
+                            long long *pairs_used, long long *host_decided, void *stream);
+
+/* Where scarf_execute draws its harmonics: SCARF_SAMPLER_AUTO (device,
+ * unless a uniform source was installed), _HOST or _DEVICE. */
+#define SCARF_SAMPLER_AUTO 0
+#define SCARF_SAMPLER_HOST 1
+#define SCARF_SAMPLER_DEVICE 2
+int scarf_set_sampler(int where);
+/* Upper bound on the uniform pairs one device pass tests (0 = sized from the
+ * acceptance rate); further passes are chained as needed. */
+int scarf_set_sampler_pass_pairs(long long pairs);
+
 /* FP32 direct sum, structured block: field[i + n0*(j + n1*k)] for the grid
  * x = (i + fs[0] - 1) * ds (0-based i), likewise y, z; scaled by s->scaling.
  * d_table: nh rows of 5 floats on the device. */

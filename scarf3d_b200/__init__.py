@@ -35,7 +35,9 @@ EXPORTED_SYMBOLS = (
     "scarf_last_error", "scarf_set_nharm", "scarf_get_nharm", "scarf_set_form",
     "scarf_set_uniform_source", "scarf_set_stream", "scarf_set_host_threads", "scarf_set_kernel_timing",
     "scarf_last_kernel_ms", "scarf_set_tc_chunk", "scarf_execute_ex",
-    "scarf_srm_compute_setup", "scarf_srm_sample", "scarf_srm_direct_structured",
+    "scarf_srm_compute_setup", "scarf_srm_sample", "scarf_srm_sample_device", "scarf_set_sampler",
+    "scarf_set_sampler_pass_pairs",
+    "scarf_srm_direct_structured",
     "scarf_srm_direct_points", "scarf_srm_tc_workspace_bytes", "scarf_srm_tc_structured",
     "scarf_srm_tc_noalloc_capacity_bytes", "scarf_srm_tc_structured_noalloc",
     "scarf_srm_tc_batch_workspace_bytes", "scarf_srm_tc_batch_create", "scarf_srm_tc_batch_launch",
@@ -116,6 +118,10 @@ def _load() -> ctypes.CDLL:
         "scarf_srm_compute_setup": (c_int, [ctypes.POINTER(SrmParams), ctypes.POINTER(SrmSetup)]),
         "scarf_srm_sample": (c_int, [ctypes.POINTER(SrmParams), ctypes.POINTER(SrmSetup), c_void_p, ip,
                                      ctypes.POINTER(c_ll)]),
+        "scarf_srm_sample_device": (c_int, [ctypes.POINTER(SrmParams), ctypes.POINTER(SrmSetup), c_void_p, ip,
+                                            ctypes.POINTER(c_ll), ctypes.POINTER(c_ll), c_void_p]),
+        "scarf_set_sampler": (c_int, [c_int]),
+        "scarf_set_sampler_pass_pairs": (c_int, [c_ll]),
         "scarf_srm_direct_structured": (c_int, [ctypes.POINTER(SrmSetup), ip, ip, c_float, c_void_p, c_int,
                                                 c_void_p, c_void_p]),
         "scarf_srm_direct_points": (c_int, [ctypes.POINTER(SrmSetup), c_void_p, c_void_p, c_void_p, c_ll,
@@ -305,6 +311,25 @@ def sample(p: SrmParams, s: SrmSetup) -> tuple[np.ndarray, int]:
     check(lib.scarf_srm_sample(ctypes.byref(p), ctypes.byref(s), tab.ctypes.data_as(ctypes.c_void_p),
                                ctypes.byref(kept), ctypes.byref(used)))
     return tab[: kept.value].copy(), used.value
+
+
+SAMPLER_AUTO, SAMPLER_HOST, SAMPLER_DEVICE = 0, 1, 2
+
+
+def sample_device(p: SrmParams, s: SrmSetup, stream_handle: int | None = None):
+    """Device-assisted sampler: (table, pairs used, pairs decided on the host)."""
+    tab = np.zeros((max(p.nharm, 1), 5), np.float32)
+    kept = ctypes.c_int()
+    used = ctypes.c_longlong()
+    open_ = ctypes.c_longlong()
+    check(lib.scarf_srm_sample_device(ctypes.byref(p), ctypes.byref(s), tab.ctypes.data_as(ctypes.c_void_p),
+                                      ctypes.byref(kept), ctypes.byref(used), ctypes.byref(open_),
+                                      ctypes.c_void_p(stream_handle or 0)))
+    return tab[: kept.value].copy(), used.value, open_.value
+
+
+def set_sampler(where: int):
+    check(lib.scarf_set_sampler(int(where)))
 
 
 def set_nharm(n: int):

@@ -53,6 +53,7 @@ struct Config {
   UniformSource src;
   cudaStream_t stream = nullptr;
   int threads = 0;
+  int sampler = SCARF_SAMPLER_AUTO;
   bool kernel_timing = false;
 };
 Config g_cfg;
@@ -208,7 +209,10 @@ int execute_impl(int seed, float* field, float stats[8], int flags) {
   std::vector<float> table(5 * static_cast<size_t>(p.nharm));
   const int threads = g_cfg.threads > 0 ? g_cfg.threads : host_threads();
   long long pairs = 0;
-  const int nh = srm_sample(p, s, &g_cfg.src, threads, table.data(), &pairs);
+  const bool on_gpu = !g_cfg.src.srng && g_cfg.sampler != SCARF_SAMPLER_HOST;
+  const int nh = on_gpu ? srm_sample_device(p, s, table.data(), &pairs, st, nullptr)
+                        : srm_sample(p, s, &g_cfg.src, threads, table.data(), &pairs);
+  if (nh == -2) return fail(SCARF_ERR_CUDA, "device sampler: CUDA error");
   if (nh < 0)
     return fail(SCARF_ERR_ARG,
                 "rejection sampling infeasible: acceptance rate %.3g < %.1g (domain too small for the correlation "
@@ -589,6 +593,34 @@ int scarf_srm_compute_setup(const scarf_srm_params* p, scarf_srm_setup* s) {
   if (!p || !s) return fail(SCARF_ERR_ARG, "NULL argument");
   const int rc = srm_setup(*p, s);
   if (rc) return fail(rc, "invalid SRM parameters");
+  return SCARF_OK;
+}
+
+int scarf_set_sampler(int where) {
+  if (where < SCARF_SAMPLER_AUTO || where > SCARF_SAMPLER_DEVICE) return fail(SCARF_ERR_ARG, "unknown sampler");
+  std::lock_guard<std::mutex> lk(g_mu);
+  g_cfg.sampler = where;
+  return SCARF_OK;
+}
+
+int scarf_set_sampler_pass_pairs(long long pairs) {
+  if (pairs < 0) return fail(SCARF_ERR_ARG, "pairs must be >= 0");
+  set_device_sampler_pass_cap(pairs);
+  return SCARF_OK;
+}
+
+int scarf_srm_sample_device(const scarf_srm_params* p, const scarf_srm_setup* s, float* table, int* n_kept,
+                            long long* pairs_used, long long* host_decided, void* stream) {
+  if (!p || !s || !table) return fail(SCARF_ERR_ARG, "NULL argument");
+  long long used = 0, open = 0;
+  const int kept = srm_sample_device(*p, *s, table, &used, stream, &open);
+  if (kept == -1)
+    return fail(SCARF_ERR_ARG, "rejection sampling infeasible: acceptance rate %.3g < %.1g", acceptance_rate(*s),
+                kMinAcceptance);
+  if (kept < 0) return fail(SCARF_ERR_CUDA, "device sampler: CUDA error");
+  if (n_kept) *n_kept = kept;
+  if (pairs_used) *pairs_used = used;
+  if (host_decided) *host_decided = open;
   return SCARF_OK;
 }
 

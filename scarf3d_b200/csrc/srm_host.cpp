@@ -3,6 +3,8 @@
 // operation rounds exactly as the reference's Fortran statement does.
 #include "srm_host.h"
 
+#include <cuda_runtime.h>
+
 #include <algorithm>
 #include <atomic>
 #include <cmath>
@@ -11,6 +13,8 @@
 #include <mutex>
 #include <thread>
 #include <vector>
+
+#include "srm_kernels.h"
 
 namespace scarf {
 
@@ -367,6 +371,174 @@ double acceptance_rate(const scarf_srm_setup& s) {
   const double width = static_cast<double>(s.kmax) - static_cast<double>(s.kmin);
   if (!(width > 0.0)) return 0.0;
   return static_cast<double>(s.intg_band) * s.cnst / width;
+}
+
+// ------------------------------------------------- device-assisted sampler --
+namespace {
+
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  cudaError_t ensure(size_t need) {
+    if (need <= bytes) return cudaSuccess;
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+    const cudaError_t e = cudaMalloc(&p, need);
+    if (e == cudaSuccess) bytes = need;
+    return e;
+  }
+};
+
+struct DeviceSamplerState {
+  int device = -1;
+  bool tables = false;
+  DevBuf counts, offsets, entries;
+};
+DeviceSamplerState g_dev_sampler;
+std::mutex g_dev_sampler_mu;
+long long g_pass_pairs_cap = 0;  // 0: size passes from the acceptance rate
+
+// Host decision for a pair the device left open (glibc spectrum).
+bool host_accept(const scarf_srm_setup& s, int acf, float r1, float r2) {
+  float u;
+  return accept(r1, r2, s, acf, &u);
+}
+
+}  // namespace
+
+void set_device_sampler_pass_cap(long long pairs) {
+  std::lock_guard<std::mutex> lk(g_dev_sampler_mu);
+  g_pass_pairs_cap = pairs > 0 ? pairs : 0;
+}
+
+int srm_sample_device(const scarf_srm_params& p, const scarf_srm_setup& s, float* table, long long* pairs_used,
+                      void* stream_handle, long long* uncertain) {
+  const cudaStream_t stream = static_cast<cudaStream_t>(stream_handle);
+  const double acc = acceptance_rate(s);
+  if (acc < kMinAcceptance) return -1;
+  std::lock_guard<std::mutex> lk(g_dev_sampler_mu);
+  DeviceSamplerState& D = g_dev_sampler;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return -2;
+  if (D.device != dev) {
+    D = DeviceSamplerState();
+    D.device = dev;
+  }
+  if (!D.tables) {
+    const PowTables& t = pow_tables();
+    if (sampler_upload_tables(t.lo.data(), t.hi.data()) != cudaSuccess) return -2;
+    D.tables = true;
+  }
+  Yarn2 g;
+  g.seed(p.seed);
+  SamplerArgs A{};
+  A.r0 = g.r0;
+  A.r1 = g.r1;
+  A.kmin = s.kmin;
+  A.kmax = s.kmax;
+  A.cnst = s.cnst;
+  A.nu = s.nu;
+  A.ndim = s.ndim;
+  A.acf = p.acf;
+  // Device and host spectra differ by a few ulps at most; 2e-5 relative is a
+  // wide bound around the decision r2 < d.
+  A.margin = 2e-5f;
+
+  std::vector<SampleEntry> entries;
+  std::vector<int> counts;
+  std::vector<long long> offsets;
+  long long open = 0;
+  auto run_pass = [&](long long q_begin, long long count) -> bool {
+    A.q_begin = q_begin;
+    A.q_count = count;
+    A.pairs_per_thread = static_cast<int>(std::min<long long>(8192, std::max<long long>(256, count / (148 * 2048))));
+    A.nthreads = (count + A.pairs_per_thread - 1) / A.pairs_per_thread;
+    if (D.counts.ensure(sizeof(int) * A.nthreads) != cudaSuccess) return false;
+    if (D.offsets.ensure(sizeof(long long) * A.nthreads) != cudaSuccess) return false;
+    A.counts = static_cast<int*>(D.counts.p);
+    A.offsets = static_cast<const long long*>(D.offsets.p);
+    A.write = 0;
+    if (launch_sampler(A, stream) != cudaSuccess) return false;
+    counts.resize(A.nthreads);
+    if (cudaMemcpyAsync(counts.data(), D.counts.p, sizeof(int) * A.nthreads, cudaMemcpyDeviceToHost, stream) !=
+            cudaSuccess ||
+        cudaStreamSynchronize(stream) != cudaSuccess)
+      return false;
+    offsets.resize(A.nthreads);
+    long long total = 0;
+    for (long long t = 0; t < A.nthreads; ++t) {
+      offsets[t] = total;
+      total += counts[t];
+    }
+    entries.resize(total);
+    if (total > 0) {
+      if (D.entries.ensure(sizeof(SampleEntry) * total) != cudaSuccess) return false;
+      if (cudaMemcpyAsync(D.offsets.p, offsets.data(), sizeof(long long) * A.nthreads, cudaMemcpyHostToDevice,
+                          stream) != cudaSuccess)
+        return false;
+      A.out = static_cast<SampleEntry*>(D.entries.p);
+      A.write = 1;
+      if (launch_sampler(A, stream) != cudaSuccess) return false;
+      if (cudaMemcpyAsync(entries.data(), D.entries.p, sizeof(SampleEntry) * total, cudaMemcpyDeviceToHost,
+                          stream) != cudaSuccess ||
+          cudaStreamSynchronize(stream) != cudaSuccess)
+        return false;
+    }
+    return true;
+  };
+
+  // Walk the candidates in stream order exactly as the serial loop consumes
+  // pairs: reject until an accepted pair, then one pair of angles, then (for
+  // a kept harmonic) two pairs for a and b.
+  auto capped = [](long long n) { return g_pass_pairs_cap > 0 ? std::min(n, g_pass_pairs_cap) : n; };
+  long long pass_begin = 0, pass_end = capped(static_cast<long long>(p.nharm * (1.0 / acc + 3.0) * 1.1) + 4096);
+  if (!run_pass(pass_begin, pass_end)) return -2;
+  size_t ei = 0;
+  long long pos = 0;
+  int kept = 0;
+  for (int l = 0; l < p.nharm; ++l) {
+    for (;;) {
+      while (ei < entries.size() && entries[ei].q < pos) ++ei;
+      if (ei == entries.size()) {
+        const long long more = capped(static_cast<long long>((p.nharm - l) * (1.0 / acc + 3.0) * 1.2) + 4096);
+        pass_begin = pass_end;
+        pass_end = pass_begin + more;
+        if (!run_pass(pass_begin, more)) return -2;
+        ei = 0;
+        continue;
+      }
+      const SampleEntry& e = entries[ei];
+      bool ok = e.flag == 1;
+      if (e.flag == 2) {
+        ++open;
+        ok = host_accept(s, p.acf, e.r[0], e.r[1]);
+      }
+      if (!ok) {
+        ++ei;
+        continue;
+      }
+      Draws d{};
+      d.u = e.r[0] * (s.kmax - s.kmin) + s.kmin;
+      if (d.u > s.kc) {
+        pos = e.q + 2;
+        break;
+      }
+      d.ang[0] = e.r[2];
+      d.ang[1] = e.r[3];
+      d.ra[0] = e.r[4];
+      d.ra[1] = e.r[5];
+      d.rb[0] = e.r[6];
+      d.rb[1] = e.r[7];
+      harmonic_row(d, s.ndim, p.cl, table + 5 * static_cast<size_t>(kept));
+      ++kept;
+      pos = e.q + 4;
+      break;
+    }
+  }
+  if (pairs_used) *pairs_used = pos;
+  if (uncertain) *uncertain = open;
+  return kept;
 }
 
 int srm_sample(const scarf_srm_params& p, const scarf_srm_setup& s, const UniformSource* src, int threads,

@@ -69,6 +69,19 @@ int srm_sample(const scarf_srm_params& p, const scarf_srm_setup& s, const Unifor
 constexpr double kMinAcceptance = 1e-6;
 double acceptance_rate(const scarf_srm_setup& s);
 
+// Same table as srm_sample with the built-in generator, with the rejection
+// tests run on the current GPU: the device evaluates every pair of the
+// stream and the host walks the accepted ones (and decides the few pairs
+// whose test lies within float rounding of the threshold), so the result is
+// bit-identical to the serial host loop. Returns the harmonics kept, -1 if
+// rejection sampling is infeasible, -2 on a CUDA error. *uncertain counts the
+// pairs decided on the host.
+int srm_sample_device(const scarf_srm_params& p, const scarf_srm_setup& s, float* table, long long* pairs_used,
+                      void* stream, long long* uncertain);
+// Upper bound on the pairs tested per device pass (0 = sized from the
+// acceptance rate); smaller passes are chained until every harmonic is drawn.
+void set_device_sampler_pass_cap(long long pairs);
+
 int host_threads();
 
 }  // namespace scarf

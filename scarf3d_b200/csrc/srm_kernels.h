@@ -72,6 +72,28 @@ cudaError_t tc_batch_upload(const TcBatchInput* in, const TcBatchPlan& plan, voi
 cudaError_t tc_batch_launch(const TcBatchPlan& plan, void* d_work, cudaStream_t stream,
                             cudaEvent_t ev_main0 = nullptr, cudaEvent_t ev_main1 = nullptr);
 
+// ---- device side of the harmonic sampler (srm_sampler.cu) ----
+struct SampleEntry {
+  long long q;  // pair index in the stream
+  int flag;     // 1 = accepted, 2 = to be decided on the host
+  int pad;
+  float r[8];   // pairs q, q+1, q+2, q+3
+};
+struct SamplerArgs {
+  unsigned long long r0, r1;  // generator state after seeding (pair 0 next)
+  long long q_begin, q_count;
+  int pairs_per_thread;
+  long long nthreads;
+  float kmin, kmax, cnst, nu, margin;
+  int ndim, acf;
+  int write;                 // 0: count per thread, 1: write entries
+  int* counts;               // [nthreads]
+  const long long* offsets;  // [nthreads]
+  SampleEntry* out;
+};
+cudaError_t sampler_upload_tables(const unsigned int* lo, const unsigned int* hi);
+cudaError_t launch_sampler(const SamplerArgs& args, cudaStream_t stream);
+
 // ---- statistics and post-processing (srm_stats.cu) ----
 size_t stats_partials_bytes(long long n);
 // Two passes (mean, then centred sums) in FP64; writes mean/var (FP32

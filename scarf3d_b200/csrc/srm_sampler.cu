@@ -1,0 +1,146 @@
+// Device side of the harmonic sampler: the rejection tests of the sampling
+// loop (scarflib_srm.f90:731-745) evaluated for a whole range of uniform
+// pairs at once.
+//
+// Thread t owns pairs [q0, q0 + P) of the stream, jumps a copy of the
+// generator to draw 2*q0 and tests each pair exactly as the host does: the
+// same integer recursion and output power, the same float mapping, u in FP32
+// with the reference's operation order. Only the spectrum (powf / expf) may
+// differ from the host's libm by a few ulps, so a decision whose margin
+// |r2 - d| is below a relative bound that covers those ulps is flagged
+// "uncertain" and left to the host. Certain rejections are dropped; accepted
+// and uncertain pairs are written, in stream order, with the raw floats of
+// the pair and of the three pairs that follow it (angles, a, b), which is
+// everything the host walk needs.
+//
+// Two passes over the same range: the first counts candidates per thread,
+// the host turns the counts into offsets, the second writes them.
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "srm_kernels.h"
+
+namespace scarf {
+namespace {
+
+constexpr uint64_t kMod = 2147483647ull;
+constexpr uint64_t kA1 = 1498809829ull;
+constexpr uint64_t kA2 = 1160990996ull;
+
+__device__ uint32_t g_pow_lo[1 << 16];  // g^k mod m, k < 2^16
+__device__ uint32_t g_pow_hi[1 << 15];  // g^(k 2^16) mod m, k < 2^15
+
+__device__ __forceinline__ uint64_t mulmod(uint64_t a, uint64_t b) {
+  uint64_t p = a * b;  // < 2^62
+  p = (p & kMod) + (p >> 31);
+  p = (p & kMod) + (p >> 31);
+  return p >= kMod ? p - kMod : p;
+}
+__device__ __forceinline__ uint64_t addmod(uint64_t a, uint64_t b) {
+  const uint64_t s = a + b;
+  return s >= kMod ? s - kMod : s;
+}
+
+struct Gen {
+  uint64_t r0, r1;
+  __device__ __forceinline__ uint32_t next() {
+    const uint64_t t = addmod(mulmod(kA1, r0), mulmod(kA2, r1));
+    r1 = r0;
+    r0 = t;
+    if (t == 0) return 0u;
+    return static_cast<uint32_t>(mulmod(g_pow_lo[t & 0xFFFFu], g_pow_hi[t >> 16]));
+  }
+  __device__ __forceinline__ void jump(uint64_t n) {
+    uint64_t m00 = kA1, m01 = kA2, m10 = 1, m11 = 0;
+    uint64_t p00 = 1, p01 = 0, p10 = 0, p11 = 1;
+    while (n) {
+      if (n & 1) {
+        const uint64_t q00 = addmod(mulmod(p00, m00), mulmod(p01, m10));
+        const uint64_t q01 = addmod(mulmod(p00, m01), mulmod(p01, m11));
+        const uint64_t q10 = addmod(mulmod(p10, m00), mulmod(p11, m10));
+        const uint64_t q11 = addmod(mulmod(p10, m01), mulmod(p11, m11));
+        p00 = q00, p01 = q01, p10 = q10, p11 = q11;
+      }
+      const uint64_t s00 = addmod(mulmod(m00, m00), mulmod(m01, m10));
+      const uint64_t s01 = addmod(mulmod(m00, m01), mulmod(m01, m11));
+      const uint64_t s10 = addmod(mulmod(m10, m00), mulmod(m11, m10));
+      const uint64_t s11 = addmod(mulmod(m10, m01), mulmod(m11, m11));
+      m00 = s00, m01 = s01, m10 = s10, m11 = s11;
+      n >>= 1;
+    }
+    const uint64_t n0 = addmod(mulmod(p00, r0), mulmod(p01, r1));
+    const uint64_t n1 = addmod(mulmod(p10, r0), mulmod(p11, r1));
+    r0 = n0;
+    r1 = n1;
+  }
+};
+
+__device__ __forceinline__ float to_u01(uint32_t y) {
+  return __fmul_rn(__fadd_rn(static_cast<float>(y >> 8), 0.5f), 1.0f / 8388608.0f);
+}
+
+// 0 = certain reject, 1 = certain accept, 2 = uncertain.
+__device__ __forceinline__ int classify(const SamplerArgs& A, float r1, float r2) {
+  const float u = __fadd_rn(__fmul_rn(r1, __fsub_rn(A.kmax, A.kmin)), A.kmin);
+  float fv;
+  if (A.acf == 0) {
+    fv = __fdiv_rn(1.0f, powf(__fadd_rn(1.0f, __fmul_rn(u, u)), A.nu));
+  } else {
+    fv = expf(__fmul_rn(-0.25f, __fmul_rn(u, u)));
+  }
+  double srm = static_cast<double>(u) * static_cast<double>(fv);
+  if (A.ndim == 3) srm = srm * static_cast<double>(u);
+  const float d = static_cast<float>(srm * static_cast<double>(A.cnst));
+  if (r2 < d * (1.0f - A.margin)) return 1;
+  if (r2 >= d * (1.0f + A.margin)) return 0;
+  return 2;
+}
+
+__global__ void sampler_kernel(const SamplerArgs A) {
+  const long long t = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (t >= A.nthreads) return;
+  const long long q0 = A.q_begin + t * A.pairs_per_thread;
+  long long q1 = q0 + A.pairs_per_thread;
+  if (q1 > A.q_begin + A.q_count) q1 = A.q_begin + A.q_count;
+  Gen g{A.r0, A.r1};
+  g.jump(2ull * static_cast<uint64_t>(q0));
+  int count = 0;
+  long long slot = A.write ? A.offsets[t] : 0;
+  for (long long q = q0; q < q1; ++q) {
+    const float r1 = to_u01(g.next());
+    const float r2 = to_u01(g.next());
+    const int c = classify(A, r1, r2);
+    if (c == 0) continue;
+    ++count;
+    if (A.write) {
+      SampleEntry e;
+      e.q = q;
+      e.flag = c;
+      e.r[0] = r1;
+      e.r[1] = r2;
+      Gen look = g;  // the three pairs after q, without disturbing the scan
+      for (int k = 2; k < 8; ++k) e.r[k] = to_u01(look.next());
+      A.out[slot++] = e;
+    }
+  }
+  if (!A.write) A.counts[t] = count;
+}
+
+}  // namespace
+
+cudaError_t sampler_upload_tables(const uint32_t* lo, const uint32_t* hi) {
+  cudaError_t e = cudaMemcpyToSymbol(g_pow_lo, lo, sizeof(uint32_t) * (1u << 16));
+  if (e == cudaSuccess) e = cudaMemcpyToSymbol(g_pow_hi, hi, sizeof(uint32_t) * (1u << 15));
+  return e;
+}
+
+cudaError_t launch_sampler(const SamplerArgs& A, cudaStream_t stream) {
+  const int block = 128;
+  const long long blocks = (A.nthreads + block - 1) / block;
+  if (blocks <= 0) return cudaSuccess;
+  sampler_kernel<<<static_cast<unsigned>(blocks), block, 0, stream>>>(A);
+  return cudaGetLastError();
+}
+
+}  // namespace scarf
