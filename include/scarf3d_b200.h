@@ -88,6 +88,21 @@ float scarf_last_kernel_ms(void);
  * does not round to nearest, so its error grows with this length. */
 int scarf_set_tc_chunk(int harmonics);
 
+/* Host-field output of scarf_execute on a structured mesh with the
+ * tensor-core form, no rescale and no taper: the field is copied to the host
+ * in slabs (a column tile x a run of row blocks, about items_per_slab work
+ * items of 128 x <=256 points each) while the kernel computes the rest.
+ * 1 = default slab size (256 items), >= 2 = that size, 0 = copy the whole
+ * field after the kernel. The field is identical either way. */
+int scarf_set_output_overlap(int items_per_slab);
+
+/* Where the tensor-core form keeps its generated A operand, for plans made
+ * after the call: 0 = shared memory (default; column tiles <= 256), 1 =
+ * tensor memory (column tiles <= 192). Both give identical sums; tensor
+ * memory takes the A tile off the shared-memory port but narrows the column
+ * tile, so it is slower on the grids measured so far. */
+int scarf_set_tc_a_in_tmem(int on);
+
 /* Status-returning scarf_execute (c_binding.c:138-143); stats[8] as the
  * reference fills it (stats[4] host seconds, stats[5] device seconds). */
 int scarf_execute_ex(int seed, float *field, float stats[8], int flags);

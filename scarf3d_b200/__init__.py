@@ -34,7 +34,8 @@ EXPORTED_SYMBOLS = (
     # extended (include/scarf3d_b200.h)
     "scarf_last_error", "scarf_set_nharm", "scarf_get_nharm", "scarf_set_form",
     "scarf_set_uniform_source", "scarf_set_stream", "scarf_set_host_threads", "scarf_set_kernel_timing",
-    "scarf_last_kernel_ms", "scarf_set_tc_chunk", "scarf_execute_ex",
+    "scarf_last_kernel_ms", "scarf_set_tc_chunk", "scarf_set_tc_a_in_tmem", "scarf_set_output_overlap",
+    "scarf_execute_ex",
     "scarf_srm_compute_setup", "scarf_srm_sample", "scarf_srm_sample_device", "scarf_set_sampler",
     "scarf_set_sampler_pass_pairs",
     "scarf_srm_direct_structured",
@@ -114,6 +115,8 @@ def _load() -> ctypes.CDLL:
         "scarf_set_kernel_timing": (c_int, [c_int]),
         "scarf_last_kernel_ms": (c_float, []),
         "scarf_set_tc_chunk": (c_int, [c_int]),
+        "scarf_set_tc_a_in_tmem": (c_int, [c_int]),
+        "scarf_set_output_overlap": (c_int, [c_int]),
         "scarf_execute_ex": (c_int, [c_int, c_void_p, fp, c_int]),
         "scarf_srm_compute_setup": (c_int, [ctypes.POINTER(SrmParams), ctypes.POINTER(SrmSetup)]),
         "scarf_srm_sample": (c_int, [ctypes.POINTER(SrmParams), ctypes.POINTER(SrmSetup), c_void_p, ip,
@@ -338,6 +341,19 @@ def set_nharm(n: int):
 
 def set_form(form: int):
     check(lib.scarf_set_form(int(form)))
+
+
+def set_tc_a_in_tmem(on: bool):
+    """Tensor-core form: generated A operand in tensor memory (True) or
+    shared memory (False, the default); applies to plans made afterwards."""
+    check(lib.scarf_set_tc_a_in_tmem(1 if on else 0))
+
+
+def set_output_overlap(items_per_slab: int = 1):
+    """scarf_execute: copy finished field slabs (about items_per_slab work
+    items each; 1 = default size) to the host while the kernel runs, or the
+    whole field afterwards (0)."""
+    check(lib.scarf_set_output_overlap(int(items_per_slab)))
 
 
 def set_host_threads(n: int):

@@ -14,6 +14,7 @@
 #include <mutex>
 #include <new>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "scarf3d.h"
@@ -55,6 +56,7 @@ struct Config {
   int threads = 0;
   int sampler = SCARF_SAMPLER_AUTO;
   bool kernel_timing = false;
+  int overlap_items = 256;  // work items per slab copied out while the kernel runs; 0 = off
 };
 Config g_cfg;
 float g_last_kernel_ms = 0.0f;
@@ -101,9 +103,21 @@ struct DeviceBuf {
 
 struct Resources {
   int device = -1;
-  DeviceBuf status, stats, table, field, coords, work;
-  cudaEvent_t ev0 = nullptr, ev1 = nullptr, evk0 = nullptr, evk1 = nullptr;
+  DeviceBuf status, stats, table, field, coords, work, slab_cnt;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr, evk0 = nullptr, evk1 = nullptr, evs = nullptr;
+  cudaStream_t copy_stream = nullptr;  // non-blocking: runs beside the legacy stream too
+  int* slab_flags = nullptr;           // host-mapped, written by the kernel
+  int* slab_flags_dev = nullptr;
+  int slab_cap = 0;
   void release() {
+    if (slab_flags) cudaFreeHost(slab_flags);
+    slab_flags = slab_flags_dev = nullptr;
+    slab_cap = 0;
+    slab_cnt.release();
+    if (copy_stream) cudaStreamDestroy(copy_stream);
+    copy_stream = nullptr;
+    if (evs) cudaEventDestroy(evs);
+    evs = nullptr;
     if (evk0) cudaEventDestroy(evk0);
     if (evk1) cudaEventDestroy(evk1);
     evk0 = evk1 = nullptr;
@@ -134,6 +148,62 @@ int ensure_resources() {
   if (!g_res.ev1) SCARF_CUDA(cudaEventCreate(&g_res.ev1));
   if (!g_res.evk0) SCARF_CUDA(cudaEventCreate(&g_res.evk0));
   if (!g_res.evk1) SCARF_CUDA(cudaEventCreate(&g_res.evk1));
+  return SCARF_OK;
+}
+
+// Slab flags (host-mapped) and device counters for at least n slabs, plus the
+// copy stream and its join event.
+int ensure_slab_resources(int n) {
+  if (!g_res.copy_stream) SCARF_CUDA(cudaStreamCreateWithFlags(&g_res.copy_stream, cudaStreamNonBlocking));
+  if (!g_res.evs) SCARF_CUDA(cudaEventCreateWithFlags(&g_res.evs, cudaEventDisableTiming));
+  if (n > g_res.slab_cap) {
+    if (g_res.slab_flags) cudaFreeHost(g_res.slab_flags);
+    g_res.slab_flags = g_res.slab_flags_dev = nullptr;
+    g_res.slab_cap = 0;
+    void* h = nullptr;
+    SCARF_CUDA(cudaHostAlloc(&h, sizeof(int) * n, cudaHostAllocMapped));
+    g_res.slab_flags = static_cast<int*>(h);
+    void* d = nullptr;
+    SCARF_CUDA(cudaHostGetDevicePointer(&d, h, 0));
+    g_res.slab_flags_dev = static_cast<int*>(d);
+    g_res.slab_cap = n;
+  }
+  SCARF_CUDA(g_res.slab_cnt.ensure(sizeof(int) * n));
+  return SCARF_OK;
+}
+
+inline void cpu_relax() {
+#if defined(__x86_64__) || defined(__i386__)
+  __builtin_ia32_pause();
+#else
+  std::this_thread::yield();
+#endif
+}
+
+// Copies the slabs of a running single-field launch to the host field in
+// slab order, each as soon as the kernel has flagged it, on the copy stream.
+// Once the launch stream is idle every remaining slab is copied without
+// waiting (the status check that follows reports a failed launch).
+int copy_slabs_out(const TcPlan& plan, const TcSlabSignal& sig, const float* d_field, float* field,
+                   cudaStream_t st) {
+  volatile int* flags = g_res.slab_flags;
+  const size_t plane = static_cast<size_t>(plan.n1) * plan.n2;
+  bool idle = false;
+  for (int q = 0; q < sig.nslabs; ++q) {
+    for (uint32_t spins = 0; !idle && !flags[q]; ++spins) {
+      if ((spins & 1023u) == 1023u && cudaStreamQuery(st) != cudaErrorNotReady) {
+        cudaGetLastError();
+        idle = true;
+      }
+      cpu_relax();
+    }
+    const TcSlab e = tc_slab_extent(plan, sig, q);
+    if (e.z1 <= e.z0 || e.y1 <= e.y0) continue;
+    const size_t off = static_cast<size_t>(e.z0) * plane + static_cast<size_t>(e.y0) * plan.n1;
+    SCARF_CUDA(cudaMemcpy2DAsync(field + off, plane * sizeof(float), d_field + off, plane * sizeof(float),
+                                 static_cast<size_t>(e.y1 - e.y0) * plan.n1 * sizeof(float), e.z1 - e.z0,
+                                 cudaMemcpyDeviceToHost, g_res.copy_stream));
+  }
   return SCARF_OK;
 }
 
@@ -247,13 +317,42 @@ int execute_impl(int seed, float* field, float stats[8], int flags) {
   const float* dx = nullptr;
   const float* dy = nullptr;
   const float* dz = nullptr;
+  const bool taper_ok = g_obj.structured || (flags & SCARF_TAPER_UNSTRUCTURED);
+  const bool tapering = taper_ok && g_obj.poi && g_obj.npoi > 0;
+  // Set once slab copies into the caller's buffer are in flight: every exit
+  // from here on first waits for them.
+  struct CopyJoin {
+    bool active = false;
+    ~CopyJoin() {
+      if (active && g_res.copy_stream) cudaStreamSynchronize(g_res.copy_stream);
+    }
+  } copy_join;
+  bool copied_out = false;  // field already on its way to the host (slab copies)
   if (g_obj.structured) {
     const bool use_tc = (g_cfg.form != SCARF_FORM_DIRECT);
     TcPlan plan{};
     if (use_tc && nh > 0 && tc_make_plan(s.ndim, n, nh, &plan)) {
       SCARF_CUDA(g_res.work.ensure(plan.bytes));
+      // Without rescale or taper the field is final when the kernel stores
+      // it: copy it out slab by slab while the kernel still runs.
+      TcSlabSignal sig;
+      const bool overlap = g_cfg.overlap_items > 0 && !on_device && p.rescale != 1 && !tapering;
+      if (overlap) {
+        tc_slab_layout(plan, g_cfg.overlap_items, &sig);
+        rc = ensure_slab_resources(sig.nslabs);
+        if (rc) return rc;
+        std::memset(g_res.slab_flags, 0, sizeof(int) * sig.nslabs);
+        sig.d_cnt = static_cast<int*>(g_res.slab_cnt.p);
+        sig.flag_dev = g_res.slab_flags_dev;
+      }
       SCARF_CUDA(launch_tc_structured(s, g_obj.fs, n, p.ds, d_table, nh, d_field, g_res.work.p, plan, d_status, st,
-                                      kernel_ev0(), kernel_ev1()));
+                                      kernel_ev0(), kernel_ev1(), overlap ? &sig : nullptr));
+      if (overlap) {
+        copy_join.active = true;
+        rc = copy_slabs_out(plan, sig, d_field, field, st);
+        if (rc) return rc;
+        copied_out = true;
+      }
     } else if (nh > 0) {
       if (kernel_ev0()) SCARF_CUDA(cudaEventRecord(kernel_ev0(), st));
       SCARF_CUDA(launch_direct_structured(s, g_obj.fs, n, p.ds, d_table, nh, d_field, d_status, st));
@@ -304,8 +403,7 @@ int execute_impl(int seed, float* field, float stats[8], int flags) {
     stats[2] = p.sigma;
     stats[3] = 0.0f;
   }
-  const bool taper_ok = g_obj.structured || (flags & SCARF_TAPER_UNSTRUCTURED);
-  if (taper_ok && g_obj.poi && g_obj.npoi > 0) {
+  if (tapering) {
     for (int q = 0; q < g_obj.npoi; ++q) {
       float pt[3] = {0.0f, 0.0f, 0.0f};
       for (int c = 0; c < s.ndim; ++c) pt[c] = g_obj.poi[g_obj.nd * q + c];
@@ -315,9 +413,17 @@ int execute_impl(int seed, float* field, float stats[8], int flags) {
         SCARF_CUDA(launch_taper_points(d_field, dx, dy, dz, npts, pt, g_obj.mute, g_obj.taper, st));
     }
   }
-  SCARF_CUDA(cudaEventRecord(g_res.ev1, st));
-  if (!on_device)
-    SCARF_CUDA(cudaMemcpyAsync(field, d_field, sizeof(float) * npts, cudaMemcpyDeviceToHost, st));
+  if (copied_out) {
+    // Device time ends with the last slab copy.
+    SCARF_CUDA(cudaEventRecord(g_res.evs, st));
+    SCARF_CUDA(cudaStreamWaitEvent(g_res.copy_stream, g_res.evs, 0));
+    SCARF_CUDA(cudaEventRecord(g_res.ev1, g_res.copy_stream));
+    SCARF_CUDA(cudaStreamSynchronize(g_res.copy_stream));
+  } else {
+    SCARF_CUDA(cudaEventRecord(g_res.ev1, st));
+    if (!on_device)
+      SCARF_CUDA(cudaMemcpyAsync(field, d_field, sizeof(float) * npts, cudaMemcpyDeviceToHost, st));
+  }
   SCARF_CUDA(cudaStreamSynchronize(st));
   float ms = 0.0f;
   cudaEventElapsedTime(&ms, g_res.ev0, g_res.ev1);
@@ -815,6 +921,19 @@ int scarf_set_tc_chunk(int harmonics) {
   if (harmonics < 0) return fail(SCARF_ERR_ARG, "chunk must be >= 0");
   std::lock_guard<std::mutex> lk(g_mu);
   tc_set_chunk_harmonics(harmonics);
+  return SCARF_OK;
+}
+
+int scarf_set_output_overlap(int items_per_slab) {
+  if (items_per_slab < 0) return fail(SCARF_ERR_ARG, "items_per_slab must be >= 0");
+  std::lock_guard<std::mutex> lk(g_mu);
+  g_cfg.overlap_items = items_per_slab == 1 ? 256 : items_per_slab;
+  return SCARF_OK;
+}
+
+int scarf_set_tc_a_in_tmem(int on) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  tc_set_a_in_tmem(on);
   return SCARF_OK;
 }
 

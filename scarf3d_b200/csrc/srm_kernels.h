@@ -32,19 +32,41 @@ struct TcPlan {
   int nh_pad;            // padded to a multiple of the stage size
   int stages;            // nh_pad / kStageHarm
   int chunk_stages;      // stages per TMEM accumulation chunk (FP32 sum of chunks)
+  int tmem_a;            // 1: A operand generated into tensor memory (ntile_n <= 192)
   size_t off_r, off_s, off_c, off_status, bytes;  // workspace layout
 };
+
+// Placement of the generated A operand for plans made from now on: 0 shared
+// memory (default), 1 tensor memory.
+void tc_set_a_in_tmem(int on);
 
 // tj_force > 0 fixes the row tile to (128 / tj_force) x tj_force.
 bool tc_make_plan(int ndim, const int n[3], int nh, TcPlan* plan, int tj_force = 0);
 // Harmonics accumulated in tensor memory before each FP32 drain (rounded up
 // to whole pipeline stages); 0 restores the default.
 void tc_set_chunk_harmonics(int harmonics);
+// Slab-wise completion signal of a single-field launch. Slab q covers column
+// tile q / spn and row blocks j in [(q % spn) * jbs, +jbs): rows x columns
+// that are one strided block of the column-major field. The kernel sets
+// flag[q] = 1 (host-mapped memory) once every item of slab q is stored.
+struct TcSlab {
+  int z0, z1;  // column (plan axis 3) range
+  int y0, y1;  // row-block j range in grid rows (plan axis 2)
+};
+struct TcSlabSignal {
+  int* d_cnt = nullptr;    // >= nslabs device counters (zeroed by the launch)
+  int* flag_dev = nullptr; // device address of >= nslabs host-mapped ints, zeroed by the caller
+  int jbs = 0, spn = 0, nslabs = 0;
+};
+// Slab layout of a plan with about target_items work items per slab.
+void tc_slab_layout(const TcPlan& p, int target_items, TcSlabSignal* sig);
+TcSlab tc_slab_extent(const TcPlan& p, const TcSlabSignal& sig, int q);
+
 // Status word at d_status[0]; d_status[1] is used as the work-queue counter.
 cudaError_t launch_tc_structured(const scarf_srm_setup& s, const int fs[3], const int n[3], float ds,
                                  const float* d_table, int nh, float* d_field, void* d_work, const TcPlan& plan,
                                  int* d_status, cudaStream_t stream, cudaEvent_t ev_main0 = nullptr,
-                                 cudaEvent_t ev_main1 = nullptr);
+                                 cudaEvent_t ev_main1 = nullptr, const TcSlabSignal* slabs = nullptr);
 
 // Batched form: many fields in one persistent launch fed by a device work
 // queue. All fields of a batch share one row-tile shape.
@@ -58,7 +80,7 @@ struct TcBatchInput {
   int tj;  // row-tile shape (0 = automatic)
 };
 struct TcBatchPlan {
-  int nfields = 0, num_items = 0, ti = 0, tj = 0, ntile_max = 0;
+  int nfields = 0, num_items = 0, ti = 0, tj = 0, ntile_max = 0, tmem_a = 0;
   size_t off_fields = 0, off_jobs = 0, off_items = 0, off_status = 0, bytes = 0;
   std::vector<TcPlan> plans;
   std::vector<size_t> field_off;

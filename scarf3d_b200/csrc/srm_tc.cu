@@ -37,10 +37,15 @@ constexpr int kStageHarm = 16;                  // harmonics per pipeline stage 
 constexpr int kRows = 128;                      // M of one tile (one CTA)
 constexpr int kRowBytes = 64;                   // 32 fp16 along K = one 64-B swizzle row
 constexpr int kATileBytes = kRows * kRowBytes;  // 8 KB per hi or lo
-constexpr int kThreads = 512;                   // 16 warps
-constexpr int kGenWarp0 = 8;                    // warps 8..15 generate A
+#ifndef SCARF_TC_GEN_WARPS
+#define SCARF_TC_GEN_WARPS 8
+#endif
+constexpr int kGenWarps = SCARF_TC_GEN_WARPS;   // A generators: 8 or 16
+constexpr int kGenWarp0 = 8;                    // warps 8.. generate A (8 % 4 == 0: lane quadrants line up)
 constexpr int kEpiWarp0 = 4;                    // warps 4..7 drain the accumulators
-constexpr int kGenWarps = kThreads / 32 - kGenWarp0;
+constexpr int kThreads = 32 * (kGenWarp0 + kGenWarps);
+constexpr int kGenHarm = kStageHarm * 4 / kGenWarps;  // harmonics per generator thread and stage
+static_assert(kGenWarps == 8 || kGenWarps == 16, "generator warps: 8 or 16");
 constexpr int kItemRing = 4;                    // work items in flight between roles
 constexpr int kItemConsumers = 1 + 4 + kGenWarps;  // MMA warp, epilogue warps, generator warps
 constexpr uint32_t kSwizzle64 = 4;              // tcgen05 descriptor: 64-B swizzle
@@ -71,6 +76,12 @@ struct TcKernelArgs {
   int ti, tj, ti_shift;   // row-tile shape (uniform over a launch)
   int nstage_buf;
   uint32_t stage_bytes, off_b, off_a, off_r, off_s, bars_off;
+  // Slab completion signal (single-field launches; null otherwise): a slab
+  // is one column tile x a run of slab_jbs row blocks along j, contiguous
+  // pieces of the field that the host copies out while the kernel runs.
+  int* slab_cnt;            // device counters, zero at launch
+  volatile int* slab_flag;  // host-mapped flags, set once a slab is stored
+  int slab_jbs, slab_spn;   // row blocks per slab, slabs per column tile
 };
 
 // Per-field inputs of the table builders.
@@ -201,8 +212,25 @@ __device__ __forceinline__ Item decode_item(const TcKernelArgs& A, int idx) {
   return it;
 }
 
+// TMEM columns (512 allocated). Shared-memory A: chunk accumulator [0, 256),
+// FP32 master [256, 512). TMEM A: accumulator [0, 192), master [192, 384) and
+// an A ring of kTmemAStages stages [384, 512), each stage holding the hi half
+// (16 columns: 32 fp16 along K) then the lo half.
+constexpr int kMaxNSmemA = 256;
+constexpr int kMaxNTmemA = 192;
+constexpr int kTmemAStages = 4;
+constexpr uint32_t kTmemACol0 = 384;
+constexpr uint32_t kTmemAStageCols = 32;
+
 // ------------------------------------------------------------- main kernel --
+// kTmemA selects where the generated A operand lives: shared memory (the
+// tensor core reads both operands from shared memory) or tensor memory
+// (tcgen05.st from the generator registers, MMA in its TMEM-A form). The
+// TMEM-A form takes the A tile's writes and its three operand reads per
+// stage off the shared-memory port, which is the pipeline's bottleneck.
+template <bool kTmemA>
 __global__ void __launch_bounds__(kThreads, 1) srm_tc_kernel(const TcKernelArgs A) {
+  constexpr uint32_t kMasterCol = kTmemA ? kMaxNTmemA : kMaxNSmemA;
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   const int S = A.nstage_buf;
@@ -258,118 +286,132 @@ __global__ void __launch_bounds__(kThreads, 1) srm_tc_kernel(const TcKernelArgs 
 
   if (warp == 0) {
     // ------------------------------------------------------ producer -------
-    uint32_t cnt = 0;
-    uint32_t last_cnt[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-    bool used[8] = {false, false, false, false, false, false, false, false};
-    for (uint32_t it = 0; ok; ++it) {
-      const int q = it % kItemRing;
-      if (!mbar_wait_bounded(&item_empty[q], ((it / kItemRing) & 1) ^ 1, A.status)) {
-        ok = false;
-        break;
-      }
-      int idx = 0;
-      if (lane == 0) {
-        idx = atomicAdd(A.queue, 1);
+    // One thread; stage slot and phase advance incrementally.
+    if (lane == 0) {
+      int s = 0;
+      uint32_t ph = 0, issued = 0;
+      for (uint32_t it = 0; ok; ++it) {
+        const int q = it % kItemRing;
+        if (!mbar_wait_bounded(&item_empty[q], ((it / kItemRing) & 1) ^ 1, A.status)) {
+          ok = false;
+          break;
+        }
+        int idx = atomicAdd(A.queue, 1);
         if (idx >= A.num_items) idx = -1;
         item_slot[q] = idx;
         mbar_arrive(&item_full[q]);  // release: the slot write is visible to waiters
-      }
-      idx = __shfl_sync(0xffffffffu, idx, 0);
-      if (idx < 0) break;
-      const Item w = decode_item(A, idx);
-      const uint32_t bbytes = 2u * w.f.ntile_n * kRowBytes;
-      const uint32_t rbytes = kStageHarm * A.ti * 8u;
-      const uint32_t sbytes = kStageHarm * A.tj * 8u;
-      for (int k = 0; k < w.f.stages; ++k, ++cnt) {
-        const int s = cnt % S;
-        const uint32_t ph = (cnt / S) & 1;
-        if (!mbar_wait_bounded(&empty[s], ph ^ 1, A.status)) {
-          ok = false;
-          break;
-        }
-        if (lane == 0) {
+        if (idx < 0) break;
+        const Item w = decode_item(A, idx);
+        const uint32_t bbytes = 2u * w.f.ntile_n * kRowBytes;
+        const uint32_t rbytes = kStageHarm * A.ti * 8u;
+        const uint32_t sbytes = kStageHarm * A.tj * 8u;
+        const uint8_t* csrc = w.f.cimg + static_cast<size_t>(w.nt) * w.f.stages * bbytes;
+        const float2* rsrc = w.f.rimg + static_cast<size_t>(w.ib) * w.f.stages * kStageHarm * A.ti;
+        const float2* ssrc = w.f.simg + static_cast<size_t>(w.jb) * w.f.stages * kStageHarm * A.tj;
+        for (int k = 0; k < w.f.stages; ++k) {
+          if (!mbar_wait_bounded(&empty[s], ph ^ 1, A.status)) {
+            ok = false;
+            break;
+          }
           uint8_t* st = smem + s * A.stage_bytes;
           mbar_arrive_expect_tx(&full[s], bbytes + rbytes + sbytes);
-          bulk_g2s(st + A.off_b, w.f.cimg + (static_cast<size_t>(w.nt) * w.f.stages + k) * bbytes, bbytes,
-                   &full[s]);
-          bulk_g2s(st + A.off_r, w.f.rimg + (static_cast<size_t>(w.ib) * w.f.stages + k) * kStageHarm * A.ti, rbytes,
-                   &full[s]);
-          bulk_g2s(st + A.off_s, w.f.simg + (static_cast<size_t>(w.jb) * w.f.stages + k) * kStageHarm * A.tj, sbytes,
-                   &full[s]);
+          bulk_g2s(st + A.off_b, csrc + static_cast<size_t>(k) * bbytes, bbytes, &full[s]);
+          bulk_g2s(st + A.off_r, rsrc + static_cast<size_t>(k) * kStageHarm * A.ti, rbytes, &full[s]);
+          bulk_g2s(st + A.off_s, ssrc + static_cast<size_t>(k) * kStageHarm * A.tj, sbytes, &full[s]);
+          ++issued;
+          if (++s == S) {
+            s = 0;
+            ph ^= 1;
+          }
         }
-        last_cnt[s] = cnt;
-        used[s] = true;
-        __syncwarp();
+      }
+      if (!ok) {
+        // Let every issued copy land before shared memory is released: the
+        // last min(issued, S) stages, each in the phase it was issued in.
+        const uint32_t n_in_flight = issued < static_cast<uint32_t>(S) ? issued : S;
+        for (uint32_t b = 1; b <= n_in_flight; ++b) {
+          const uint32_t c = issued - b;
+          mbar_wait_drain(&full[c % S], (c / S) & 1);
+        }
       }
     }
-    if (!ok) {
-      // Let every issued copy land before shared memory is released.
-      for (int s = 0; s < S; ++s)
-        if (used[s]) mbar_wait_drain(&full[s], (last_cnt[s] / S) & 1);
-    }
+    __syncwarp();
   } else if (warp == 1) {
     // ------------------------------------------------------- MMA issuer ----
     // The K loop of an item runs in chunks of chunk_stages stages, each
-    // accumulated from zero in the TMEM chunk buffer (columns 0..255). At the
+    // accumulated from zero in the TMEM chunk buffer (columns from 0). At the
     // end of a chunk the epilogue adds the buffer into an FP32 master
-    // accumulator held in TMEM columns 256..511 (round to nearest), or, for
+    // accumulator held in TMEM from column kMasterCol (round to nearest), or, for
     // the last chunk, writes master + chunk to the field. The tensor core's
     // own FP32 accumulation is not round-to-nearest, so its error grows with
     // the number of accumulation steps into one buffer; chunking bounds it.
-    uint32_t cnt = 0, chunk = 0;
-    bool issued_any = false;
-    for (uint32_t it = 0; ok; ++it) {
-      int idx;
-      if (!next_item(it, idx)) {
-        ok = false;
-        break;
-      }
-      if (idx < 0) break;
-      const Item w = decode_item(A, idx);
-      for (int c0 = 0; c0 < w.f.stages && ok; c0 += w.f.chunk_stages, ++chunk) {
-        const int c1 = min(w.f.stages, c0 + w.f.chunk_stages);
-        // The previous chunk must be drained before the buffer restarts.
-        if (chunk > 0 && !mbar_wait_bounded(acce, (chunk - 1) & 1, A.status)) {
+    // One thread issues; stage slot and phase advance incrementally.
+    if (lane == 0) {
+      int s = 0;
+      uint32_t ph = 0, chunk = 0;
+      bool issued_any = false;
+      for (uint32_t it = 0; ok; ++it) {
+        const int q = it % kItemRing;
+        if (!mbar_wait_bounded(&item_full[q], (it / kItemRing) & 1, A.status)) {
           ok = false;
           break;
         }
-        tc_fence_after();
-        for (int k = c0; k < c1; ++k, ++cnt) {
-          const int s = cnt % S;
-          const uint32_t ph = (cnt / S) & 1;
-          if (!mbar_wait_bounded(&full[s], ph, A.status) || !mbar_wait_bounded(&agen[s], ph, A.status)) {
+        const int idx = *reinterpret_cast<volatile int*>(&item_slot[q]);
+        mbar_arrive(&item_empty[q]);
+        if (idx < 0) break;
+        const Item w = decode_item(A, idx);
+        const uint32_t b_lo_off = A.off_b + w.f.ntile_n * kRowBytes;
+        for (int c0 = 0; c0 < w.f.stages && ok; c0 += w.f.chunk_stages, ++chunk) {
+          const int c1 = min(w.f.stages, c0 + w.f.chunk_stages);
+          // The previous chunk must be drained before the buffer restarts.
+          if (chunk > 0 && !mbar_wait_bounded(acce, (chunk - 1) & 1, A.status)) {
             ok = false;
             break;
           }
           tc_fence_after();
-          if (lane == 0) {
+          for (int k = c0; k < c1; ++k) {
+            if (!mbar_wait_bounded(&full[s], ph, A.status) || !mbar_wait_bounded(&agen[s], ph, A.status)) {
+              ok = false;
+              break;
+            }
+            tc_fence_after();
             const uint32_t st = smem_u32(smem + s * A.stage_bytes);
-            const uint32_t a_hi = st + A.off_a, a_lo = a_hi + kATileBytes;
-            const uint32_t b_hi = st + A.off_b, b_lo = b_hi + w.f.ntile_n * kRowBytes;
+            const uint32_t b_hi = st + A.off_b, b_lo = st + b_lo_off;
 #pragma unroll
             for (int kk = 0; kk < 2; ++kk) {
-              const uint64_t dah = umma_smem_desc(a_hi + 32 * kk, 16, 512, kSwizzle64);
-              const uint64_t dal = umma_smem_desc(a_lo + 32 * kk, 16, 512, kSwizzle64);
               const uint64_t dbh = umma_smem_desc(b_hi + 32 * kk, 16, 512, kSwizzle64);
               const uint64_t dbl = umma_smem_desc(b_lo + 32 * kk, 16, 512, kSwizzle64);
-              umma_f16(tmem_base, dah, dbh, w.f.idesc, (k > c0 || kk > 0) ? 1u : 0u);
-              umma_f16(tmem_base, dah, dbl, w.f.idesc, 1u);
-              umma_f16(tmem_base, dal, dbh, w.f.idesc, 1u);
+              const uint32_t acc = (k > c0 || kk > 0) ? 1u : 0u;
+              if constexpr (kTmemA) {
+                const uint32_t ta = tmem_base + kTmemACol0 + s * kTmemAStageCols + 8 * kk;
+                umma_f16_ts(tmem_base, ta, dbh, w.f.idesc, acc);
+                umma_f16_ts(tmem_base, ta, dbl, w.f.idesc, 1u);
+                umma_f16_ts(tmem_base, ta + 16, dbh, w.f.idesc, 1u);
+              } else {
+                const uint32_t a_hi = st + A.off_a, a_lo = a_hi + kATileBytes;
+                const uint64_t dah = umma_smem_desc(a_hi + 32 * kk, 16, 512, kSwizzle64);
+                const uint64_t dal = umma_smem_desc(a_lo + 32 * kk, 16, 512, kSwizzle64);
+                umma_f16(tmem_base, dah, dbh, w.f.idesc, acc);
+                umma_f16(tmem_base, dah, dbl, w.f.idesc, 1u);
+                umma_f16(tmem_base, dal, dbh, w.f.idesc, 1u);
+              }
             }
             umma_commit(&empty[s]);
             issued_any = true;
+            if (++s == S) {
+              s = 0;
+              ph ^= 1;
+            }
           }
-          __syncwarp();
+          if (!ok) break;
+          umma_commit(accf);
         }
-        if (!ok) break;
-        if (lane == 0) umma_commit(accf);
-        __syncwarp();
       }
-    }
-    if (lane == 0 && issued_any) {
-      // All MMAs of this CTA complete before tensor memory is released.
-      umma_commit(fin);
-      mbar_wait_drain(fin, 0);
+      if (issued_any) {
+        // All MMAs of this CTA complete before tensor memory is released.
+        umma_commit(fin);
+        mbar_wait_drain(fin, 0);
+      }
     }
     __syncwarp();
   } else if (warp >= kEpiWarp0 && warp < kEpiWarp0 + 4) {
@@ -402,29 +444,28 @@ __global__ void __launch_bounds__(kThreads, 1) srm_tc_kernel(const TcKernelArgs 
           break;
         }
         tc_fence_after();
-        for (int c0 = 0; c0 < w.f.ntile_n; c0 += 32) {
-          uint32_t v[32];
-          tmem_ld_32x32b_x32(lane_base + c0, v);
+        for (int c0 = 0; c0 < w.f.ntile_n; c0 += 16) {
+          uint32_t v[16];
+          tmem_ld_32x32b_x16(lane_base + c0, v);
           if (!first) {
             // master (FP32, round to nearest) += chunk partial
-            uint32_t m[32];
-            tmem_ld_32x32b_x32(lane_base + 256 + c0, m);
+            uint32_t m[16];
+            tmem_ld_32x32b_x16(lane_base + kMasterCol + c0, m);
             tmem_wait_ld();
 #pragma unroll
-            for (int c = 0; c < 32; ++c)
+            for (int c = 0; c < 16; ++c)
               v[c] = __float_as_uint(__fadd_rn(__uint_as_float(m[c]), __uint_as_float(v[c])));
           } else {
             tmem_wait_ld();
           }
           if (!last) {
-            tmem_st_32x32b_x32(lane_base + 256 + c0, v);
+            tmem_st_32x32b_x16(lane_base + kMasterCol + c0, v);
           } else if (row_ok) {
             // The scaling of scarflib_srm.f90:847, applied once to the sum.
 #pragma unroll
-            for (int c = 0; c < 32; ++c) {
+            for (int c = 0; c < 16; ++c) {
               const int kcol = k0 + c0 + c;
-              if (c0 + c < w.f.ntile_n && kcol < w.f.n3)
-                dst[plane * kcol] = __fmul_rn(__uint_as_float(v[c]), w.f.scaling);
+              if (kcol < w.f.n3) dst[plane * kcol] = __fmul_rn(__uint_as_float(v[c]), w.f.scaling);
             }
           }
         }
@@ -432,13 +473,32 @@ __global__ void __launch_bounds__(kThreads, 1) srm_tc_kernel(const TcKernelArgs 
         tc_fence_before();
         __syncwarp();
         if (lane == 0) mbar_arrive(acce);
+        if (last && A.slab_cnt) {
+          // Count this warp's rows of the item; the last of the slab's
+          // 4 x items arrivals raises the host flag. System-scope fences
+          // order the field stores before the count and the count before
+          // the flag, so the host may copy the slab out as soon as it sees it.
+          __threadfence_system();
+          __syncwarp();
+          if (lane == 0) {
+            const int jb0 = (w.jb / A.slab_jbs) * A.slab_jbs;
+            const int slab = w.nt * A.slab_spn + w.jb / A.slab_jbs;
+            const int expect = 4 * w.f.bi * min(A.slab_jbs, w.f.bj - jb0);
+            if (atomicAdd(&A.slab_cnt[slab], 1) == expect - 1) {
+              __threadfence_system();
+              A.slab_flag[slab] = 1;
+            }
+          }
+        }
       }
     }
   } else if (warp >= kGenWarp0) {
     // -------------------------------------------------------- generators ---
-    const int g = threadIdx.x - kGenWarp0 * 32;  // 0..255
+    // Thread g owns row r of the A tile (TMEM lane r: warp % 4 is the lane
+    // quadrant) and kGenHarm consecutive harmonics of every stage.
+    const int g = threadIdx.x - kGenWarp0 * 32;
     const int r = g & (kRows - 1);
-    const int half = g >> 7;                     // harmonics [8*half, 8*half+8)
+    const int h0 = (g >> 7) * kGenHarm;
     const int ii = r & (A.ti - 1);
     const int jj = r >> A.ti_shift;
     uint32_t cnt = 0;
@@ -458,30 +518,41 @@ __global__ void __launch_bounds__(kThreads, 1) srm_tc_kernel(const TcKernelArgs 
           break;
         }
         uint8_t* st = smem + s * A.stage_bytes;
-        const float2* rt = reinterpret_cast<const float2*>(st + A.off_r);
-        const float2* stt = reinterpret_cast<const float2*>(st + A.off_s);
-        uint8_t* a_hi = st + A.off_a;
-        uint8_t* a_lo = a_hi + kATileBytes;
+        const float2* rt = reinterpret_cast<const float2*>(st + A.off_r) + h0 * A.ti + ii;
+        const float2* stt = reinterpret_cast<const float2*>(st + A.off_s) + h0 * A.tj + jj;
+        __half2 hv[kGenHarm], lv[kGenHarm];
 #pragma unroll
-        for (int cc = 0; cc < 2; ++cc) {
-          const int chunk = half * 2 + cc;
-          __half2 hv[4], lv[4];
-#pragma unroll
-          for (int u = 0; u < 4; ++u) {
-            const int hp = chunk * 4 + u;
-            const float2 x = rt[hp * A.ti + ii];
-            const float2 y = stt[hp * A.tj + jj];
-            const float re = x.x * y.x - x.y * y.y;
-            const float nim = -(x.x * y.y + x.y * y.x);
-            hv[u] = __floats2half2_rn(re, nim);
-            const float2 hf = __half22float2(hv[u]);
-            lv[u] = __floats2half2_rn(re - hf.x, nim - hf.y);
-          }
-          const uint32_t off = swz64(static_cast<uint32_t>(r), static_cast<uint32_t>(chunk));
-          *reinterpret_cast<uint4*>(a_hi + off) = *reinterpret_cast<const uint4*>(hv);
-          *reinterpret_cast<uint4*>(a_lo + off) = *reinterpret_cast<const uint4*>(lv);
+        for (int u = 0; u < kGenHarm; ++u) {
+          const float2 x = rt[u * A.ti];
+          const float2 y = stt[u * A.tj];
+          const float re = x.x * y.x - x.y * y.y;
+          const float nim = -(x.x * y.y + x.y * y.x);
+          hv[u] = __floats2half2_rn(re, nim);
+          const float2 hf = __half22float2(hv[u]);
+          lv[u] = __floats2half2_rn(re - hf.x, nim - hf.y);
         }
-        fence_proxy_async_smem();
+        if constexpr (kTmemA) {
+          // Harmonic h = column h of the stage's hi half (16 + h: lo half).
+          // The slot's previous MMAs completed before its bulk copies were
+          // issued (empty -> full).
+          tc_fence_after();
+          const uint32_t ta = tmem_base + (static_cast<uint32_t>(r & ~31) << 16) + kTmemACol0 +
+                              s * kTmemAStageCols + h0;
+          tmem_st_cols<kGenHarm>(ta, reinterpret_cast<const uint32_t*>(hv));
+          tmem_st_cols<kGenHarm>(ta + 16, reinterpret_cast<const uint32_t*>(lv));
+          tmem_wait_st();
+          tc_fence_before();
+        } else {
+          uint8_t* a_hi = st + A.off_a;
+          uint8_t* a_lo = a_hi + kATileBytes;
+#pragma unroll
+          for (int cc = 0; cc < kGenHarm / 4; ++cc) {
+            const uint32_t off = swz64(static_cast<uint32_t>(r), static_cast<uint32_t>(h0 / 4 + cc));
+            *reinterpret_cast<uint4*>(a_hi + off) = *reinterpret_cast<const uint4*>(hv + 4 * cc);
+            *reinterpret_cast<uint4*>(a_lo + off) = *reinterpret_cast<const uint4*>(lv + 4 * cc);
+          }
+          fence_proxy_async_smem();
+        }
         __syncwarp();
         if (lane == 0) mbar_arrive(&agen[s]);
       }
@@ -506,6 +577,7 @@ int ilog2(int v) {
 // below ~4e-6 of the field's standard deviation at any harmonic count.
 constexpr int kDefaultChunkStages = 32;
 int g_chunk_stages = kDefaultChunkStages;
+bool g_a_in_tmem = false;
 
 TableJob make_job(const scarf_srm_setup& s, const int fs[3], float ds, const float* d_table, int nh,
                   const TcPlan& p, void* d_work) {
@@ -559,19 +631,20 @@ constexpr int kMaxDynSmem = 227 * 1024;
 
 // Shared-memory carve-up for a launch with row tiles ti x tj and column
 // tiles up to ntile_max; returns the dynamic shared-memory size (0 if the
-// ring cannot hold two stages).
-size_t compute_layout(TcKernelArgs& A, int ti, int tj, int ntile_max) {
+// ring cannot hold two stages). With A in tensor memory a stage holds only
+// the B image and the factor tiles, and the ring depth is the TMEM A ring's.
+size_t compute_layout(TcKernelArgs& A, int ti, int tj, int ntile_max, bool tmem_a) {
   A.ti = ti;
   A.tj = tj;
   A.ti_shift = ilog2(ti);
   const uint32_t b_bytes = 2u * ntile_max * kRowBytes;
   A.off_b = 0;
   A.off_a = (b_bytes + 1023u) & ~1023u;
-  A.off_r = A.off_a + 2u * kATileBytes;
+  A.off_r = A.off_a + (tmem_a ? 0u : 2u * kATileBytes);
   A.off_s = A.off_r + kStageHarm * ti * 8u;
   A.stage_bytes = (A.off_s + kStageHarm * tj * 8u + 1023u) & ~1023u;
   const uint32_t budget = kMaxDynSmem - 1024u - 512u;
-  const int nbuf = std::min(8, static_cast<int>(budget / A.stage_bytes));
+  const int nbuf = std::min(tmem_a ? kTmemAStages : 8, static_cast<int>(budget / A.stage_bytes));
   if (nbuf < 2) return 0;
   A.nstage_buf = nbuf;
   A.bars_off = nbuf * A.stage_bytes;
@@ -586,7 +659,9 @@ cudaError_t ensure_smem_attribute() {
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
   if (dev >= 0 && dev < 64 && done[dev]) return cudaSuccess;
-  e = cudaFuncSetAttribute(srm_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
+  e = cudaFuncSetAttribute(srm_tc_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(srm_tc_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
   if (e == cudaSuccess && dev >= 0 && dev < 64) done[dev] = true;
   return e;
 }
@@ -598,7 +673,16 @@ int device_sms() {
   return nsm;
 }
 
+void launch_tc_kernel(const TcKernelArgs& A, bool tmem_a, int grid, size_t smem, cudaStream_t stream) {
+  if (tmem_a)
+    srm_tc_kernel<true><<<grid, kThreads, smem, stream>>>(A);
+  else
+    srm_tc_kernel<false><<<grid, kThreads, smem, stream>>>(A);
+}
+
 }  // namespace
+
+void tc_set_a_in_tmem(int on) { g_a_in_tmem = on != 0; }
 
 void tc_set_chunk_harmonics(int harmonics) {
   g_chunk_stages = harmonics > 0 ? (harmonics + kStageHarm - 1) / kStageHarm : kDefaultChunkStages;
@@ -625,8 +709,10 @@ bool tc_make_plan(int ndim, const int n[3], int nh, TcPlan* P, int tj_force) {
   p.ti = kRows / p.tj;
   p.bi = (p.n1 + p.ti - 1) / p.ti;
   p.bj = (p.n2 + p.tj - 1) / p.tj;
+  p.tmem_a = g_a_in_tmem ? 1 : 0;
+  const int max_n = p.tmem_a ? kMaxNTmemA : kMaxNSmemA;
   const int n3_16 = (p.n3 + 15) / 16 * 16;
-  p.bn = (n3_16 + 255) / 256;
+  p.bn = (n3_16 + max_n - 1) / max_n;
   p.ntile_n = ((p.n3 + p.bn - 1) / p.bn + 15) / 16 * 16;
   p.nh = nh;
   p.nh_pad = (nh + kStageHarm - 1) / kStageHarm * kStageHarm;
@@ -647,9 +733,26 @@ bool tc_make_plan(int ndim, const int n[3], int nh, TcPlan* P, int tj_force) {
   return true;
 }
 
+void tc_slab_layout(const TcPlan& p, int target_items, TcSlabSignal* sig) {
+  sig->jbs = std::max(1, std::min(p.bj, target_items / std::max(1, p.bi)));
+  sig->spn = (p.bj + sig->jbs - 1) / sig->jbs;
+  sig->nslabs = sig->spn * p.bn;
+}
+
+TcSlab tc_slab_extent(const TcPlan& p, const TcSlabSignal& sig, int q) {
+  const int nt = q / sig.spn, jb0 = (q % sig.spn) * sig.jbs;
+  TcSlab e;
+  e.z0 = nt * p.ntile_n;
+  e.z1 = std::min(p.n3, e.z0 + p.ntile_n);
+  e.y0 = jb0 * p.tj;
+  e.y1 = std::min(p.n2, (jb0 + sig.jbs) * p.tj);
+  return e;
+}
+
 cudaError_t launch_tc_structured(const scarf_srm_setup& s, const int fs[3], const int n[3], float ds,
                                  const float* d_table, int nh, float* d_field, void* d_work, const TcPlan& p,
-                                 int* d_status, cudaStream_t stream, cudaEvent_t ev_main0, cudaEvent_t ev_main1) {
+                                 int* d_status, cudaStream_t stream, cudaEvent_t ev_main0, cudaEvent_t ev_main1,
+                                 const TcSlabSignal* slabs) {
   const TableJob T = make_job(s, fs, ds, d_table, nh, p, d_work);
   const int nsm = device_sms();
   tc_build_rs<<<nsm * 8, 256, 0, stream>>>(T, nullptr);
@@ -664,14 +767,22 @@ cudaError_t launch_tc_structured(const scarf_srm_setup& s, const int fs[3], cons
   A.num_items = p.bi * p.bj * p.bn;
   A.status = d_status;
   A.queue = d_status + 1;
-  const size_t smem = compute_layout(A, p.ti, p.tj, p.ntile_n);
+  const size_t smem = compute_layout(A, p.ti, p.tj, p.ntile_n, p.tmem_a != 0);
   if (!smem) return cudaErrorInvalidConfiguration;
   cudaError_t e = ensure_smem_attribute();
   if (e != cudaSuccess) return e;
   e = cudaMemsetAsync(A.queue, 0, sizeof(int), stream);
   if (e != cudaSuccess) return e;
+  if (slabs && slabs->nslabs > 0) {
+    e = cudaMemsetAsync(slabs->d_cnt, 0, sizeof(int) * slabs->nslabs, stream);
+    if (e != cudaSuccess) return e;
+    A.slab_cnt = slabs->d_cnt;
+    A.slab_flag = slabs->flag_dev;
+    A.slab_jbs = slabs->jbs;
+    A.slab_spn = slabs->spn;
+  }
   if (ev_main0) cudaEventRecord(ev_main0, stream);
-  srm_tc_kernel<<<std::min(A.num_items, nsm), kThreads, smem, stream>>>(A);
+  launch_tc_kernel(A, p.tmem_a != 0, std::min(A.num_items, nsm), smem, stream);
   if (ev_main1) cudaEventRecord(ev_main1, stream);
   return cudaGetLastError();
 }
@@ -694,8 +805,9 @@ size_t tc_batch_plan(const TcBatchInput* in, int nfields, TcBatchPlan* out) {
     if (f == 0) {
       ti = p.ti;
       tj = p.tj;
-    } else if (p.ti != ti || p.tj != tj) {
-      return 0;  // one row-tile shape per launch
+      bp.tmem_a = p.tmem_a;
+    } else if (p.ti != ti || p.tj != tj || p.tmem_a != bp.tmem_a) {
+      return 0;  // one row-tile shape and A placement per launch
     }
     ntile_max = std::max(ntile_max, p.ntile_n);
     items += static_cast<long long>(p.bi) * p.bj * p.bn;
@@ -762,10 +874,10 @@ cudaError_t tc_batch_launch(const TcBatchPlan& bp, void* d_work, cudaStream_t st
   A.num_items = bp.num_items;
   A.status = status;
   A.queue = status + 1;
-  const size_t smem = compute_layout(A, bp.ti, bp.tj, bp.ntile_max);
+  const size_t smem = compute_layout(A, bp.ti, bp.tj, bp.ntile_max, bp.tmem_a != 0);
   if (!smem) return cudaErrorInvalidConfiguration;
   if (ev_main0) cudaEventRecord(ev_main0, stream);
-  srm_tc_kernel<<<std::min(bp.num_items, nsm), kThreads, smem, stream>>>(A);
+  launch_tc_kernel(A, bp.tmem_a != 0, std::min(bp.num_items, nsm), smem, stream);
   if (ev_main1) cudaEventRecord(ev_main1, stream);
   return cudaGetLastError();
 }

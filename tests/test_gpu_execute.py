@@ -136,3 +136,38 @@ def test_infeasible_domain_returns_an_error():
     with pytest.raises(sb.ScarfError) as e:
         sb.scarf_execute(1)
     assert e.value.code == sb.SCARF_ERR_ARG
+
+
+@pytest.mark.parametrize("fs,fe,items", [
+    ([2, 3, 1], [150, 130, 290], 3),    # ragged row blocks and column tiles, many slabs
+    ([1, 1, 1], [64, 64, 520], 1),      # default slab size, three column tiles
+    ([1, 1], [300, 600], 2),            # 2D: three column tiles along y
+])
+def test_execute_overlapped_output_matches_serial(fs, fe, items):
+    kw = dict(acf=0, hurst=0.25, sigma=0.05, ds=50.0, cl=[2000.0] * len(fe), method=1)
+    sb.set_form(sb.FORM_TC)
+    sb.scarf_initialize(fs=fs, fe=fe, **kw)
+    try:
+        sb.set_output_overlap(0)
+        serial, st0 = sb.scarf_execute(4321)
+        sb.set_output_overlap(items)
+        overlapped, st1 = sb.scarf_execute(4321)
+    finally:
+        sb.set_output_overlap(1)
+    assert np.array_equal(overlapped.view(np.uint32), serial.view(np.uint32))
+    assert np.array_equal(st0[:4], st1[:4])
+
+
+def test_execute_overlap_falls_back_when_rescaling():
+    fs, fe = [1, 1, 1], [96, 80, 300]
+    sb.set_form(sb.FORM_TC)
+    sb.scarf_initialize(fs=fs, fe=fe, acf=1, ds=50.0, cl=[1500.0] * 3, sigma=0.05, method=1, rescale=1)
+    try:
+        sb.set_output_overlap(0)
+        a, sa = sb.scarf_execute(99)
+        sb.set_output_overlap(2)
+        b, sbb = sb.scarf_execute(99)
+    finally:
+        sb.set_output_overlap(1)
+    assert np.array_equal(a, b) and np.array_equal(sa[:4], sbb[:4])
+    assert sbb[2] == np.float32(0.05)
