@@ -96,12 +96,19 @@ int scarf_set_tc_chunk(int harmonics);
  * field after the kernel. The field is identical either way. */
 int scarf_set_output_overlap(int items_per_slab);
 
-/* Where the tensor-core form keeps its generated A operand, for plans made
- * after the call: 0 = shared memory (default; column tiles <= 256), 1 =
- * tensor memory (column tiles <= 192). Both give identical sums; tensor
- * memory takes the A tile off the shared-memory port but narrows the column
- * tile, so it is slower on the grids measured so far. */
-int scarf_set_tc_a_in_tmem(int on);
+/* Kernel form of the tensor-core sum, for plans made after the call. All
+ * give identical sums (the same products accumulated in the same order per
+ * output point).
+ *   SCARF_TC_SINGLE       (default) one CTA per 128-row tile, A in shared
+ *                         memory;
+ *   SCARF_TC_PAIR         a cluster of two CTAs per 256-row tile,
+ *                         cta_group::2 MMAs, each SM staging half of B;
+ *   SCARF_TC_SINGLE_TMEM_A one CTA per tile, A in tensor memory (column
+ *                         tiles <= 192). */
+#define SCARF_TC_PAIR 0
+#define SCARF_TC_SINGLE 1
+#define SCARF_TC_SINGLE_TMEM_A 2
+int scarf_set_tc_variant(int variant);
 
 /* Status-returning scarf_execute (c_binding.c:138-143); stats[8] as the
  * reference fills it (stats[4] host seconds, stats[5] device seconds). */

@@ -34,7 +34,7 @@ EXPORTED_SYMBOLS = (
     # extended (include/scarf3d_b200.h)
     "scarf_last_error", "scarf_set_nharm", "scarf_get_nharm", "scarf_set_form",
     "scarf_set_uniform_source", "scarf_set_stream", "scarf_set_host_threads", "scarf_set_kernel_timing",
-    "scarf_last_kernel_ms", "scarf_set_tc_chunk", "scarf_set_tc_a_in_tmem", "scarf_set_output_overlap",
+    "scarf_last_kernel_ms", "scarf_set_tc_chunk", "scarf_set_tc_variant", "scarf_set_output_overlap",
     "scarf_execute_ex",
     "scarf_srm_compute_setup", "scarf_srm_sample", "scarf_srm_sample_device", "scarf_set_sampler",
     "scarf_set_sampler_pass_pairs",
@@ -115,7 +115,7 @@ def _load() -> ctypes.CDLL:
         "scarf_set_kernel_timing": (c_int, [c_int]),
         "scarf_last_kernel_ms": (c_float, []),
         "scarf_set_tc_chunk": (c_int, [c_int]),
-        "scarf_set_tc_a_in_tmem": (c_int, [c_int]),
+        "scarf_set_tc_variant": (c_int, [c_int]),
         "scarf_set_output_overlap": (c_int, [c_int]),
         "scarf_execute_ex": (c_int, [c_int, c_void_p, fp, c_int]),
         "scarf_srm_compute_setup": (c_int, [ctypes.POINTER(SrmParams), ctypes.POINTER(SrmSetup)]),
@@ -343,10 +343,13 @@ def set_form(form: int):
     check(lib.scarf_set_form(int(form)))
 
 
-def set_tc_a_in_tmem(on: bool):
-    """Tensor-core form: generated A operand in tensor memory (True) or
-    shared memory (False, the default); applies to plans made afterwards."""
-    check(lib.scarf_set_tc_a_in_tmem(1 if on else 0))
+TC_PAIR, TC_SINGLE, TC_SINGLE_TMEM_A = 0, 1, 2
+
+
+def set_tc_variant(variant: int):
+    """Tensor-core kernel form for plans made afterwards: TC_SINGLE (default),
+    TC_PAIR (CTA pairs with cta_group::2 MMAs) or TC_SINGLE_TMEM_A."""
+    check(lib.scarf_set_tc_variant(int(variant)))
 
 
 def set_output_overlap(items_per_slab: int = 1):

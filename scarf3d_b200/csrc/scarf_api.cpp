@@ -931,9 +931,11 @@ int scarf_set_output_overlap(int items_per_slab) {
   return SCARF_OK;
 }
 
-int scarf_set_tc_a_in_tmem(int on) {
+int scarf_set_tc_variant(int variant) {
+  if (variant != SCARF_TC_PAIR && variant != SCARF_TC_SINGLE && variant != SCARF_TC_SINGLE_TMEM_A)
+    return fail(SCARF_ERR_ARG, "unknown tensor-core variant %d", variant);
   std::lock_guard<std::mutex> lk(g_mu);
-  tc_set_a_in_tmem(on);
+  tc_set_variant(variant);
   return SCARF_OK;
 }
 

@@ -33,12 +33,17 @@ struct TcPlan {
   int stages;            // nh_pad / kStageHarm
   int chunk_stages;      // stages per TMEM accumulation chunk (FP32 sum of chunks)
   int tmem_a;            // 1: A operand generated into tensor memory (ntile_n <= 192)
+  int pair;              // 1: CTA-pair form (M = 256 over two SMs, each holding half of B)
+  int pair_i;            // pairs split along i (when bj == 1) instead of j
+  int bix, bjx;          // item grid (bi x bj, halved along the pair axis, rounded up)
   size_t off_r, off_s, off_c, off_status, bytes;  // workspace layout
 };
 
-// Placement of the generated A operand for plans made from now on: 0 shared
-// memory (default), 1 tensor memory.
-void tc_set_a_in_tmem(int on);
+// Kernel form for plans made from now on (SCARF_TC_* of scarf3d_b200.h).
+constexpr int kTcVariantPair = 0;         // cta_group::2 pairs, A in shared memory
+constexpr int kTcVariantSingle = 1;       // one CTA per tile, A in shared memory (default)
+constexpr int kTcVariantSingleTmemA = 2;  // one CTA per tile, A in tensor memory
+void tc_set_variant(int v);
 
 // tj_force > 0 fixes the row tile to (128 / tj_force) x tj_force.
 bool tc_make_plan(int ndim, const int n[3], int nh, TcPlan* plan, int tj_force = 0);
@@ -80,7 +85,7 @@ struct TcBatchInput {
   int tj;  // row-tile shape (0 = automatic)
 };
 struct TcBatchPlan {
-  int nfields = 0, num_items = 0, ti = 0, tj = 0, ntile_max = 0, tmem_a = 0;
+  int nfields = 0, num_items = 0, ti = 0, tj = 0, ntile_max = 0, tmem_a = 0, pair = 0;
   size_t off_fields = 0, off_jobs = 0, off_items = 0, off_status = 0, bytes = 0;
   std::vector<TcPlan> plans;
   std::vector<size_t> field_off;

@@ -58,11 +58,13 @@ __host__ __device__ constexpr uint32_t swz64(uint32_t row, uint32_t chunk) {
 struct TcField {
   int n1, n2, n3;
   int bi, bj, ntile_n, stages, chunk_stages;
+  int bix, bjx;         // item grid: bi x bj, or CTA pairs along j (bi x ceil(bj/2)) or i (ceil(bi/2) x bj)
+  int pair_i;           // CTA pairs split along i (2D fields: one row block along j)
   uint32_t idesc;
   float scaling;
   const float2* rimg;   // [bi][stages][16][ti]
   const float2* simg;   // [bj][stages][16][tj]
-  const uint8_t* cimg;  // [bn][stages][hi,lo][ntile_n * 64 B]
+  const uint8_t* cimg;  // [bn][stages][part][hi,lo][ntile_n / parts * 64 B]
   float* field;
 };
 
@@ -76,6 +78,9 @@ struct TcKernelArgs {
   int ti, tj, ti_shift;   // row-tile shape (uniform over a launch)
   int nstage_buf;
   uint32_t stage_bytes, off_b, off_a, off_r, off_s, bars_off;
+  // CTA-pair layout only: a separate ring of nrs factor-tile (R, S) slots.
+  int nrs;
+  uint32_t rs_base, rs_bytes;
   // Slab completion signal (single-field launches; null otherwise): a slab
   // is one column tile x a run of slab_jbs row blocks along j, contiguous
   // pieces of the field that the host copies out while the kernel runs.
@@ -92,7 +97,8 @@ struct TableJob {
   double ds;
   int off[3];            // coordinate of 0-based index t on axis a: (t + off[a]) * ds
   int ax_r, ax_s, ax_c;  // physical axis of the row-fast, row-slow and column factors
-  int n1, n2, n3, ti, tj, bi, bj, ntile_n, bn;
+  int n1, n2, n3, ti, tj, bi, bj, ntile_n, bn;  // bj: S-image blocks (even for CTA pairs)
+  int parts;             // column image split: 1, or 2 halves (one per CTA of a pair)
   float2* rimg;
   float2* simg;
   uint8_t* cimg;
@@ -163,6 +169,8 @@ __global__ void tc_build_c(const TableJob j0, const TableJob* jobs) {
     const int k = static_cast<int>(q2 % T.stages);
     const int nb = static_cast<int>(q2 / T.stages);
     const int col = nb * T.ntile_n + row;
+    const int part_rows = T.ntile_n / T.parts;
+    const int part = row / part_rows, prow = row - part * part_rows;
     __half2 hi[4], lo[4];
 #pragma unroll
     for (int u = 0; u < 4; ++u) {
@@ -181,10 +189,11 @@ __global__ void tc_build_c(const TableJob j0, const TableJob* jobs) {
       const float2 hf = __half22float2(hi[u]);
       lo[u] = __floats2half2_rn(cs32 - hf.x, sn32 - hf.y);
     }
-    uint8_t* base = T.cimg + (static_cast<size_t>(nb) * T.stages + k) * (2u * T.ntile_n * kRowBytes);
-    const uint32_t off = swz64(static_cast<uint32_t>(row), static_cast<uint32_t>(chunk));
+    uint8_t* base = T.cimg + ((static_cast<size_t>(nb) * T.stages + k) * T.parts + part) *
+                                 (2u * part_rows * kRowBytes);
+    const uint32_t off = swz64(static_cast<uint32_t>(prow), static_cast<uint32_t>(chunk));
     *reinterpret_cast<uint4*>(base + off) = *reinterpret_cast<const uint4*>(hi);
-    *reinterpret_cast<uint4*>(base + static_cast<size_t>(T.ntile_n) * kRowBytes + off) =
+    *reinterpret_cast<uint4*>(base + static_cast<size_t>(part_rows) * kRowBytes + off) =
         *reinterpret_cast<const uint4*>(lo);
   }
 }
@@ -204,12 +213,104 @@ __device__ __forceinline__ Item decode_item(const TcKernelArgs& A, int idx) {
     local = e.y;
   }
   it.f = A.fields ? A.fields[fid] : A.f0;
-  const int tiles_m = it.f.bi * it.f.bj;
+  const int tiles_m = it.f.bix * it.f.bjx;
   it.nt = local / tiles_m;
   const int mt = local - it.nt * tiles_m;
-  it.ib = mt % it.f.bi;
-  it.jb = mt / it.f.bi;
+  it.ib = mt % it.f.bix;
+  it.jb = mt / it.f.bix;
   return it;
+}
+
+// W (16 or 32) columns of a chunk drain: all TMEM loads issued before one
+// wait, so each round trip to tensor memory covers W columns.
+template <int W>
+__device__ __forceinline__ void drain_cols(uint32_t lane_base, uint32_t master_col, int c0, bool first, bool last,
+                                           bool row_ok, float* dst, long long plane, int k0, int n3, float scaling) {
+  uint32_t v[W], m[W];
+#pragma unroll
+  for (int h = 0; h < W / 16; ++h) {
+    tmem_ld_32x32b_x16(lane_base + c0 + 16 * h, *reinterpret_cast<uint32_t(*)[16]>(v + 16 * h));
+    if (!first) tmem_ld_32x32b_x16(lane_base + master_col + c0 + 16 * h, *reinterpret_cast<uint32_t(*)[16]>(m + 16 * h));
+  }
+  tmem_wait_ld();
+  if (!first) {
+#pragma unroll
+    for (int c = 0; c < W; ++c) v[c] = __float_as_uint(__fadd_rn(__uint_as_float(m[c]), __uint_as_float(v[c])));
+  }
+  if (!last) {
+#pragma unroll
+    for (int h = 0; h < W / 16; ++h)
+      tmem_st_32x32b_x16(lane_base + master_col + c0 + 16 * h, *reinterpret_cast<const uint32_t(*)[16]>(v + 16 * h));
+  } else if (row_ok) {
+    // The scaling of scarflib_srm.f90:847, applied once to the sum.
+#pragma unroll
+    for (int c = 0; c < W; ++c) {
+      const int kcol = k0 + c0 + c;
+      if (kcol < n3) dst[plane * kcol] = __fmul_rn(__uint_as_float(v[c]), scaling);
+    }
+  }
+}
+
+// One chunk drain of the epilogue for the 32 rows of this warp: the TMEM
+// chunk accumulator is added (round to nearest) into the FP32 master at
+// master_col, or, for the last chunk, master + chunk is scaled and stored.
+__device__ __forceinline__ void drain_chunk(uint32_t lane_base, uint32_t master_col, int ntile_n, bool first,
+                                            bool last, bool row_ok, float* dst, long long plane, int k0, int n3,
+                                            float scaling) {
+  int c0 = 0;
+  for (; c0 + 32 <= ntile_n; c0 += 32)
+    drain_cols<32>(lane_base, master_col, c0, first, last, row_ok, dst, plane, k0, n3, scaling);
+  if (c0 < ntile_n) drain_cols<16>(lane_base, master_col, c0, first, last, row_ok, dst, plane, k0, n3, scaling);
+  if (!last) tmem_wait_st();
+}
+
+// Slab accounting after a warp stored its 32 rows of row tile (ib, jb) of
+// column tile nt: the last of the slab's 4 x tiles arrivals raises the host
+// flag. System-scope fences order the field stores before the count and the
+// count before the flag, so the host may copy the slab out once it sees it.
+__device__ __forceinline__ void signal_slab(const TcKernelArgs& A, const TcField& f, int ib, int jb, int nt,
+                                            int lane) {
+  __threadfence_system();
+  __syncwarp();
+  if (lane == 0 && ib < f.bi && jb < f.bj) {
+    const int jb0 = (jb / A.slab_jbs) * A.slab_jbs;
+    const int slab = nt * A.slab_spn + jb / A.slab_jbs;
+    const int expect = 4 * f.bi * min(A.slab_jbs, f.bj - jb0);
+    if (atomicAdd(&A.slab_cnt[slab], 1) == expect - 1) {
+      __threadfence_system();
+      A.slab_flag[slab] = 1;
+    }
+  }
+}
+
+// A operand of one stage into shared memory: row r of the tile (the
+// (ii, jj) point of the row block), kGenHarm harmonics from h0, FP16 hi and lo
+// images in the 64-B-swizzled K-major layout.
+__device__ __forceinline__ void generate_a_smem(const TcKernelArgs& A, uint8_t* st, const uint8_t* rs, int r, int ii,
+                                                int jj, int h0) {
+  // rs: the stage's R tile [16][ti] followed by its S tile [16][tj] (float2)
+  const float2* rt = reinterpret_cast<const float2*>(rs) + h0 * A.ti + ii;
+  const float2* stt = reinterpret_cast<const float2*>(rs) + kStageHarm * A.ti + h0 * A.tj + jj;
+  __half2 hv[kGenHarm], lv[kGenHarm];
+#pragma unroll
+  for (int u = 0; u < kGenHarm; ++u) {
+    const float2 x = rt[u * A.ti];
+    const float2 y = stt[u * A.tj];
+    const float re = x.x * y.x - x.y * y.y;
+    const float nim = -(x.x * y.y + x.y * y.x);
+    hv[u] = __floats2half2_rn(re, nim);
+    const float2 hf = __half22float2(hv[u]);
+    lv[u] = __floats2half2_rn(re - hf.x, nim - hf.y);
+  }
+  uint8_t* a_hi = st + A.off_a;
+  uint8_t* a_lo = a_hi + kATileBytes;
+#pragma unroll
+  for (int cc = 0; cc < kGenHarm / 4; ++cc) {
+    const uint32_t off = swz64(static_cast<uint32_t>(r), static_cast<uint32_t>(h0 / 4 + cc));
+    *reinterpret_cast<uint4*>(a_hi + off) = *reinterpret_cast<const uint4*>(hv + 4 * cc);
+    *reinterpret_cast<uint4*>(a_lo + off) = *reinterpret_cast<const uint4*>(lv + 4 * cc);
+  }
+  fence_proxy_async_smem();
 }
 
 // TMEM columns (512 allocated). Shared-memory A: chunk accumulator [0, 256),
@@ -277,7 +378,7 @@ __global__ void __launch_bounds__(kThreads, 1) srm_tc_kernel(const TcKernelArgs 
   // queue is exhausted). Lane 0 of each consumer warp acknowledges the slot.
   auto next_item = [&](uint32_t it, int& idx) -> bool {
     const int q = it % kItemRing;
-    if (!mbar_wait_bounded(&item_full[q], (it / kItemRing) & 1, A.status)) return false;
+    if (!warp_wait_bounded(&item_full[q], (it / kItemRing) & 1, A.status, false)) return false;
     idx = *reinterpret_cast<volatile int*>(&item_slot[q]);
     __syncwarp();
     if (lane == 0) mbar_arrive(&item_empty[q]);
@@ -439,57 +540,16 @@ __global__ void __launch_bounds__(kThreads, 1) srm_tc_kernel(const TcKernelArgs 
       for (int s0 = 0; s0 < w.f.stages; s0 += w.f.chunk_stages, ++chunk) {
         const bool first = (s0 == 0);
         const bool last = (s0 + w.f.chunk_stages >= w.f.stages);
-        if (!mbar_wait_bounded(accf, chunk & 1, A.status)) {
+        if (!warp_wait_bounded(accf, chunk & 1, A.status, false)) {
           ok = false;
           break;
         }
         tc_fence_after();
-        for (int c0 = 0; c0 < w.f.ntile_n; c0 += 16) {
-          uint32_t v[16];
-          tmem_ld_32x32b_x16(lane_base + c0, v);
-          if (!first) {
-            // master (FP32, round to nearest) += chunk partial
-            uint32_t m[16];
-            tmem_ld_32x32b_x16(lane_base + kMasterCol + c0, m);
-            tmem_wait_ld();
-#pragma unroll
-            for (int c = 0; c < 16; ++c)
-              v[c] = __float_as_uint(__fadd_rn(__uint_as_float(m[c]), __uint_as_float(v[c])));
-          } else {
-            tmem_wait_ld();
-          }
-          if (!last) {
-            tmem_st_32x32b_x16(lane_base + kMasterCol + c0, v);
-          } else if (row_ok) {
-            // The scaling of scarflib_srm.f90:847, applied once to the sum.
-#pragma unroll
-            for (int c = 0; c < 16; ++c) {
-              const int kcol = k0 + c0 + c;
-              if (kcol < w.f.n3) dst[plane * kcol] = __fmul_rn(__uint_as_float(v[c]), w.f.scaling);
-            }
-          }
-        }
-        if (!last) tmem_wait_st();
+        drain_chunk(lane_base, kMasterCol, w.f.ntile_n, first, last, row_ok, dst, plane, k0, w.f.n3, w.f.scaling);
         tc_fence_before();
         __syncwarp();
         if (lane == 0) mbar_arrive(acce);
-        if (last && A.slab_cnt) {
-          // Count this warp's rows of the item; the last of the slab's
-          // 4 x items arrivals raises the host flag. System-scope fences
-          // order the field stores before the count and the count before
-          // the flag, so the host may copy the slab out as soon as it sees it.
-          __threadfence_system();
-          __syncwarp();
-          if (lane == 0) {
-            const int jb0 = (w.jb / A.slab_jbs) * A.slab_jbs;
-            const int slab = w.nt * A.slab_spn + w.jb / A.slab_jbs;
-            const int expect = 4 * w.f.bi * min(A.slab_jbs, w.f.bj - jb0);
-            if (atomicAdd(&A.slab_cnt[slab], 1) == expect - 1) {
-              __threadfence_system();
-              A.slab_flag[slab] = 1;
-            }
-          }
-        }
+        if (last && A.slab_cnt) signal_slab(A, w.f, w.ib, w.jb, w.nt, lane);
       }
     }
   } else if (warp >= kGenWarp0) {
@@ -513,7 +573,7 @@ __global__ void __launch_bounds__(kThreads, 1) srm_tc_kernel(const TcKernelArgs 
       for (int k = 0; k < stages; ++k, ++cnt) {
         const int s = cnt % S;
         const uint32_t ph = (cnt / S) & 1;
-        if (!mbar_wait_bounded(&full[s], ph, A.status)) {
+        if (!warp_wait_bounded(&full[s], ph, A.status, false)) {
           ok = false;
           break;
         }
@@ -567,6 +627,399 @@ __global__ void __launch_bounds__(kThreads, 1) srm_tc_kernel(const TcKernelArgs 
   }
 }
 
+// -------------------------------------------------------- CTA-pair kernel --
+// The tile of a work item is split over the two CTAs of a cluster: 256 rows
+// (row blocks jb = 2 jbp + rank, or ib = 2 ibp + rank when the field has a
+// single row block along j) x N columns. Each CTA generates its 128 rows of
+// A, stages half of the B image (N / 2 rows) and drains its own accumulators;
+// the even CTA issues one cta_group::2 MMA per K step for both. Per SM this
+// halves the B traffic of the one-CTA form, and the pair MMA runs at the
+// tensor core's full rate down to small N.
+//
+// Two rings per CTA decouple the inputs: the small factor tiles (R, S) run
+// up to nrs stages ahead so the generators never wait on copies, and the
+// A / B stage ring (nstage_buf slots) feeds the MMA.
+//
+// Barriers (the same offsets in both CTAs):
+//   item ring    the even CTA's R/S producer takes items from the queue and
+//                publishes each in both CTAs; the other consumers of both
+//                CTAs release slots on the even CTA's item_empty.
+//   rs_full/rs_empty[r]  local: R/S tiles of stage r landed / consumed.
+//   b_full[s]    local: this CTA's B half of stage s landed.
+//   agen[s]      local generators wrote stage s's A rows; the even CTA's
+//                also counts the odd CTA's forwarder, which relays the odd
+//                CTA's agen[s] and b_full[s] with one cluster-scope arrive.
+//   empty[s]     both: the pair MMAs of stage s completed (multicast commit).
+//   accf         both: a chunk is accumulated (multicast commit).
+//   acce         even CTA: the epilogues of both CTAs drained the chunk.
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1) srm_tc_pair_kernel(const TcKernelArgs A) {
+  constexpr uint32_t kMasterCol = kMaxNSmemA;
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  const int S = A.nstage_buf;
+  const int NR = A.nrs;
+  uint64_t* b_full = reinterpret_cast<uint64_t*>(smem + A.bars_off);
+  uint64_t* agen = b_full + S;
+  uint64_t* empty = agen + S;
+  uint64_t* rs_full = empty + S;
+  uint64_t* rs_empty = rs_full + NR;
+  uint64_t* accf = rs_empty + NR;
+  uint64_t* acce = accf + 1;
+  uint64_t* fin = acce + 1;
+  uint64_t* item_full = fin + 1;
+  uint64_t* item_empty = item_full + kItemRing;
+  int* item_slot = reinterpret_cast<int*>(item_empty + kItemRing);
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(item_slot + kItemRing);
+
+  const int warp = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31;
+  const uint32_t rank = cluster_ctarank();
+  const bool even = rank == 0;
+  // Consumers of one item: B producers (2), the even CTA's MMA thread, the
+  // odd CTA's R/S producer and forwarder, epilogue (2 x 4) and generator
+  // (2 x kGenWarps) warps. The even CTA's R/S producer publishes.
+  constexpr int kPairConsumers = 2 + 1 + 2 + 2 * 4 + 2 * kGenWarps;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < S; ++s) {
+      mbar_init(&b_full[s], 1);
+      mbar_init(&agen[s], even ? kGenWarps + 1 : kGenWarps);
+      mbar_init(&empty[s], 1);
+    }
+    for (int r = 0; r < NR; ++r) {
+      mbar_init(&rs_full[r], 1);
+      mbar_init(&rs_empty[r], kGenWarps);
+    }
+    mbar_init(accf, 1);
+    mbar_init(acce, 8);
+    mbar_init(fin, 1);
+    for (int q = 0; q < kItemRing; ++q) {
+      mbar_init(&item_full[q], 1);
+      mbar_init(&item_empty[q], kPairConsumers);
+    }
+    fence_mbar_init();
+  }
+  if (warp == 2) {
+    tmem_alloc_pair(tmem_slot, 512);
+    tmem_relinquish_pair();
+  }
+  tc_fence_before();
+  __syncthreads();
+  cluster_sync_all();  // barrier initialisation and TMEM of both CTAs visible to the pair
+  tc_fence_after();
+  const uint32_t tmem_base = *tmem_slot;
+  bool ok = true;
+
+  const uint32_t agen0 = cluster_map(agen, 0);
+  const uint32_t acce0 = cluster_map(acce, 0);
+  const uint32_t item_empty0 = cluster_map(item_empty, 0);
+
+  // Item ring, consumer side (one thread or a whole warp).
+  auto take_item = [&](uint32_t it, int& idx) -> bool {
+    const int q = it % kItemRing;
+    if (!mbar_wait_bounded_cluster(&item_full[q], (it / kItemRing) & 1, A.status)) return false;
+    idx = *reinterpret_cast<volatile int*>(&item_slot[q]);
+    return true;
+  };
+  auto release_item = [&](uint32_t it) { mbar_arrive_cluster(item_empty0 + 8u * (it % kItemRing)); };
+  // Whole-warp consumers: lane 0 waits and releases, the warp shares the item.
+  auto take_item_warp = [&](uint32_t it, int& idx) -> bool {
+    const int q = it % kItemRing;
+    if (!warp_wait_bounded(&item_full[q], (it / kItemRing) & 1, A.status, true)) return false;
+    idx = *reinterpret_cast<volatile int*>(&item_slot[q]);
+    __syncwarp();
+    if (lane == 0) release_item(it);
+    return true;
+  };
+  auto tile_of = [&](const Item& w, int& ib, int& jb) {
+    ib = w.f.pair_i ? 2 * w.ib + static_cast<int>(rank) : w.ib;
+    jb = w.f.pair_i ? w.jb : 2 * w.jb + static_cast<int>(rank);
+  };
+
+  if (warp == 2) {
+    // ------------------------------------------------- R / S producer ------
+    if (lane == 0) {
+      int r = 0;
+      uint32_t rph = 0, issued = 0;
+      const uint32_t peer_full = cluster_map(item_full, 1);
+      const uint32_t peer_slot = cluster_map(item_slot, 1);
+      for (uint32_t it = 0; ok; ++it) {
+        const int q = it % kItemRing;
+        int idx;
+        if (even) {
+          if (!mbar_wait_bounded_cluster(&item_empty[q], ((it / kItemRing) & 1) ^ 1, A.status)) {
+            ok = false;
+            break;
+          }
+          idx = atomicAdd(A.queue, 1);
+          if (idx >= A.num_items) idx = -1;
+          item_slot[q] = idx;
+          st_cluster_u32(peer_slot + 4u * q, static_cast<uint32_t>(idx));
+          mbar_arrive(&item_full[q]);
+          mbar_arrive_cluster(peer_full + 8u * q);  // release: the remote slot store first
+        } else {
+          if (!take_item(it, idx)) {
+            ok = false;
+            break;
+          }
+          release_item(it);
+        }
+        if (idx < 0) break;
+        const Item w = decode_item(A, idx);
+        int ib, jb;
+        tile_of(w, ib, jb);
+        const uint32_t rbytes = kStageHarm * A.ti * 8u;
+        const uint32_t sbytes = kStageHarm * A.tj * 8u;
+        const float2* rsrc = w.f.rimg + static_cast<size_t>(ib) * w.f.stages * kStageHarm * A.ti;
+        const float2* ssrc = w.f.simg + static_cast<size_t>(jb) * w.f.stages * kStageHarm * A.tj;
+        for (int k = 0; k < w.f.stages; ++k) {
+          if (!mbar_wait_bounded(&rs_empty[r], rph ^ 1, A.status)) {
+            ok = false;
+            break;
+          }
+          uint8_t* rs = smem + A.rs_base + r * A.rs_bytes;
+          mbar_arrive_expect_tx(&rs_full[r], rbytes + sbytes);
+          bulk_g2s(rs, rsrc + static_cast<size_t>(k) * kStageHarm * A.ti, rbytes, &rs_full[r]);
+          bulk_g2s(rs + rbytes, ssrc + static_cast<size_t>(k) * kStageHarm * A.tj, sbytes, &rs_full[r]);
+          ++issued;
+          if (++r == NR) {
+            r = 0;
+            rph ^= 1;
+          }
+        }
+      }
+      if (!ok) {
+        const uint32_t n_in_flight = issued < static_cast<uint32_t>(NR) ? issued : NR;
+        for (uint32_t b = 1; b <= n_in_flight; ++b) {
+          const uint32_t c = issued - b;
+          mbar_wait_drain(&rs_full[c % NR], (c / NR) & 1);
+        }
+      }
+    }
+    __syncwarp();
+  } else if (warp == 0) {
+    // ------------------------------------------------------ B producer -----
+    if (lane == 0) {
+      int s = 0;
+      uint32_t ph = 0, issued = 0;
+      for (uint32_t it = 0; ok; ++it) {
+        int idx;
+        if (!take_item(it, idx)) {
+          ok = false;
+          break;
+        }
+        release_item(it);
+        if (idx < 0) break;
+        const Item w = decode_item(A, idx);
+        const uint32_t bbytes = w.f.ntile_n * kRowBytes;  // this CTA's half: N / 2 rows, hi and lo
+        const uint8_t* csrc = w.f.cimg + (static_cast<size_t>(w.nt) * w.f.stages * 2 + rank) * bbytes;
+        for (int k = 0; k < w.f.stages; ++k) {
+          if (!mbar_wait_bounded_cluster(&empty[s], ph ^ 1, A.status)) {
+            ok = false;
+            break;
+          }
+          mbar_arrive_expect_tx(&b_full[s], bbytes);
+          bulk_g2s(smem + s * A.stage_bytes + A.off_b, csrc + static_cast<size_t>(k) * 2 * bbytes, bbytes, &b_full[s]);
+          ++issued;
+          if (++s == S) {
+            s = 0;
+            ph ^= 1;
+          }
+        }
+      }
+      if (!ok) {
+        const uint32_t n_in_flight = issued < static_cast<uint32_t>(S) ? issued : S;
+        for (uint32_t b = 1; b <= n_in_flight; ++b) {
+          const uint32_t c = issued - b;
+          mbar_wait_drain(&b_full[c % S], (c / S) & 1);
+        }
+      }
+    }
+    __syncwarp();
+  } else if (warp == 1) {
+    // ------------------------------------------- MMA issuer (even CTA) -----
+    if (even && lane == 0) {
+      int s = 0;
+      uint32_t ph = 0, chunk = 0;
+      bool issued_any = false;
+      for (uint32_t it = 0; ok; ++it) {
+        int idx;
+        if (!take_item(it, idx)) {
+          ok = false;
+          break;
+        }
+        release_item(it);
+        if (idx < 0) break;
+        const Item w = decode_item(A, idx);
+        const uint32_t b_lo_off = A.off_b + (w.f.ntile_n / 2) * kRowBytes;
+        for (int c0 = 0; c0 < w.f.stages && ok; c0 += w.f.chunk_stages, ++chunk) {
+          const int c1 = min(w.f.stages, c0 + w.f.chunk_stages);
+          if (chunk > 0 && !mbar_wait_bounded_cluster(acce, (chunk - 1) & 1, A.status)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          for (int k = c0; k < c1; ++k) {
+            if (!mbar_wait_bounded(&b_full[s], ph, A.status) || !mbar_wait_bounded_cluster(&agen[s], ph, A.status)) {
+              ok = false;
+              break;
+            }
+            tc_fence_after();
+            const uint32_t st = smem_u32(smem + s * A.stage_bytes);
+            const uint32_t a_hi = st + A.off_a, a_lo = a_hi + kATileBytes;
+            const uint32_t b_hi = st + A.off_b, b_lo = st + b_lo_off;
+#pragma unroll
+            for (int kk = 0; kk < 2; ++kk) {
+              const uint64_t dah = umma_smem_desc(a_hi + 32 * kk, 16, 512, kSwizzle64);
+              const uint64_t dal = umma_smem_desc(a_lo + 32 * kk, 16, 512, kSwizzle64);
+              const uint64_t dbh = umma_smem_desc(b_hi + 32 * kk, 16, 512, kSwizzle64);
+              const uint64_t dbl = umma_smem_desc(b_lo + 32 * kk, 16, 512, kSwizzle64);
+              umma_f16_pair(tmem_base, dah, dbh, w.f.idesc, (k > c0 || kk > 0) ? 1u : 0u);
+              umma_f16_pair(tmem_base, dah, dbl, w.f.idesc, 1u);
+              umma_f16_pair(tmem_base, dal, dbh, w.f.idesc, 1u);
+            }
+            umma_commit_pair_both(&empty[s]);
+            issued_any = true;
+            if (++s == S) {
+              s = 0;
+              ph ^= 1;
+            }
+          }
+          if (!ok) break;
+          umma_commit_pair_both(accf);
+        }
+      }
+      if (issued_any) {
+        umma_commit_pair_local(fin);
+        mbar_wait_drain(fin, 0);
+      }
+    }
+    __syncwarp();
+  } else if (warp == 3) {
+    // ------------------------------------------- forwarder (odd CTA) -------
+    // One cluster-scope arrive per stage on the even CTA's agen[s] once this
+    // CTA's A rows and B half of stage s are in place.
+    if (!even && lane == 0) {
+      int s = 0;
+      uint32_t ph = 0;
+      for (uint32_t it = 0; ok; ++it) {
+        int idx;
+        if (!take_item(it, idx)) {
+          ok = false;
+          break;
+        }
+        release_item(it);
+        if (idx < 0) break;
+        const int stages = (A.fields ? A.fields[A.items ? A.items[idx].x : 0] : A.f0).stages;
+        for (int k = 0; k < stages; ++k) {
+          if (!mbar_wait_bounded(&agen[s], ph, A.status) || !mbar_wait_bounded(&b_full[s], ph, A.status)) {
+            ok = false;
+            break;
+          }
+          // This CTA's A rows (generic stores, proxy fence, local release)
+          // and B half (bulk-copy completion) are in place: a plain signal
+          // suffices, and only this SM's tensor core reads them.
+          mbar_arrive_cluster_relaxed(agen0 + 8u * s);
+          if (++s == S) {
+            s = 0;
+            ph ^= 1;
+          }
+        }
+      }
+    }
+    __syncwarp();
+  } else if (warp >= kEpiWarp0 && warp < kEpiWarp0 + 4) {
+    // --------------------------------------------------------- epilogue ----
+    const int q = warp & 3;
+    const int r = q * 32 + lane;
+    const int ii = r & (A.ti - 1);
+    const int jj = r >> A.ti_shift;
+    const uint32_t lane_base = tmem_base + (static_cast<uint32_t>(q * 32) << 16);
+    uint32_t chunk = 0;
+    for (uint32_t it = 0; ok; ++it) {
+      int idx;
+      if (!take_item_warp(it, idx)) {
+        ok = false;
+        break;
+      }
+      if (idx < 0) break;
+      const Item w = decode_item(A, idx);
+      int ib, jb;
+      tile_of(w, ib, jb);
+      const int i = ib * A.ti + ii;
+      const int j = jb * A.tj + jj;
+      const bool row_ok = (i < w.f.n1) && (j < w.f.n2);
+      const long long plane = static_cast<long long>(w.f.n1) * w.f.n2;
+      float* dst = w.f.field + i + static_cast<long long>(w.f.n1) * j;
+      const int k0 = w.nt * w.f.ntile_n;
+      for (int s0 = 0; s0 < w.f.stages; s0 += w.f.chunk_stages, ++chunk) {
+        const bool first = (s0 == 0);
+        const bool last = (s0 + w.f.chunk_stages >= w.f.stages);
+        if (!warp_wait_bounded(accf, chunk & 1, A.status, true)) {
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        drain_chunk(lane_base, kMasterCol, w.f.ntile_n, first, last, row_ok, dst, plane, k0, w.f.n3, w.f.scaling);
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive_cluster(acce0);
+        if (last && A.slab_cnt) signal_slab(A, w.f, ib, jb, w.nt, lane);
+      }
+    }
+  } else if (warp >= kGenWarp0) {
+    // -------------------------------------------------------- generators ---
+    const int g = threadIdx.x - kGenWarp0 * 32;
+    const int r = g & (kRows - 1);
+    const int h0 = (g >> 7) * kGenHarm;
+    const int ii = r & (A.ti - 1);
+    const int jj = r >> A.ti_shift;
+    int s = 0, rr = 0;
+    uint32_t ph = 0, rph = 0;
+    for (uint32_t it = 0; ok; ++it) {
+      int idx;
+      if (!take_item_warp(it, idx)) {
+        ok = false;
+        break;
+      }
+      if (idx < 0) break;
+      const int stages = (A.fields ? A.fields[A.items ? A.items[idx].x : 0] : A.f0).stages;
+      for (int k = 0; k < stages; ++k) {
+        // factor tiles in place, and the A slot's previous MMAs complete
+        if (!warp_wait_bounded(&rs_full[rr], rph, A.status, false) ||
+            !warp_wait_bounded(&empty[s], ph ^ 1, A.status, true)) {
+          ok = false;
+          break;
+        }
+        generate_a_smem(A, smem + s * A.stage_bytes, smem + A.rs_base + rr * A.rs_bytes, r, ii, jj, h0);
+        __syncwarp();
+        if (lane == 0) {
+          mbar_arrive(&agen[s]);
+          mbar_arrive(&rs_empty[rr]);
+        }
+        if (++s == S) {
+          s = 0;
+          ph ^= 1;
+        }
+        if (++rr == NR) {
+          rr = 0;
+          rph ^= 1;
+        }
+      }
+    }
+  }
+
+  // Both CTAs stay resident until the pair is done with each other's shared
+  // and tensor memory.
+  tc_fence_before();
+  __syncthreads();
+  cluster_sync_all();
+  if (warp == 2) {
+    tc_fence_after();
+    tmem_dealloc_pair(tmem_base, 512);
+  }
+}
+
 int ilog2(int v) {
   int s = 0;
   while ((1 << s) < v) ++s;
@@ -577,7 +1030,7 @@ int ilog2(int v) {
 // below ~4e-6 of the field's standard deviation at any harmonic count.
 constexpr int kDefaultChunkStages = 32;
 int g_chunk_stages = kDefaultChunkStages;
-bool g_a_in_tmem = false;
+int g_variant = kTcVariantSingle;
 
 TableJob make_job(const scarf_srm_setup& s, const int fs[3], float ds, const float* d_table, int nh,
                   const TcPlan& p, void* d_work) {
@@ -598,10 +1051,11 @@ TableJob make_job(const scarf_srm_setup& s, const int fs[3], float ds, const flo
   T.n3 = p.n3;
   T.ti = p.ti;
   T.tj = p.tj;
-  T.bi = p.bi;
-  T.bj = p.bj;
+  T.bi = p.pair_i ? 2 * p.bix : p.bi;
+  T.bj = (p.pair && !p.pair_i) ? 2 * p.bjx : p.bj;
   T.ntile_n = p.ntile_n;
   T.bn = p.bn;
+  T.parts = p.pair ? 2 : 1;
   T.rimg = reinterpret_cast<float2*>(work + p.off_r);
   T.simg = reinterpret_cast<float2*>(work + p.off_s);
   T.cimg = work + p.off_c;
@@ -615,10 +1069,13 @@ TcField make_field(const scarf_srm_setup& s, const TcPlan& p, const TableJob& T,
   f.n3 = p.n3;
   f.bi = p.bi;
   f.bj = p.bj;
+  f.bix = p.bix;
+  f.bjx = p.bjx;
+  f.pair_i = p.pair_i;
   f.ntile_n = p.ntile_n;
   f.stages = p.stages;
   f.chunk_stages = std::max(1, p.chunk_stages);
-  f.idesc = umma_idesc_f16_f32(kRows, static_cast<uint32_t>(p.ntile_n));
+  f.idesc = umma_idesc_f16_f32(p.pair ? 2 * kRows : kRows, static_cast<uint32_t>(p.ntile_n));
   f.scaling = s.scaling;
   f.rimg = T.rimg;
   f.simg = T.simg;
@@ -632,18 +1089,37 @@ constexpr int kMaxDynSmem = 227 * 1024;
 // Shared-memory carve-up for a launch with row tiles ti x tj and column
 // tiles up to ntile_max; returns the dynamic shared-memory size (0 if the
 // ring cannot hold two stages). With A in tensor memory a stage holds only
-// the B image and the factor tiles, and the ring depth is the TMEM A ring's.
-size_t compute_layout(TcKernelArgs& A, int ti, int tj, int ntile_max, bool tmem_a) {
+// the B image and the factor tiles, and the ring depth is the TMEM A ring's;
+// a CTA of a pair holds half of the B image.
+size_t compute_layout(TcKernelArgs& A, int ti, int tj, int ntile_max, bool tmem_a, bool pair) {
   A.ti = ti;
   A.tj = tj;
   A.ti_shift = ilog2(ti);
+  const uint32_t budget = kMaxDynSmem - 1024u - 1024u;
+  if (pair) {
+    // A / B ring: this CTA's half of the B image, then the A tile (hi, lo).
+    A.off_b = 0;
+    A.off_a = (ntile_max * kRowBytes + 1023u) & ~1023u;
+    A.off_r = A.off_s = 0;
+    A.stage_bytes = A.off_a + 2u * kATileBytes;
+    // R / S ring: up to 16 stages ahead (at least 4), ~48 KB.
+    A.rs_bytes = (kStageHarm * (ti + tj) * 8u + 127u) & ~127u;
+    A.nrs = std::max(4, std::min(16, static_cast<int>((48u * 1024u) / A.rs_bytes)));
+    const uint32_t rs_total = A.nrs * A.rs_bytes;
+    if (rs_total >= budget) return 0;
+    const int nbuf = std::min(8, static_cast<int>((budget - rs_total) / A.stage_bytes));
+    if (nbuf < 2) return 0;
+    A.nstage_buf = nbuf;
+    A.rs_base = nbuf * A.stage_bytes;
+    A.bars_off = (A.rs_base + rs_total + 7u) & ~7u;
+    return 1024 + A.bars_off + (3 * nbuf + 2 * A.nrs + 3 + 2 * kItemRing) * 8 + kItemRing * 4 + 16;
+  }
   const uint32_t b_bytes = 2u * ntile_max * kRowBytes;
   A.off_b = 0;
   A.off_a = (b_bytes + 1023u) & ~1023u;
   A.off_r = A.off_a + (tmem_a ? 0u : 2u * kATileBytes);
   A.off_s = A.off_r + kStageHarm * ti * 8u;
   A.stage_bytes = (A.off_s + kStageHarm * tj * 8u + 1023u) & ~1023u;
-  const uint32_t budget = kMaxDynSmem - 1024u - 512u;
   const int nbuf = std::min(tmem_a ? kTmemAStages : 8, static_cast<int>(budget / A.stage_bytes));
   if (nbuf < 2) return 0;
   A.nstage_buf = nbuf;
@@ -662,6 +1138,8 @@ cudaError_t ensure_smem_attribute() {
   e = cudaFuncSetAttribute(srm_tc_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(srm_tc_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(srm_tc_pair_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
   if (e == cudaSuccess && dev >= 0 && dev < 64) done[dev] = true;
   return e;
 }
@@ -673,16 +1151,21 @@ int device_sms() {
   return nsm;
 }
 
-void launch_tc_kernel(const TcKernelArgs& A, bool tmem_a, int grid, size_t smem, cudaStream_t stream) {
-  if (tmem_a)
-    srm_tc_kernel<true><<<grid, kThreads, smem, stream>>>(A);
-  else
-    srm_tc_kernel<false><<<grid, kThreads, smem, stream>>>(A);
+// Persistent launch: one CTA (or CTA pair) per SM (pair), at most one per item.
+void launch_tc_kernel(const TcKernelArgs& A, bool tmem_a, bool pair, int nsm, size_t smem, cudaStream_t stream) {
+  if (pair) {
+    const int pairs = std::max(1, std::min(A.num_items, nsm / 2));
+    srm_tc_pair_kernel<<<2 * pairs, kThreads, smem, stream>>>(A);
+  } else if (tmem_a) {
+    srm_tc_kernel<true><<<std::min(A.num_items, nsm), kThreads, smem, stream>>>(A);
+  } else {
+    srm_tc_kernel<false><<<std::min(A.num_items, nsm), kThreads, smem, stream>>>(A);
+  }
 }
 
 }  // namespace
 
-void tc_set_a_in_tmem(int on) { g_a_in_tmem = on != 0; }
+void tc_set_variant(int v) { g_variant = v; }
 
 void tc_set_chunk_harmonics(int harmonics) {
   g_chunk_stages = harmonics > 0 ? (harmonics + kStageHarm - 1) / kStageHarm : kDefaultChunkStages;
@@ -709,7 +1192,11 @@ bool tc_make_plan(int ndim, const int n[3], int nh, TcPlan* P, int tj_force) {
   p.ti = kRows / p.tj;
   p.bi = (p.n1 + p.ti - 1) / p.ti;
   p.bj = (p.n2 + p.tj - 1) / p.tj;
-  p.tmem_a = g_a_in_tmem ? 1 : 0;
+  p.pair = g_variant == kTcVariantPair ? 1 : 0;
+  p.tmem_a = g_variant == kTcVariantSingleTmemA ? 1 : 0;
+  p.pair_i = (p.pair && p.bj == 1) ? 1 : 0;  // one row block along j (2D): pair along i
+  p.bix = (p.pair && p.pair_i) ? (p.bi + 1) / 2 : p.bi;
+  p.bjx = (p.pair && !p.pair_i) ? (p.bj + 1) / 2 : p.bj;
   const int max_n = p.tmem_a ? kMaxNTmemA : kMaxNSmemA;
   const int n3_16 = (p.n3 + 15) / 16 * 16;
   p.bn = (n3_16 + max_n - 1) / max_n;
@@ -721,9 +1208,10 @@ bool tc_make_plan(int ndim, const int n[3], int nh, TcPlan* P, int tj_force) {
   auto align = [](size_t v) { return (v + 255) / 256 * 256; };
   size_t off = 0;
   p.off_r = off;
-  off = align(off + static_cast<size_t>(p.bi) * p.stages * kStageHarm * p.ti * sizeof(float2));
+  off = align(off + static_cast<size_t>(p.pair_i ? 2 * p.bix : p.bi) * p.stages * kStageHarm * p.ti * sizeof(float2));
   p.off_s = off;
-  off = align(off + static_cast<size_t>(p.bj) * p.stages * kStageHarm * p.tj * sizeof(float2));
+  off = align(off + static_cast<size_t>((p.pair && !p.pair_i) ? 2 * p.bjx : p.bj) * p.stages * kStageHarm * p.tj *
+                        sizeof(float2));
   p.off_c = off;
   off = align(off + static_cast<size_t>(p.bn) * p.stages * 2 * p.ntile_n * kRowBytes);
   p.off_status = off;  // status word, then the work-queue counter
@@ -764,10 +1252,10 @@ cudaError_t launch_tc_structured(const scarf_srm_setup& s, const int fs[3], cons
   A.f0 = make_field(s, p, T, d_field);
   A.fields = nullptr;
   A.items = nullptr;
-  A.num_items = p.bi * p.bj * p.bn;
+  A.num_items = p.bix * p.bjx * p.bn;
   A.status = d_status;
   A.queue = d_status + 1;
-  const size_t smem = compute_layout(A, p.ti, p.tj, p.ntile_n, p.tmem_a != 0);
+  const size_t smem = compute_layout(A, p.ti, p.tj, p.ntile_n, p.tmem_a != 0, p.pair != 0);
   if (!smem) return cudaErrorInvalidConfiguration;
   cudaError_t e = ensure_smem_attribute();
   if (e != cudaSuccess) return e;
@@ -782,7 +1270,7 @@ cudaError_t launch_tc_structured(const scarf_srm_setup& s, const int fs[3], cons
     A.slab_spn = slabs->spn;
   }
   if (ev_main0) cudaEventRecord(ev_main0, stream);
-  launch_tc_kernel(A, p.tmem_a != 0, std::min(A.num_items, nsm), smem, stream);
+  launch_tc_kernel(A, p.tmem_a != 0, p.pair != 0, nsm, smem, stream);
   if (ev_main1) cudaEventRecord(ev_main1, stream);
   return cudaGetLastError();
 }
@@ -806,11 +1294,12 @@ size_t tc_batch_plan(const TcBatchInput* in, int nfields, TcBatchPlan* out) {
       ti = p.ti;
       tj = p.tj;
       bp.tmem_a = p.tmem_a;
-    } else if (p.ti != ti || p.tj != tj || p.tmem_a != bp.tmem_a) {
+      bp.pair = p.pair;
+    } else if (p.ti != ti || p.tj != tj || p.tmem_a != bp.tmem_a || p.pair != bp.pair) {
       return 0;  // one row-tile shape and A placement per launch
     }
     ntile_max = std::max(ntile_max, p.ntile_n);
-    items += static_cast<long long>(p.bi) * p.bj * p.bn;
+    items += static_cast<long long>(p.bix) * p.bjx * p.bn;
     bp.field_off.push_back(off);
     bp.plans.push_back(p);
     off = align(off + p.bytes);
@@ -837,7 +1326,7 @@ cudaError_t tc_batch_upload(const TcBatchInput* in, const TcBatchPlan& bp, void*
   for (int f = 0; f < bp.nfields; ++f) {
     jobs[f] = make_job(*in[f].s, in[f].fs, in[f].ds, in[f].d_table, in[f].nh, bp.plans[f], work + bp.field_off[f]);
     fields[f] = make_field(*in[f].s, bp.plans[f], jobs[f], in[f].d_field);
-    const int nit = bp.plans[f].bi * bp.plans[f].bj * bp.plans[f].bn;
+    const int nit = bp.plans[f].bix * bp.plans[f].bjx * bp.plans[f].bn;
     for (int l = 0; l < nit; ++l) items.push_back(make_int2(f, l));
   }
   // Longest items first (the dynamic queue then balances the tail).
@@ -874,10 +1363,10 @@ cudaError_t tc_batch_launch(const TcBatchPlan& bp, void* d_work, cudaStream_t st
   A.num_items = bp.num_items;
   A.status = status;
   A.queue = status + 1;
-  const size_t smem = compute_layout(A, bp.ti, bp.tj, bp.ntile_max, bp.tmem_a != 0);
+  const size_t smem = compute_layout(A, bp.ti, bp.tj, bp.ntile_max, bp.tmem_a != 0, bp.pair != 0);
   if (!smem) return cudaErrorInvalidConfiguration;
   if (ev_main0) cudaEventRecord(ev_main0, stream);
-  launch_tc_kernel(A, bp.tmem_a != 0, std::min(bp.num_items, nsm), smem, stream);
+  launch_tc_kernel(A, bp.tmem_a != 0, bp.pair != 0, nsm, smem, stream);
   if (ev_main1) cudaEventRecord(ev_main1, stream);
   return cudaGetLastError();
 }
