@@ -199,7 +199,7 @@ def run_batched(args, nfields=256):
     spec = batched_fields(count=nfields)
     stream = torch.cuda.current_stream()
     t0 = time.perf_counter()
-    tabs = [sb.sample_device(f["params"], f["setup"], stream.cuda_stream)[0] for f in spec]
+    tabs = sb.sample_device_batch([f["params"] for f in spec], [f["setup"] for f in spec], stream.cuda_stream)[0]
     t_sample = time.perf_counter() - t0
     work = float(sum(int(np.prod(f["n"])) * len(t) for f, t in zip(spec, tabs)))
     d_tabs = [torch.from_numpy(t.reshape(-1).copy()).cuda() for t in tabs]
@@ -242,7 +242,7 @@ def run_batched(args, nfields=256):
     hosts = [torch.empty(o.numel(), dtype=torch.float32, pin_memory=True) for o in outs]
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    tabs2 = [sb.sample_device(f["params"], f["setup"], stream.cuda_stream)[0] for f in spec]
+    tabs2 = sb.sample_device_batch([f["params"] for f in spec], [f["setup"] for f in spec], stream.cuda_stream)[0]
     for d, t in zip(d_tabs, tabs2):
         d.copy_(torch.from_numpy(t.reshape(-1)), non_blocking=True)
     graph.replay()

@@ -128,6 +128,15 @@ int scarf_srm_sample(const scarf_srm_params *p, const scarf_srm_setup *s, float 
 int scarf_srm_sample_device(const scarf_srm_params *p, const scarf_srm_setup *s, float *table, int *n_kept,
                             long long *pairs_used, long long *host_decided, void *stream);
 
+/* scarf_srm_sample_device for nfields fields at once (p[f], s[f] -> tables[f]
+ * with room for p[f].nharm rows; n_kept[f], pairs_used[f] per field, may be
+ * NULL for pairs_used; *host_decided sums the host-decided pairs). The first
+ * pass of every field runs in one count and one write launch; the tables are
+ * bit-identical to scarf_srm_sample_device's. */
+int scarf_srm_sample_device_batch(int nfields, const scarf_srm_params *p, const scarf_srm_setup *s,
+                                  float *const *tables, int *n_kept, long long *pairs_used, long long *host_decided,
+                                  void *stream);
+
 /* Where scarf_execute draws its harmonics: SCARF_SAMPLER_AUTO (device,
  * unless a uniform source was installed), _HOST or _DEVICE. */
 #define SCARF_SAMPLER_AUTO 0

@@ -36,7 +36,8 @@ EXPORTED_SYMBOLS = (
     "scarf_set_uniform_source", "scarf_set_stream", "scarf_set_host_threads", "scarf_set_kernel_timing",
     "scarf_last_kernel_ms", "scarf_set_tc_chunk", "scarf_set_tc_variant", "scarf_set_output_overlap",
     "scarf_execute_ex",
-    "scarf_srm_compute_setup", "scarf_srm_sample", "scarf_srm_sample_device", "scarf_set_sampler",
+    "scarf_srm_compute_setup", "scarf_srm_sample", "scarf_srm_sample_device", "scarf_srm_sample_device_batch",
+    "scarf_set_sampler",
     "scarf_set_sampler_pass_pairs",
     "scarf_srm_direct_structured",
     "scarf_srm_direct_points", "scarf_srm_tc_workspace_bytes", "scarf_srm_tc_structured",
@@ -123,6 +124,8 @@ def _load() -> ctypes.CDLL:
                                      ctypes.POINTER(c_ll)]),
         "scarf_srm_sample_device": (c_int, [ctypes.POINTER(SrmParams), ctypes.POINTER(SrmSetup), c_void_p, ip,
                                             ctypes.POINTER(c_ll), ctypes.POINTER(c_ll), c_void_p]),
+        "scarf_srm_sample_device_batch": (c_int, [c_int, c_void_p, c_void_p, c_void_p, ip, c_void_p,
+                                                  ctypes.POINTER(c_ll), c_void_p]),
         "scarf_set_sampler": (c_int, [c_int]),
         "scarf_set_sampler_pass_pairs": (c_int, [c_ll]),
         "scarf_srm_direct_structured": (c_int, [ctypes.POINTER(SrmSetup), ip, ip, c_float, c_void_p, c_int,
@@ -329,6 +332,26 @@ def sample_device(p: SrmParams, s: SrmSetup, stream_handle: int | None = None):
                                       ctypes.byref(kept), ctypes.byref(used), ctypes.byref(open_),
                                       ctypes.c_void_p(stream_handle or 0)))
     return tab[: kept.value].copy(), used.value, open_.value
+
+
+def sample_device_batch(params, setups, stream_handle: int | None = None):
+    """Device-assisted sampler for many fields in one pass of launches:
+    (list of tables, list of pairs used, pairs decided on the host)."""
+    n = len(params)
+    if len(setups) != n:
+        raise ValueError("params and setups differ in length")
+    p_arr = (SrmParams * n)(*params)
+    s_arr = (SrmSetup * n)(*setups)
+    tabs = [np.zeros((max(p.nharm, 1), 5), np.float32) for p in params]
+    ptrs = (ctypes.c_void_p * n)(*[t.ctypes.data for t in tabs])
+    kept = (ctypes.c_int * n)()
+    used = (ctypes.c_longlong * n)()
+    open_ = ctypes.c_longlong()
+    check(lib.scarf_srm_sample_device_batch(n, ctypes.cast(p_arr, ctypes.c_void_p), ctypes.cast(s_arr, ctypes.c_void_p),
+                                            ctypes.cast(ptrs, ctypes.c_void_p), kept,
+                                            ctypes.cast(used, ctypes.c_void_p), ctypes.byref(open_),
+                                            ctypes.c_void_p(stream_handle or 0)))
+    return [t[: kept[i]].copy() for i, t in enumerate(tabs)], list(used), open_.value
 
 
 def set_sampler(where: int):

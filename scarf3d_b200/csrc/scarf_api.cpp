@@ -730,6 +730,25 @@ int scarf_srm_sample_device(const scarf_srm_params* p, const scarf_srm_setup* s,
   return SCARF_OK;
 }
 
+int scarf_srm_sample_device_batch(int nfields, const scarf_srm_params* p, const scarf_srm_setup* s,
+                                  float* const* tables, int* n_kept, long long* pairs_used, long long* host_decided,
+                                  void* stream) {
+  if (nfields < 0 || (nfields > 0 && (!p || !s || !tables || !n_kept)))
+    return fail(SCARF_ERR_ARG, "invalid argument");
+  for (int f = 0; f < nfields; ++f)
+    if (!tables[f]) return fail(SCARF_ERR_ARG, "tables[%d] is NULL", f);
+  long long open = 0;
+  const int rc = srm_sample_device_batch(nfields, p, s, tables, n_kept, pairs_used, stream, &open);
+  if (rc <= -2 - nfields) return fail(SCARF_ERR_CUDA, "batched device sampler: CUDA error");
+  if (rc < 0) {
+    const int f = -1 - rc;
+    return fail(SCARF_ERR_ARG, "field %d: rejection sampling infeasible: acceptance rate %.3g < %.1g", f,
+                acceptance_rate(s[f]), kMinAcceptance);
+  }
+  if (host_decided) *host_decided = open;
+  return SCARF_OK;
+}
+
 int scarf_srm_sample(const scarf_srm_params* p, const scarf_srm_setup* s, float* table, int* n_kept,
                      long long* pairs_used) {
   if (!p || !s || !table) return fail(SCARF_ERR_ARG, "NULL argument");

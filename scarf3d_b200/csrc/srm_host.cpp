@@ -10,6 +10,7 @@
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
+#include <memory>
 #include <mutex>
 #include <thread>
 #include <vector>
@@ -393,7 +394,9 @@ struct DevBuf {
 struct DeviceSamplerState {
   int device = -1;
   bool tables = false;
-  DevBuf counts, offsets, entries;
+  DevBuf counts, offsets, entries, slots, batch_args, batch_tbeg;
+  SampleEntry* host_entries = nullptr;  // page-locked staging of candidate entries
+  long long host_entries_cap = 0;
 };
 DeviceSamplerState g_dev_sampler;
 std::mutex g_dev_sampler_mu;
@@ -412,24 +415,9 @@ void set_device_sampler_pass_cap(long long pairs) {
   g_pass_pairs_cap = pairs > 0 ? pairs : 0;
 }
 
-int srm_sample_device(const scarf_srm_params& p, const scarf_srm_setup& s, float* table, long long* pairs_used,
-                      void* stream_handle, long long* uncertain) {
-  const cudaStream_t stream = static_cast<cudaStream_t>(stream_handle);
-  const double acc = acceptance_rate(s);
-  if (acc < kMinAcceptance) return -1;
-  std::lock_guard<std::mutex> lk(g_dev_sampler_mu);
-  DeviceSamplerState& D = g_dev_sampler;
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess) return -2;
-  if (D.device != dev) {
-    D = DeviceSamplerState();
-    D.device = dev;
-  }
-  if (!D.tables) {
-    const PowTables& t = pow_tables();
-    if (sampler_upload_tables(t.lo.data(), t.hi.data()) != cudaSuccess) return -2;
-    D.tables = true;
-  }
+namespace {
+
+SamplerArgs make_sampler_args(const scarf_srm_params& p, const scarf_srm_setup& s) {
   Yarn2 g;
   g.seed(p.seed);
   SamplerArgs A{};
@@ -444,101 +432,293 @@ int srm_sample_device(const scarf_srm_params& p, const scarf_srm_setup& s, float
   // Device and host spectra differ by a few ulps at most; 2e-5 relative is a
   // wide bound around the decision r2 < d.
   A.margin = 2e-5f;
+  return A;
+}
 
-  std::vector<SampleEntry> entries;
-  std::vector<int> counts;
-  std::vector<long long> offsets;
-  long long open = 0;
-  auto run_pass = [&](long long q_begin, long long count) -> bool {
-    A.q_begin = q_begin;
-    A.q_count = count;
-    A.pairs_per_thread = static_cast<int>(std::min<long long>(8192, std::max<long long>(256, count / (148 * 2048))));
-    A.nthreads = (count + A.pairs_per_thread - 1) / A.pairs_per_thread;
-    if (D.counts.ensure(sizeof(int) * A.nthreads) != cudaSuccess) return false;
-    if (D.offsets.ensure(sizeof(long long) * A.nthreads) != cudaSuccess) return false;
-    A.counts = static_cast<int*>(D.counts.p);
-    A.offsets = static_cast<const long long*>(D.offsets.p);
-    A.write = 0;
+long long capped_pairs(long long n) { return g_pass_pairs_cap > 0 ? std::min(n, g_pass_pairs_cap) : n; }
+
+// Pairs of the first pass of a field: enough for every harmonic at the
+// expected acceptance with a 10 % margin.
+long long first_pass_pairs(const scarf_srm_params& p, double acc) {
+  return capped_pairs(static_cast<long long>(p.nharm * (1.0 / acc + 3.0) * 1.1) + 4096);
+}
+
+// Uploads the pow tables once per device (caller holds g_dev_sampler_mu).
+bool ensure_sampler_device(DeviceSamplerState& D) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return false;
+  if (D.device != dev) {
+    D = DeviceSamplerState();
+    D.device = dev;
+  }
+  if (!D.tables) {
+    const PowTables& t = pow_tables();
+    if (sampler_upload_tables(t.lo.data(), t.hi.data()) != cudaSuccess) return false;
+    D.tables = true;
+  }
+  return true;
+}
+
+// One device pass of one field over pairs [q_begin, q_begin + count): the
+// candidate entries (accepted or undecided pairs) in stream order.
+bool single_pass(DeviceSamplerState& D, SamplerArgs A, long long q_begin, long long count,
+                 std::vector<SampleEntry>& entries, cudaStream_t stream) {
+  A.q_begin = q_begin;
+  A.q_count = count;
+  A.pairs_per_thread = static_cast<int>(std::min<long long>(8192, std::max<long long>(256, count / (148 * 2048))));
+  A.nthreads = (count + A.pairs_per_thread - 1) / A.pairs_per_thread;
+  if (D.counts.ensure(sizeof(int) * A.nthreads) != cudaSuccess) return false;
+  if (D.offsets.ensure(sizeof(long long) * A.nthreads) != cudaSuccess) return false;
+  A.counts = static_cast<int*>(D.counts.p);
+  A.offsets = static_cast<const long long*>(D.offsets.p);
+  A.write = 0;
+  if (launch_sampler(A, stream) != cudaSuccess) return false;
+  std::vector<int> counts(A.nthreads);
+  if (cudaMemcpyAsync(counts.data(), D.counts.p, sizeof(int) * A.nthreads, cudaMemcpyDeviceToHost, stream) !=
+          cudaSuccess ||
+      cudaStreamSynchronize(stream) != cudaSuccess)
+    return false;
+  std::vector<long long> offsets(A.nthreads);
+  long long total = 0;
+  for (long long t = 0; t < A.nthreads; ++t) {
+    offsets[t] = total;
+    total += counts[t];
+  }
+  entries.resize(total);
+  if (total > 0) {
+    if (D.entries.ensure(sizeof(SampleEntry) * total) != cudaSuccess) return false;
+    if (cudaMemcpyAsync(D.offsets.p, offsets.data(), sizeof(long long) * A.nthreads, cudaMemcpyHostToDevice,
+                        stream) != cudaSuccess)
+      return false;
+    A.out = static_cast<SampleEntry*>(D.entries.p);
+    A.write = 1;
     if (launch_sampler(A, stream) != cudaSuccess) return false;
-    counts.resize(A.nthreads);
-    if (cudaMemcpyAsync(counts.data(), D.counts.p, sizeof(int) * A.nthreads, cudaMemcpyDeviceToHost, stream) !=
+    if (cudaMemcpyAsync(entries.data(), D.entries.p, sizeof(SampleEntry) * total, cudaMemcpyDeviceToHost, stream) !=
             cudaSuccess ||
         cudaStreamSynchronize(stream) != cudaSuccess)
       return false;
-    offsets.resize(A.nthreads);
-    long long total = 0;
-    for (long long t = 0; t < A.nthreads; ++t) {
-      offsets[t] = total;
-      total += counts[t];
-    }
-    entries.resize(total);
-    if (total > 0) {
-      if (D.entries.ensure(sizeof(SampleEntry) * total) != cudaSuccess) return false;
-      if (cudaMemcpyAsync(D.offsets.p, offsets.data(), sizeof(long long) * A.nthreads, cudaMemcpyHostToDevice,
-                          stream) != cudaSuccess)
-        return false;
-      A.out = static_cast<SampleEntry*>(D.entries.p);
-      A.write = 1;
-      if (launch_sampler(A, stream) != cudaSuccess) return false;
-      if (cudaMemcpyAsync(entries.data(), D.entries.p, sizeof(SampleEntry) * total, cudaMemcpyDeviceToHost,
-                          stream) != cudaSuccess ||
-          cudaStreamSynchronize(stream) != cudaSuccess)
-        return false;
-    }
-    return true;
-  };
+  }
+  return true;
+}
 
-  // Walk the candidates in stream order exactly as the serial loop consumes
-  // pairs: reject until an accepted pair, then one pair of angles, then (for
-  // a kept harmonic) two pairs for a and b.
-  auto capped = [](long long n) { return g_pass_pairs_cap > 0 ? std::min(n, g_pass_pairs_cap) : n; };
-  long long pass_begin = 0, pass_end = capped(static_cast<long long>(p.nharm * (1.0 / acc + 3.0) * 1.1) + 4096);
-  if (!run_pass(pass_begin, pass_end)) return -2;
+// The host walk of one field over its candidate entries, in stream order
+// exactly as the serial loop consumes pairs: reject until an accepted pair,
+// then one pair of angles, then (for a kept harmonic) two pairs for a and b.
+// Resumable: walk() returns false when the entries ran out before every
+// harmonic was decided; the caller then supplies the next pass.
+struct DeviceWalk {
+  const scarf_srm_params* p = nullptr;
+  const scarf_srm_setup* s = nullptr;
+  float* table = nullptr;
+  double acc = 0.0;
+  // Candidates of the current pass: a view into a shared buffer (first pass
+  // of a batch) or into `owned` (passes of this field alone).
+  const SampleEntry* ent = nullptr;
+  size_t nent = 0;
+  std::vector<SampleEntry> owned;
   size_t ei = 0;
-  long long pos = 0;
-  int kept = 0;
-  for (int l = 0; l < p.nharm; ++l) {
-    for (;;) {
-      while (ei < entries.size() && entries[ei].q < pos) ++ei;
-      if (ei == entries.size()) {
-        const long long more = capped(static_cast<long long>((p.nharm - l) * (1.0 / acc + 3.0) * 1.2) + 4096);
-        pass_begin = pass_end;
-        pass_end = pass_begin + more;
-        if (!run_pass(pass_begin, more)) return -2;
-        ei = 0;
-        continue;
-      }
-      const SampleEntry& e = entries[ei];
-      bool ok = e.flag == 1;
-      if (e.flag == 2) {
-        ++open;
-        ok = host_accept(s, p.acf, e.r[0], e.r[1]);
-      }
-      if (!ok) {
-        ++ei;
-        continue;
-      }
-      Draws d{};
-      d.u = e.r[0] * (s.kmax - s.kmin) + s.kmin;
-      if (d.u > s.kc) {
-        pos = e.q + 2;
+  long long pos = 0, open = 0, pass_end = 0;
+  int kept = 0, l = 0;
+
+  bool walk() {
+    for (; l < p->nharm; ++l) {
+      for (;;) {
+        while (ei < nent && ent[ei].q < pos) ++ei;
+        if (ei == nent) return false;
+        const SampleEntry& e = ent[ei];
+        bool ok = e.flag == 1;
+        if (e.flag == 2) {
+          ++open;
+          ok = host_accept(*s, p->acf, e.r[0], e.r[1]);
+        }
+        if (!ok) {
+          ++ei;
+          continue;
+        }
+        Draws d{};
+        d.u = e.r[0] * (s->kmax - s->kmin) + s->kmin;
+        if (d.u > s->kc) {
+          pos = e.q + 2;
+          break;
+        }
+        d.ang[0] = e.r[2];
+        d.ang[1] = e.r[3];
+        d.ra[0] = e.r[4];
+        d.ra[1] = e.r[5];
+        d.rb[0] = e.r[6];
+        d.rb[1] = e.r[7];
+        harmonic_row(d, s->ndim, p->cl, table + 5 * static_cast<size_t>(kept));
+        ++kept;
+        pos = e.q + 4;
         break;
       }
-      d.ang[0] = e.r[2];
-      d.ang[1] = e.r[3];
-      d.ra[0] = e.r[4];
-      d.ra[1] = e.r[5];
-      d.rb[0] = e.r[6];
-      d.rb[1] = e.r[7];
-      harmonic_row(d, s.ndim, p.cl, table + 5 * static_cast<size_t>(kept));
-      ++kept;
-      pos = e.q + 4;
-      break;
     }
+    return true;
   }
-  if (pairs_used) *pairs_used = pos;
-  if (uncertain) *uncertain = open;
+
+  // Further passes until the walk completes.
+  bool finish(DeviceSamplerState& D, const SamplerArgs& A, cudaStream_t stream) {
+    while (!walk()) {
+      const long long more = capped_pairs(static_cast<long long>((p->nharm - l) * (1.0 / acc + 3.0) * 1.2) + 4096);
+      if (!single_pass(D, A, pass_end, more, owned, stream)) return false;
+      pass_end += more;
+      ent = owned.data();
+      nent = owned.size();
+      ei = 0;
+    }
+    return true;
+  }
+};
+
+}  // namespace
+
+int srm_sample_device(const scarf_srm_params& p, const scarf_srm_setup& s, float* table, long long* pairs_used,
+                      void* stream_handle, long long* uncertain) {
+  // The batched path with one field: its first pass is a single scan.
+  int kept = 0;
+  long long used = 0;
+  float* tables[1] = {table};
+  const int rc = srm_sample_device_batch(1, &p, &s, tables, &kept, &used, stream_handle, uncertain);
+  if (rc == -1) return -1;
+  if (rc < 0) return -2;
+  if (pairs_used) *pairs_used = used;
   return kept;
+}
+
+int srm_sample_device_batch(int nfields, const scarf_srm_params* p, const scarf_srm_setup* s, float* const* tables,
+                            int* kept, long long* pairs_used, void* stream_handle, long long* uncertain) {
+  const cudaStream_t stream = static_cast<cudaStream_t>(stream_handle);
+  if (nfields <= 0) return 0;
+  std::vector<double> acc(nfields);
+  for (int f = 0; f < nfields; ++f) {
+    acc[f] = acceptance_rate(s[f]);
+    if (acc[f] < kMinAcceptance) return -1 - f;
+  }
+  std::lock_guard<std::mutex> lk(g_dev_sampler_mu);
+  DeviceSamplerState& D = g_dev_sampler;
+  if (!ensure_sampler_device(D)) return -2 - nfields;
+  // First pass of every field in one scan: each thread keeps up to `cap`
+  // candidates in its own slot (cap sized from the expected count, with a
+  // wide Poisson margin); a gather launch compacts them. The fields share
+  // ~300k threads (2 048 at least each), 256 to 65 536 pairs per thread.
+  const long long thread_goal = std::max<long long>(2048, 148LL * 2048 / nfields);
+  std::vector<SamplerArgs> args(nfields);
+  std::vector<long long> tbeg(nfields + 1, 0), sbeg(nfields + 1, 0);
+  for (int f = 0; f < nfields; ++f) {
+    SamplerArgs& A = args[f];
+    A = make_sampler_args(p[f], s[f]);
+    A.q_begin = 0;
+    A.q_count = first_pass_pairs(p[f], acc[f]);
+    A.pairs_per_thread =
+        static_cast<int>(std::min<long long>(65536, std::max<long long>(256, A.q_count / thread_goal)));
+    A.nthreads = (A.q_count + A.pairs_per_thread - 1) / A.pairs_per_thread;
+    const double lambda = A.pairs_per_thread * std::min(1.0, acc[f]);
+    A.cap = static_cast<int>(std::ceil(1.25 * lambda + 6.0 * std::sqrt(lambda) + 8.0));
+    tbeg[f + 1] = tbeg[f] + A.nthreads;
+    sbeg[f + 1] = sbeg[f] + A.nthreads * A.cap;
+  }
+  const long long T = tbeg[nfields];
+  const int err = -2 - nfields;
+  if (D.counts.ensure(sizeof(int) * T) != cudaSuccess || D.offsets.ensure(sizeof(long long) * T) != cudaSuccess ||
+      D.slots.ensure(sizeof(SampleEntry) * sbeg[nfields]) != cudaSuccess ||
+      D.batch_args.ensure(sizeof(SamplerArgs) * nfields) != cudaSuccess ||
+      D.batch_tbeg.ensure(sizeof(long long) * (nfields + 1)) != cudaSuccess)
+    return err;
+  int* d_counts = static_cast<int*>(D.counts.p);
+  long long* d_offsets = static_cast<long long*>(D.offsets.p);
+  SampleEntry* d_slots = static_cast<SampleEntry*>(D.slots.p);
+  for (int f = 0; f < nfields; ++f) {
+    args[f].counts = d_counts + tbeg[f];
+    args[f].offsets = nullptr;
+    args[f].out = d_slots + sbeg[f];
+  }
+  if (cudaMemcpyAsync(D.batch_args.p, args.data(), sizeof(SamplerArgs) * nfields, cudaMemcpyHostToDevice, stream) !=
+          cudaSuccess ||
+      cudaMemcpyAsync(D.batch_tbeg.p, tbeg.data(), sizeof(long long) * (nfields + 1), cudaMemcpyHostToDevice,
+                      stream) != cudaSuccess)
+    return err;
+  const SamplerArgs* d_args = static_cast<const SamplerArgs*>(D.batch_args.p);
+  const long long* d_tbeg = static_cast<const long long*>(D.batch_tbeg.p);
+  if (launch_sampler_batch(d_args, d_tbeg, nfields, T, 2, stream) != cudaSuccess) return err;
+  std::vector<int> counts(T);
+  if (cudaMemcpyAsync(counts.data(), d_counts, sizeof(int) * T, cudaMemcpyDeviceToHost, stream) != cudaSuccess ||
+      cudaStreamSynchronize(stream) != cudaSuccess)
+    return err;
+  std::vector<long long> offsets(T);
+  std::vector<long long> ebeg(nfields + 1, 0);  // entry range of each field
+  std::vector<char> overflow(nfields, 0);       // a slot overflowed: the field is redone alone
+  long long total = 0;
+  for (int f = 0; f < nfields; ++f) {
+    for (long long t = tbeg[f]; t < tbeg[f + 1]; ++t) {
+      offsets[t] = total;
+      if (counts[t] > args[f].cap) overflow[f] = 1;
+      total += std::min(counts[t], args[f].cap);
+    }
+    ebeg[f + 1] = total;
+  }
+  if (total > 0) {
+    if (D.entries.ensure(sizeof(SampleEntry) * total) != cudaSuccess) return err;
+    if (D.host_entries_cap < total) {
+      if (D.host_entries) cudaFreeHost(D.host_entries);
+      D.host_entries = nullptr;
+      D.host_entries_cap = 0;
+      void* h = nullptr;
+      if (cudaHostAlloc(&h, sizeof(SampleEntry) * total, cudaHostAllocDefault) != cudaSuccess) return err;
+      D.host_entries = static_cast<SampleEntry*>(h);
+      D.host_entries_cap = total;
+    }
+    if (cudaMemcpyAsync(d_offsets, offsets.data(), sizeof(long long) * T, cudaMemcpyHostToDevice, stream) !=
+            cudaSuccess ||
+        launch_sampler_gather(d_args, d_tbeg, nfields, T, d_offsets, static_cast<SampleEntry*>(D.entries.p),
+                              stream) != cudaSuccess ||
+        cudaMemcpyAsync(D.host_entries, D.entries.p, sizeof(SampleEntry) * total, cudaMemcpyDeviceToHost, stream) !=
+            cudaSuccess ||
+        cudaStreamSynchronize(stream) != cudaSuccess)
+      return err;
+  }
+  const SampleEntry* entries = D.host_entries;
+  // Host walks over the first passes, fields spread over host threads (each
+  // walk is independent); a field whose first pass ran short then continues
+  // with its own device passes, one field at a time.
+  std::vector<DeviceWalk> walks(nfields);
+  std::vector<char> done(nfields, 0);
+  for (int f = 0; f < nfields; ++f) {
+    DeviceWalk& w = walks[f];
+    w.p = &p[f];
+    w.s = &s[f];
+    w.table = tables[f];
+    w.acc = acc[f];
+    w.pass_end = args[f].q_count;
+    // an overflowed field starts over with its own passes (empty first pass)
+    w.ent = overflow[f] ? nullptr : entries + ebeg[f];
+    w.nent = overflow[f] ? 0 : static_cast<size_t>(ebeg[f + 1] - ebeg[f]);
+    if (overflow[f]) w.pass_end = 0;
+  }
+  const int nthr = std::max(1, std::min(host_threads(), nfields));
+  std::atomic<int> next{0};
+  auto worker = [&]() {
+    for (int f = next.fetch_add(1); f < nfields; f = next.fetch_add(1)) done[f] = walks[f].walk() ? 1 : 0;
+  };
+  std::vector<std::thread> pool;
+  for (int t = 1; t < nthr; ++t) pool.emplace_back(worker);
+  worker();
+  for (auto& th : pool) th.join();
+  long long open_total = 0;
+  for (int f = 0; f < nfields; ++f) {
+    DeviceWalk& w = walks[f];
+    if (!done[f]) {
+      SamplerArgs A = args[f];
+      A.counts = nullptr;
+      A.offsets = nullptr;
+      A.out = nullptr;
+      if (!w.finish(D, A, stream)) return err;
+    }
+    if (kept) kept[f] = w.kept;
+    if (pairs_used) pairs_used[f] = w.pos;
+    open_total += w.open;
+  }
+  if (uncertain) *uncertain = open_total;
+  return 0;
 }
 
 int srm_sample(const scarf_srm_params& p, const scarf_srm_setup& s, const UniformSource* src, int threads,

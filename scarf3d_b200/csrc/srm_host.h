@@ -78,6 +78,13 @@ double acceptance_rate(const scarf_srm_setup& s);
 // pairs decided on the host.
 int srm_sample_device(const scarf_srm_params& p, const scarf_srm_setup& s, float* table, long long* pairs_used,
                       void* stream, long long* uncertain);
+// srm_sample_device for many fields at once: the first pass of every field
+// runs in one count launch and one write launch, then the host walks the
+// fields one by one (further passes per field only if needed). Tables are
+// bit-identical to srm_sample_device's. Returns 0; -1 - f if field f is
+// infeasible; -2 - nfields on a CUDA error.
+int srm_sample_device_batch(int nfields, const scarf_srm_params* p, const scarf_srm_setup* s, float* const* tables,
+                            int* kept, long long* pairs_used, void* stream, long long* uncertain);
 // Upper bound on the pairs tested per device pass (0 = sized from the
 // acceptance rate); smaller passes are chained until every harmonic is drawn.
 void set_device_sampler_pass_cap(long long pairs);

@@ -117,9 +117,18 @@ struct SamplerArgs {
   int* counts;               // [nthreads]
   const long long* offsets;  // [nthreads]
   SampleEntry* out;
+  int cap;                   // batch mode 2: entries per thread slot (out + t * cap), counts kept in full
 };
 cudaError_t sampler_upload_tables(const unsigned int* lo, const unsigned int* hi);
 cudaError_t launch_sampler(const SamplerArgs& args, cudaStream_t stream);
+// One pass for each of nfields fields in a single launch: d_fields[f] holds
+// field f's pass (its counts / offsets pointers already at the field's slice),
+// d_tbeg the prefix of the fields' thread counts (nfields + 1 entries).
+cudaError_t launch_sampler_batch(const SamplerArgs* d_fields, const long long* d_tbeg, int nfields, long long total,
+                                 int write, cudaStream_t stream);
+// Compaction after a write = 2 batch pass (see SamplerArgs::cap).
+cudaError_t launch_sampler_gather(const SamplerArgs* d_fields, const long long* d_tbeg, int nfields, long long total,
+                                  const long long* d_offsets, SampleEntry* d_dst, cudaStream_t stream);
 
 // ---- statistics and post-processing (srm_stats.cu) ----
 size_t stats_partials_bytes(long long n);

@@ -97,23 +97,27 @@ __device__ __forceinline__ int classify(const SamplerArgs& A, float r1, float r2
   return 2;
 }
 
-__global__ void sampler_kernel(const SamplerArgs A) {
-  const long long t = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (t >= A.nthreads) return;
+// Pairs [q0, q1) of local thread t of one field's pass: count (write = 0),
+// write the candidate entries at the thread's offset (write = 1), or write
+// up to A.cap of them into the thread's own slot out + t * cap while
+// counting them all (write = 2: one scan instead of two; a count above cap
+// tells the host to redo that field).
+__device__ __forceinline__ void sample_range(const SamplerArgs& A, long long t, int write) {
   const long long q0 = A.q_begin + t * A.pairs_per_thread;
   long long q1 = q0 + A.pairs_per_thread;
   if (q1 > A.q_begin + A.q_count) q1 = A.q_begin + A.q_count;
   Gen g{A.r0, A.r1};
   g.jump(2ull * static_cast<uint64_t>(q0));
   int count = 0;
-  long long slot = A.write ? A.offsets[t] : 0;
+  long long slot = write == 1 ? A.offsets[t] : (write == 2 ? t * A.cap : 0);
+  const long long slot_end = write == 2 ? slot + A.cap : (1ll << 62);
   for (long long q = q0; q < q1; ++q) {
     const float r1 = to_u01(g.next());
     const float r2 = to_u01(g.next());
     const int c = classify(A, r1, r2);
     if (c == 0) continue;
     ++count;
-    if (A.write) {
+    if (write && slot < slot_end) {
       SampleEntry e;
       e.q = q;
       e.flag = c;
@@ -124,7 +128,49 @@ __global__ void sampler_kernel(const SamplerArgs A) {
       A.out[slot++] = e;
     }
   }
-  if (!A.write) A.counts[t] = count;
+  if (write != 1) A.counts[t] = count;
+}
+
+__global__ void sampler_kernel(const SamplerArgs A) {
+  const long long t = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (t >= A.nthreads) return;
+  sample_range(A, t, A.write);
+}
+
+// Passes of many fields in one launch: global thread t belongs to the field
+// f with tbeg[f] <= t < tbeg[f + 1] (binary search over the prefix).
+__global__ void sampler_batch_kernel(const SamplerArgs* fields, const long long* tbeg, int nfields,
+                                     long long total, int write) {
+  const long long t = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (t >= total) return;
+  int lo = 0, hi = nfields - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (tbeg[mid] <= t) lo = mid;
+    else hi = mid - 1;
+  }
+  const SamplerArgs A = fields[lo];
+  sample_range(A, t - tbeg[lo], write);
+}
+
+// Compacts the per-thread slots of a write = 2 pass: thread t's min(count,
+// cap) entries move to dst + offsets[t] (global thread index t).
+__global__ void sampler_gather_kernel(const SamplerArgs* fields, const long long* tbeg, int nfields, long long total,
+                                      const long long* offsets, SampleEntry* dst) {
+  const long long t = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (t >= total) return;
+  int lo = 0, hi = nfields - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (tbeg[mid] <= t) lo = mid;
+    else hi = mid - 1;
+  }
+  const SamplerArgs& A = fields[lo];
+  const long long tl = t - tbeg[lo];
+  const int n = min(A.counts[tl], A.cap);
+  const SampleEntry* src = A.out + tl * A.cap;
+  SampleEntry* o = dst + offsets[t];
+  for (int i = 0; i < n; ++i) o[i] = src[i];
 }
 
 }  // namespace
@@ -133,6 +179,25 @@ cudaError_t sampler_upload_tables(const uint32_t* lo, const uint32_t* hi) {
   cudaError_t e = cudaMemcpyToSymbol(g_pow_lo, lo, sizeof(uint32_t) * (1u << 16));
   if (e == cudaSuccess) e = cudaMemcpyToSymbol(g_pow_hi, hi, sizeof(uint32_t) * (1u << 15));
   return e;
+}
+
+cudaError_t launch_sampler_batch(const SamplerArgs* d_fields, const long long* d_tbeg, int nfields, long long total,
+                                 int write, cudaStream_t stream) {
+  const int block = 128;
+  const long long blocks = (total + block - 1) / block;
+  if (blocks <= 0 || nfields <= 0) return cudaSuccess;
+  sampler_batch_kernel<<<static_cast<unsigned>(blocks), block, 0, stream>>>(d_fields, d_tbeg, nfields, total, write);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_sampler_gather(const SamplerArgs* d_fields, const long long* d_tbeg, int nfields, long long total,
+                                  const long long* d_offsets, SampleEntry* d_dst, cudaStream_t stream) {
+  const int block = 128;
+  const long long blocks = (total + block - 1) / block;
+  if (blocks <= 0 || nfields <= 0) return cudaSuccess;
+  sampler_gather_kernel<<<static_cast<unsigned>(blocks), block, 0, stream>>>(d_fields, d_tbeg, nfields, total,
+                                                                             d_offsets, d_dst);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_sampler(const SamplerArgs& A, cudaStream_t stream) {

@@ -90,3 +90,62 @@ def test_execute_device_and_host_samplers_give_the_same_field():
         sb.set_sampler(sb.SAMPLER_AUTO)
         sb.scarf_finalize()
         sb.set_nharm(10000)
+
+
+def _batch_fields():
+    out = []
+    for kw, fs, fe in CASES:
+        op = oracle.structured_params(fs=fs, fe=fe, **kw)
+        pp = sb.make_params(nc=list(op.nc), fc=list(op.fc), **kw)
+        s = sb.compute_setup(pp)
+        if s.intg_band * s.cnst / max(s.kmax - s.kmin, 1e-30) >= 1e-6:
+            out.append((pp, s))
+    kw = dict(acf=1, nharm=300, seed=77, hurst=0.0, sigma=0.05, ds=50.0, cl=[2000.0, 2000.0, 2000.0])
+    op = oracle.structured_params(fs=[1, 1, 1], fe=[48, 48, 48], **kw)
+    pp = sb.make_params(nc=list(op.nc), fc=list(op.fc), **kw)
+    out.append((pp, sb.compute_setup(pp)))  # low acceptance (~1e-5)
+    return out
+
+
+def test_batched_device_sampler_matches_per_field_sampler():
+    fields = _batch_fields()
+    tabs, used, _ = sb.sample_device_batch([f[0] for f in fields], [f[1] for f in fields])
+    for (pp, s), t, u in zip(fields, tabs, used):
+        ref, ref_pairs, _ = sb.sample_device(pp, s)
+        assert u == ref_pairs
+        assert np.array_equal(t.view(np.uint32), ref.view(np.uint32))
+
+
+def test_batched_device_sampler_chains_further_passes():
+    fields = _batch_fields()
+    sb.check(sb.lib.scarf_set_sampler_pass_pairs(1_000_003))  # first passes run short
+    try:
+        tabs, used, _ = sb.sample_device_batch([f[0] for f in fields], [f[1] for f in fields])
+    finally:
+        sb.check(sb.lib.scarf_set_sampler_pass_pairs(0))
+    for (pp, s), t, u in zip(fields, tabs, used):
+        sb.set_host_threads(8)
+        host, hp = sb.sample(pp, s)
+        sb.set_host_threads(0)
+        assert u == hp
+        assert np.array_equal(t.view(np.uint32), host.view(np.uint32))
+
+
+def test_batched_device_sampler_on_the_many_realisation_workload():
+    from scarf3d_b200.workloads import batched_fields
+    spec = batched_fields(count=24)
+    tabs, used, _ = sb.sample_device_batch([f["params"] for f in spec], [f["setup"] for f in spec])
+    for f, t, u in zip(spec, tabs, used):
+        ref, ref_pairs, _ = sb.sample_device(f["params"], f["setup"])
+        assert u == ref_pairs and np.array_equal(t.view(np.uint32), ref.view(np.uint32))
+
+
+def test_batched_device_sampler_names_an_infeasible_field():
+    fields = _batch_fields()[:3]
+    kw = dict(acf=1, nharm=100, seed=5, hurst=0.0, sigma=0.05, ds=50.0, cl=[2000.0, 2000.0, 2000.0])
+    op = oracle.structured_params(fs=[1, 1, 1], fe=[12, 12, 12], **kw)
+    bad = sb.make_params(nc=list(op.nc), fc=list(op.fc), **kw)
+    ps = [f[0] for f in fields] + [bad]
+    ss = [f[1] for f in fields] + [sb.compute_setup(bad)]
+    with pytest.raises(sb.ScarfError, match="field 3"):
+        sb.sample_device_batch(ps, ss)
