@@ -812,9 +812,11 @@ int scarf_srm_direct_points(const scarf_srm_setup* s, const float* d_x, const fl
   return rc;
 }
 
+// Device-field entry points let the longer of y and z be the column axis
+// (wider column tiles); the same rule sizes their workspace.
 size_t scarf_srm_tc_workspace_bytes(int ndim, const int n[3], int nh) {
   TcPlan p{};
-  if (!n || !tc_make_plan(ndim, n, nh, &p)) return 0;
+  if (!n || !tc_make_plan(ndim, n, nh, &p, 0, true)) return 0;
   return p.bytes;
 }
 
@@ -822,7 +824,7 @@ int scarf_srm_tc_structured(const scarf_srm_setup* s, const int fs[3], const int
                             int nh, float* d_field, void* d_work, size_t work_bytes, void* stream) {
   if (!s || !fs || !n || !d_field || !d_table || nh <= 0 || !d_work) return fail(SCARF_ERR_ARG, "invalid argument");
   TcPlan p{};
-  if (!tc_make_plan(s->ndim, n, nh, &p)) return fail(SCARF_ERR_ARG, "invalid grid for the tensor-core form");
+  if (!tc_make_plan(s->ndim, n, nh, &p, 0, true)) return fail(SCARF_ERR_ARG, "invalid grid for the tensor-core form");
   if (work_bytes < p.bytes) return fail(SCARF_ERR_ARG, "workspace too small: %zu < %zu", work_bytes, p.bytes);
   if (reinterpret_cast<uintptr_t>(d_work) & 255u) return fail(SCARF_ERR_ARG, "workspace must be 256-byte aligned");
   std::lock_guard<std::mutex> lk(g_mu);

@@ -20,8 +20,10 @@ cudaError_t launch_direct_points(const scarf_srm_setup& s, const float* d_x, con
 
 // ---- factorised tensor-core form (srm_tc.cu) ----
 // Geometry of one structured field in the factorised form:
-//   out[i + n1*(j + n2*k)] = scale * Re sum_h R_h(i) S_h(j) C_h(k)
-// with (n1,n2,n3) = (nx,ny,nz) in 3D and (nx,1,ny) in 2D.
+//   out[i*sr + j*ss + k*sc] = scale * Re sum_h R_h(i) S_h(j) C_h(k)
+// with (i, j, k) along the physical axes (ax_r, ax_s, ax_c): (x, y, z) by
+// default, (x, z, y) when the plan permutes, (x, z, y) with the single z
+// plane as j in 2D.
 struct TcPlan {
   int n1, n2, n3;        // logical extents
   int ti, tj;            // row tile = ti x tj = 128 rows over (i, j)
@@ -36,6 +38,8 @@ struct TcPlan {
   int pair;              // 1: CTA-pair form (M = 256 over two SMs, each holding half of B)
   int pair_i;            // pairs split along i (when bj == 1) instead of j
   int bix, bjx;          // item grid (bi x bj, halved along the pair axis, rounded up)
+  int ax_r, ax_s, ax_c;  // physical axis (0 x, 1 y, 2 z) of i (row-fast), j (row-slow), k (column)
+  long long sr, ss, sc;  // field strides of i, j, k in elements
   size_t off_r, off_s, off_c, off_status, bytes;  // workspace layout
 };
 
@@ -46,7 +50,9 @@ constexpr int kTcVariantSingleTmemA = 2;  // one CTA per tile, A in tensor memor
 void tc_set_variant(int v);
 
 // tj_force > 0 fixes the row tile to (128 / tj_force) x tj_force.
-bool tc_make_plan(int ndim, const int n[3], int nh, TcPlan* plan, int tj_force = 0);
+// permute: let the longer of y and z be the column axis (device fields of a
+// batch; the default layout keeps k = z, which the slab copy-out relies on).
+bool tc_make_plan(int ndim, const int n[3], int nh, TcPlan* plan, int tj_force = 0, bool permute = false);
 // Harmonics accumulated in tensor memory before each FP32 drain (rounded up
 // to whole pipeline stages); 0 restores the default.
 void tc_set_chunk_harmonics(int harmonics);

@@ -74,7 +74,7 @@ extern "C" int scarf_srm_tc_structured_noalloc(const scarf_srm_setup* s, const i
   if (!s || !fs || !n || !d_table || !d_field || nh <= 0)
     return record_error(SCARF_ERR_ARG, "scarf_srm_tc_structured_noalloc: invalid argument");
   TcPlan p{};
-  if (!tc_make_plan(s->ndim, n, nh, &p))
+  if (!tc_make_plan(s->ndim, n, nh, &p, 0, true))
     return record_error(SCARF_ERR_ARG, "scarf_srm_tc_structured_noalloc: invalid grid");
   if (p.bytes > kNoAllocScratchBytes)
     return record_error(SCARF_ERR_ARG,

@@ -59,6 +59,7 @@ struct TcField {
   int n1, n2, n3;
   int bi, bj, ntile_n, stages, chunk_stages;
   int bix, bjx;         // item grid: bi x bj, or CTA pairs along j (bi x ceil(bj/2)) or i (ceil(bi/2) x bj)
+  long long sr, ss, sc; // field strides (elements) of the i, j and k axes
   int pair_i;           // CTA pairs split along i (2D fields: one row block along j)
   uint32_t idesc;
   float scaling;
@@ -534,8 +535,8 @@ __global__ void __launch_bounds__(kThreads, 1) srm_tc_kernel(const TcKernelArgs 
       const int i = w.ib * A.ti + ii;
       const int j = w.jb * A.tj + jj;
       const bool row_ok = (i < w.f.n1) && (j < w.f.n2);
-      const long long plane = static_cast<long long>(w.f.n1) * w.f.n2;
-      float* dst = w.f.field + i + static_cast<long long>(w.f.n1) * j;
+      const long long plane = w.f.sc;
+      float* dst = w.f.field + i * w.f.sr + j * w.f.ss;
       const int k0 = w.nt * w.f.ntile_n;
       for (int s0 = 0; s0 < w.f.stages; s0 += w.f.chunk_stages, ++chunk) {
         const bool first = (s0 == 0);
@@ -949,8 +950,8 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1) srm_tc_
       const int i = ib * A.ti + ii;
       const int j = jb * A.tj + jj;
       const bool row_ok = (i < w.f.n1) && (j < w.f.n2);
-      const long long plane = static_cast<long long>(w.f.n1) * w.f.n2;
-      float* dst = w.f.field + i + static_cast<long long>(w.f.n1) * j;
+      const long long plane = w.f.sc;
+      float* dst = w.f.field + i * w.f.sr + j * w.f.ss;
       const int k0 = w.nt * w.f.ntile_n;
       for (int s0 = 0; s0 < w.f.stages; s0 += w.f.chunk_stages, ++chunk) {
         const bool first = (s0 == 0);
@@ -1043,9 +1044,9 @@ TableJob make_job(const scarf_srm_setup& s, const int fs[3], float ds, const flo
   for (int i = 0; i < 3; ++i) T.bar[i] = s.bar[i];
   T.ds = ds;
   for (int a = 0; a < 3; ++a) T.off[a] = fs[a] - 1;  // 0-based t -> (t + fs - 1) * ds
-  T.ax_r = 0;
-  T.ax_s = (s.ndim == 3) ? 1 : 2;
-  T.ax_c = (s.ndim == 3) ? 2 : 1;
+  T.ax_r = p.ax_r;
+  T.ax_s = p.ax_s;
+  T.ax_c = p.ax_c;
   T.n1 = p.n1;
   T.n2 = p.n2;
   T.n3 = p.n3;
@@ -1067,6 +1068,9 @@ TcField make_field(const scarf_srm_setup& s, const TcPlan& p, const TableJob& T,
   f.n1 = p.n1;
   f.n2 = p.n2;
   f.n3 = p.n3;
+  f.sr = p.sr;
+  f.ss = p.ss;
+  f.sc = p.sc;
   f.bi = p.bi;
   f.bj = p.bj;
   f.bix = p.bix;
@@ -1171,17 +1175,28 @@ void tc_set_chunk_harmonics(int harmonics) {
   g_chunk_stages = harmonics > 0 ? (harmonics + kStageHarm - 1) / kStageHarm : kDefaultChunkStages;
 }
 
-bool tc_make_plan(int ndim, const int n[3], int nh, TcPlan* P, int tj_force) {
+bool tc_make_plan(int ndim, const int n[3], int nh, TcPlan* P, int tj_force, bool permute) {
   if (nh <= 0 || n[0] <= 0 || n[1] <= 0 || n[2] <= 0) return false;
   TcPlan p{};
-  p.n1 = n[0];
+  // Rows (i, j) over x and one of y / z, columns k over the other: by default
+  // k = z (y in 2D, whose single z plane becomes j); with `permute` the longer
+  // of y and z becomes the column axis, for wider column tiles.
+  p.ax_r = 0;
   if (ndim == 3) {
-    p.n2 = n[1];
-    p.n3 = n[2];
+    const bool swap = permute && n[1] > n[2];
+    p.ax_s = swap ? 2 : 1;
+    p.ax_c = swap ? 1 : 2;
   } else {
-    p.n2 = n[2];  // the single z plane
-    p.n3 = n[1];
+    p.ax_s = 2;
+    p.ax_c = 1;
   }
+  const long long stride[3] = {1, n[0], static_cast<long long>(n[0]) * n[1]};
+  p.n1 = n[p.ax_r];
+  p.n2 = n[p.ax_s];
+  p.n3 = n[p.ax_c];
+  p.sr = stride[p.ax_r];
+  p.ss = stride[p.ax_s];
+  p.sc = stride[p.ax_c];
   if (tj_force > 0) {
     if (tj_force > kRows || (tj_force & (tj_force - 1))) return false;
     p.tj = tj_force;
@@ -1289,7 +1304,7 @@ size_t tc_batch_plan(const TcBatchInput* in, int nfields, TcBatchPlan* out) {
   int ti = 0, tj = 0, ntile_max = 16;
   for (int f = 0; f < nfields; ++f) {
     TcPlan p{};
-    if (!tc_make_plan(in[f].s->ndim, in[f].n, in[f].nh, &p, in[f].tj)) return 0;
+    if (!tc_make_plan(in[f].s->ndim, in[f].n, in[f].nh, &p, in[f].tj, true)) return 0;
     if (f == 0) {
       ti = p.ti;
       tj = p.tj;

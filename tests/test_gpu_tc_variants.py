@@ -100,3 +100,22 @@ def test_pair_form_batch_matches_single_form():
 def test_unknown_variant_is_rejected():
     with pytest.raises(sb.ScarfError):
         sb.set_tc_variant(7)
+
+
+@pytest.mark.parametrize("n", [[64, 200, 40], [96, 130, 33], [40, 257, 100]])
+def test_y_long_grids_take_y_as_the_column_axis(n):
+    # The device-field entry point lets the longer of y and z be the column
+    # axis: the field must still agree with the FP64 oracle in the caller's
+    # x-fastest layout, for every kernel form.
+    kw = dict(acf=0, nharm=600, seed=31, hurst=0.3, sigma=0.05, ds=40.0, cl=[1500.0, 1500.0, 1500.0])
+    fc = [float(np.float32(v - 1) * np.float32(40.0)) for v in n]
+    p = sb.make_params(nc=[0.0, 0.0, 0.0], fc=fc, **kw)
+    s = sb.compute_setup(p)
+    tab, _ = sb.sample(p, s)
+    fields = [_run(v, s, [1, 1, 1], n, 40.0, tab) for v in VARIANTS]
+    for f in fields:
+        assert np.array_equal(f.view(np.uint32), fields[0].view(np.uint32))
+    op = oracle.params(acf=0, nharm=600, seed=31, hurst=0.3, sigma=0.05, ds=40.0, dh=40.0, cl=[1500.0] * 3,
+                       nc=[0.0] * 3, fc=fc)
+    ref64 = oracle.sum_structured(oracle.setup(op), [1, 1, 1], n, 40.0, tab, f64=True)
+    assert rel_rms(fields[0], ref64) <= 1e-5
