@@ -91,7 +91,7 @@ class TcField(ctypes.Structure):
 def _load() -> ctypes.CDLL:
     if not LIB_PATH.exists():
         raise ImportError(f"scarf3d_b200: {LIB_PATH} is missing; build it with "
-                          f"`python -m scarf3d_b200.build` (no CPU fallback exists)")
+                          f"`python scarf3d_b200/build.py` (no CPU fallback exists)")
     lib = ctypes.CDLL(str(LIB_PATH))
     c_int, c_float, c_void_p, c_size_t, c_ll = (ctypes.c_int, ctypes.c_float, ctypes.c_void_p,
                                                 ctypes.c_size_t, ctypes.c_longlong)
