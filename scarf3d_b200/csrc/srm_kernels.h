@@ -92,6 +92,8 @@ struct TcBatchInput {
 };
 struct TcBatchPlan {
   int nfields = 0, num_items = 0, ti = 0, tj = 0, ntile_max = 0, tmem_a = 0, pair = 0;
+  size_t smem_rs = 0, smem_c = 0;  // shared memory of the factored table builders (largest field)
+  int max_stages = 0;              // largest stage count of the fields
   size_t off_fields = 0, off_jobs = 0, off_items = 0, off_status = 0, bytes = 0;
   std::vector<TcPlan> plans;
   std::vector<size_t> field_off;

@@ -199,6 +199,167 @@ __global__ void tc_build_c(const TableJob j0, const TableJob* jobs) {
   }
 }
 
+// ---- factored table builders -------------------------------------------
+// The same images with far fewer FP64 transcendentals: along an axis the
+// phase of index t = 16 a + b splits as
+//   k ((16 a + off) ds) + c  +  k (b ds),
+// so e^{i phase} = U[a] V[b] with U, V built once per harmonic in shared
+// memory (one sincos per 16 entries, plus 16), and every entry is one FP64
+// complex product before its rounding to FP32. Used when the factor tables
+// fit kFactorSmem of shared memory; otherwise the builders above run.
+constexpr int kFactorSmem = 48 * 1024;
+
+__device__ __forceinline__ double2 cmul(double2 x, double2 y) {
+  return make_double2(x.x * y.x - x.y * y.y, x.x * y.y + x.y * y.x);
+}
+
+__device__ __forceinline__ double2 expi(double th) {
+  double s, c;
+  sincos(th, &s, &c);
+  return make_double2(c, s);
+}
+
+// R and S images: one block per harmonic at a time (grid-strided),
+// blockIdx.y the field of a batch.
+__global__ void tc_build_rs_factored(const TableJob j0, const TableJob* jobs) {
+  extern __shared__ double2 fsh[];
+  const TableJob& T = jobs ? jobs[blockIdx.y] : j0;
+  const int nr = T.bi * T.ti, ns = T.bj * T.tj;  // image widths (padded)
+  const int nur = (nr + 15) / 16, nus = (ns + 15) / 16;
+  double2* ur = fsh;
+  double2* vr = ur + nur;
+  double2* us = vr + 16;
+  double2* vs = us + nus;
+  const int nfac = nur + nus + 32;
+  const double offr = T.off[T.ax_r], offs = T.off[T.ax_s];
+  for (int h = blockIdx.x; h < T.stages * kStageHarm; h += gridDim.x) {
+    const bool valid = h < T.nh;
+    double kv[3] = {0.0, 0.0, 0.0}, c = 0.0, a = 0.0, b = 0.0;
+    if (valid) harmonic_k(T, h, kv, c, a, b);
+    const double kr = kv[T.ax_r], ks = kv[T.ax_s];
+    __syncthreads();  // the previous harmonic's entries are written
+    for (int e = threadIdx.x; e < nfac; e += blockDim.x) {
+      if (e < nur) {
+        ur[e] = expi(kr * ((16.0 * e + offr) * T.ds) + c);
+      } else if (e < nur + 16) {
+        vr[e - nur] = expi(kr * ((e - nur) * T.ds));
+      } else if (e < nur + 16 + nus) {
+        us[e - nur - 16] = expi(ks * ((16.0 * (e - nur - 16) + offs) * T.ds));
+      } else {
+        vs[e - nur - 16 - nus] = expi(ks * ((e - nur - 16 - nus) * T.ds));
+      }
+    }
+    __syncthreads();
+    const int k = h / kStageHarm, hp = h - k * kStageHarm;
+    for (int e = threadIdx.x; e < nr + ns; e += blockDim.x) {
+      const bool is_r = e < nr;
+      const int idx = is_r ? e : e - nr;
+      const int tw = is_r ? T.ti : T.tj;
+      const int blk = idx / tw, t = idx - blk * tw;
+      float2 out = make_float2(0.0f, 0.0f);
+      if (valid && idx < (is_r ? T.n1 : T.n2)) {
+        if (is_r) {
+          const double2 z = cmul(ur[idx >> 4], vr[idx & 15]);
+          // (b - i a)(cos + i sin)
+          out = make_float2(static_cast<float>(b * z.x + a * z.y), static_cast<float>(b * z.y - a * z.x));
+        } else {
+          const double2 z = cmul(us[idx >> 4], vs[idx & 15]);
+          out = make_float2(static_cast<float>(z.x), static_cast<float>(z.y));
+        }
+      }
+      const size_t q = ((static_cast<size_t>(blk) * T.stages + k) * kStageHarm + hp) * tw + t;
+      (is_r ? T.rimg : T.simg)[q] = out;
+    }
+  }
+}
+
+// Column image: one block per 4-harmonic chunk of a stage at a time
+// (grid-strided), blockIdx.y the field of a batch.
+__global__ void tc_build_c_factored(const TableJob j0, const TableJob* jobs) {
+  extern __shared__ double2 fsh[];
+  const TableJob& T = jobs ? jobs[blockIdx.y] : j0;
+  const int ncol = T.bn * T.ntile_n;
+  const int nu = (ncol + 15) / 16;
+  double2* u4 = fsh;          // [4][nu]
+  double2* v4 = u4 + 4 * nu;  // [4][16]
+  const double offc = T.off[T.ax_c];
+  const int part_rows = T.ntile_n / T.parts;
+  for (int j = blockIdx.x; j < T.stages * 4; j += gridDim.x) {
+    const int k = j >> 2, chunk = j & 3;
+    bool valid[4];
+    double kc[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int h = k * kStageHarm + chunk * 4 + u;
+      valid[u] = h < T.nh;
+      double kv[3] = {0.0, 0.0, 0.0}, c, a, b;
+      if (valid[u]) harmonic_k(T, h, kv, c, a, b);
+      kc[u] = kv[T.ax_c];
+    }
+    __syncthreads();  // the previous chunk's entries are written
+    for (int e = threadIdx.x; e < 4 * (nu + 16); e += blockDim.x) {
+      const int u = e / (nu + 16), r = e - u * (nu + 16);
+      if (r < nu) u4[u * nu + r] = expi(kc[u] * ((16.0 * r + offc) * T.ds));
+      else v4[u * 16 + (r - nu)] = expi(kc[u] * ((r - nu) * T.ds));
+    }
+    __syncthreads();
+    for (int col = threadIdx.x; col < ncol; col += blockDim.x) {
+      const int nb = col / T.ntile_n, row = col - nb * T.ntile_n;
+      const int part = row / part_rows, prow = row - part * part_rows;
+      __half2 hi[4], lo[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        float cs32 = 0.0f, sn32 = 0.0f;
+        if (valid[u] && col < T.n3) {
+          const double2 z = cmul(u4[u * nu + (col >> 4)], v4[u * 16 + (col & 15)]);
+          cs32 = static_cast<float>(z.x);
+          sn32 = static_cast<float>(z.y);
+        }
+        hi[u] = __floats2half2_rn(cs32, sn32);
+        const float2 hf = __half22float2(hi[u]);
+        lo[u] = __floats2half2_rn(cs32 - hf.x, sn32 - hf.y);
+      }
+      uint8_t* base = T.cimg + ((static_cast<size_t>(nb) * T.stages + k) * T.parts + part) *
+                                   (2u * part_rows * kRowBytes);
+      const uint32_t off = swz64(static_cast<uint32_t>(prow), static_cast<uint32_t>(chunk));
+      *reinterpret_cast<uint4*>(base + off) = *reinterpret_cast<const uint4*>(hi);
+      *reinterpret_cast<uint4*>(base + static_cast<size_t>(part_rows) * kRowBytes + off) =
+          *reinterpret_cast<const uint4*>(lo);
+    }
+  }
+}
+
+// Shared memory of the factored builders for a plan (image widths as
+// make_job sets them, padded to whole row blocks).
+size_t factor_smem_rs(const TcPlan& p) {
+  const int ni = p.pair_i ? 2 * p.bix : p.bi;
+  const int nj = (p.pair && !p.pair_i) ? 2 * p.bjx : p.bj;
+  return sizeof(double2) * (static_cast<size_t>((ni * p.ti + 15) / 16) + (nj * p.tj + 15) / 16 + 32);
+}
+size_t factor_smem_c(const TcPlan& p) {
+  return sizeof(double2) * 4 * (static_cast<size_t>((p.bn * p.ntile_n + 15) / 16) + 16);
+}
+
+// Enqueues the R/S and C image builders for nfields fields (jobs == nullptr:
+// the single field T) given their largest stage count and shared-memory
+// needs. The factored builders walk harmonics one block at a time, each
+// step latency-bound (a sincos and two barriers), so they get many small
+// blocks: ~64 per SM over all fields.
+void launch_table_builders(const TableJob& T, const TableJob* jobs, int nfields, int max_stages, size_t smem_rs,
+                           size_t smem_c, int nsm, cudaStream_t stream) {
+  const int per_field = std::max(1, nsm * 64 / std::max(1, nfields));
+  const int grid_old = std::max(1, std::min(64, nsm * 8 / std::max(1, nfields)));
+  if (smem_rs <= static_cast<size_t>(kFactorSmem))
+    tc_build_rs_factored<<<dim3(std::min(max_stages * kStageHarm, per_field), nfields), 128, smem_rs, stream>>>(
+        T, jobs);
+  else
+    tc_build_rs<<<dim3(jobs ? grid_old : nsm * 8, nfields), 256, 0, stream>>>(T, jobs);
+  if (smem_c <= static_cast<size_t>(kFactorSmem))
+    tc_build_c_factored<<<dim3(std::min(max_stages * 4, per_field), nfields), 128, smem_c, stream>>>(T, jobs);
+  else
+    tc_build_c<<<dim3(jobs ? grid_old : nsm * 8, nfields), 256, 0, stream>>>(T, jobs);
+}
+
 // One work item: field descriptor and the tile's block coordinates.
 struct Item {
   TcField f;
@@ -1258,8 +1419,7 @@ cudaError_t launch_tc_structured(const scarf_srm_setup& s, const int fs[3], cons
                                  const TcSlabSignal* slabs) {
   const TableJob T = make_job(s, fs, ds, d_table, nh, p, d_work);
   const int nsm = device_sms();
-  tc_build_rs<<<nsm * 8, 256, 0, stream>>>(T, nullptr);
-  tc_build_c<<<nsm * 8, 256, 0, stream>>>(T, nullptr);
+  launch_table_builders(T, nullptr, 1, p.stages, factor_smem_rs(p), factor_smem_c(p), nsm, stream);
   cudaError_t le = cudaGetLastError();
   if (le != cudaSuccess) return le;
 
@@ -1322,6 +1482,11 @@ size_t tc_batch_plan(const TcBatchInput* in, int nfields, TcBatchPlan* out) {
   bp.ti = ti;
   bp.tj = tj;
   bp.ntile_max = ntile_max;
+  for (const TcPlan& p : bp.plans) {
+    bp.smem_rs = std::max(bp.smem_rs, factor_smem_rs(p));
+    bp.smem_c = std::max(bp.smem_c, factor_smem_c(p));
+    bp.max_stages = std::max(bp.max_stages, p.stages);
+  }
   bp.num_items = static_cast<int>(items);
   bp.off_items = off;
   off = align(off + sizeof(int2) * static_cast<size_t>(items));
@@ -1362,14 +1527,11 @@ cudaError_t tc_batch_launch(const TcBatchPlan& bp, void* d_work, cudaStream_t st
   uint8_t* work = static_cast<uint8_t*>(d_work);
   const int nsm = device_sms();
   const TableJob* jobs = reinterpret_cast<const TableJob*>(work + bp.off_jobs);
-  const int gx = std::max(1, std::min(64, nsm * 8 / std::max(1, bp.nfields)));
-  dim3 grid(gx, bp.nfields);
   TableJob none{};
   int* status = reinterpret_cast<int*>(work + bp.off_status);
   cudaError_t e = cudaMemsetAsync(status, 0, 2 * sizeof(int), stream);
   if (e != cudaSuccess) return e;
-  tc_build_rs<<<grid, 256, 0, stream>>>(none, jobs);
-  tc_build_c<<<grid, 256, 0, stream>>>(none, jobs);
+  launch_table_builders(none, jobs, bp.nfields, bp.max_stages, bp.smem_rs, bp.smem_c, nsm, stream);
   e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   TcKernelArgs A{};
