@@ -516,6 +516,7 @@ struct DeviceWalk {
   const SampleEntry* ent = nullptr;
   size_t nent = 0;
   std::vector<SampleEntry> owned;
+  std::vector<Draws> draws;  // kept harmonics' draws; their rows are computed after the walk
   size_t ei = 0;
   long long pos = 0, open = 0, pass_end = 0;
   int kept = 0, l = 0;
@@ -547,7 +548,7 @@ struct DeviceWalk {
         d.ra[1] = e.r[5];
         d.rb[0] = e.r[6];
         d.rb[1] = e.r[7];
-        harmonic_row(d, s->ndim, p->cl, table + 5 * static_cast<size_t>(kept));
+        draws.push_back(d);
         ++kept;
         pos = e.q + 4;
         break;
@@ -717,6 +718,29 @@ int srm_sample_device_batch(int nfields, const scarf_srm_params* p, const scarf_
     if (pairs_used) pairs_used[f] = w.pos;
     open_total += w.open;
   }
+  // Table rows from the kept draws (libm trig per row), spread over host
+  // threads in blocks of rows; each row depends on its own draw only.
+  std::vector<long long> rbeg(nfields + 1, 0);
+  for (int f = 0; f < nfields; ++f) rbeg[f + 1] = rbeg[f] + walks[f].kept;
+  constexpr long long kRowBlock = 2048;
+  const long long nblocks = (rbeg[nfields] + kRowBlock - 1) / kRowBlock;
+  std::atomic<long long> next_block{0};
+  auto rows = [&]() {
+    for (long long b = next_block.fetch_add(1); b < nblocks; b = next_block.fetch_add(1)) {
+      const long long r0 = b * kRowBlock, r1 = std::min(rbeg[nfields], r0 + kRowBlock);
+      int f = static_cast<int>(std::upper_bound(rbeg.begin(), rbeg.end(), r0) - rbeg.begin()) - 1;
+      for (long long r = r0; r < r1; ++r) {
+        while (r >= rbeg[f + 1]) ++f;
+        const long long i = r - rbeg[f];
+        harmonic_row(walks[f].draws[i], s[f].ndim, p[f].cl, tables[f] + 5 * i);
+      }
+    }
+  };
+  const int nrow_thr = static_cast<int>(std::max<long long>(1, std::min<long long>(host_threads(), nblocks)));
+  std::vector<std::thread> rpool;
+  for (int t = 1; t < nrow_thr; ++t) rpool.emplace_back(rows);
+  rows();
+  for (auto& th : rpool) th.join();
   if (uncertain) *uncertain = open_total;
   return 0;
 }
