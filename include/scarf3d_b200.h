@@ -92,7 +92,7 @@ int scarf_set_tc_chunk(int harmonics);
  * tensor-core form, no rescale and no taper: the field is copied to the host
  * in slabs (a column tile x a run of row blocks, about items_per_slab work
  * items of 128 x <=256 points each) while the kernel computes the rest.
- * 1 = default slab size (256 items), >= 2 = that size, 0 = copy the whole
+ * 1 = default slab size (64 items), >= 2 = that size, 0 = copy the whole
  * field after the kernel. The field is identical either way. */
 int scarf_set_output_overlap(int items_per_slab);
 
@@ -131,8 +131,8 @@ int scarf_srm_sample_device(const scarf_srm_params *p, const scarf_srm_setup *s,
 /* scarf_srm_sample_device for nfields fields at once (p[f], s[f] -> tables[f]
  * with room for p[f].nharm rows; n_kept[f], pairs_used[f] per field, may be
  * NULL for pairs_used; *host_decided sums the host-decided pairs). The first
- * pass of every field runs in one count and one write launch; the tables are
- * bit-identical to scarf_srm_sample_device's. */
+ * pass of every field runs in one scan launch and one compaction launch; the
+ * tables are bit-identical to scarf_srm_sample_device's. */
 int scarf_srm_sample_device_batch(int nfields, const scarf_srm_params *p, const scarf_srm_setup *s,
                                   float *const *tables, int *n_kept, long long *pairs_used, long long *host_decided,
                                   void *stream);

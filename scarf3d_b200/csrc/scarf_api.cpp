@@ -48,6 +48,10 @@ int cuda_fail(cudaError_t e, const char* what) {
   } while (0)
 
 // ------------------------------------------------------------------ config --
+// Work items per output slab of the overlapped copy-out: the last slab is
+// copied after the kernel ends, so slabs are kept small (64 items of a
+// 512^3 field: 8 MB).
+constexpr int kDefaultSlabItems = 64;
 struct Config {
   int nharm = 10000;  // scarflib_srm.f90:90
   int form = SCARF_FORM_AUTO;
@@ -56,7 +60,7 @@ struct Config {
   int threads = 0;
   int sampler = SCARF_SAMPLER_AUTO;
   bool kernel_timing = false;
-  int overlap_items = 256;  // work items per slab copied out while the kernel runs; 0 = off
+  int overlap_items = kDefaultSlabItems;  // work items per slab copied out while the kernel runs; 0 = off
 };
 Config g_cfg;
 float g_last_kernel_ms = 0.0f;
@@ -948,7 +952,7 @@ int scarf_set_tc_chunk(int harmonics) {
 int scarf_set_output_overlap(int items_per_slab) {
   if (items_per_slab < 0) return fail(SCARF_ERR_ARG, "items_per_slab must be >= 0");
   std::lock_guard<std::mutex> lk(g_mu);
-  g_cfg.overlap_items = items_per_slab == 1 ? 256 : items_per_slab;
+  g_cfg.overlap_items = items_per_slab == 1 ? kDefaultSlabItems : items_per_slab;
   return SCARF_OK;
 }
 
