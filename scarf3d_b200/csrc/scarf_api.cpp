@@ -816,7 +816,7 @@ int scarf_srm_direct_points(const scarf_srm_setup* s, const float* d_x, const fl
   return rc;
 }
 
-// Device-field entry points let the longer of y and z be the column axis
+// Device-field entry points let the longest axis be the column axis
 // (wider column tiles); the same rule sizes their workspace.
 size_t scarf_srm_tc_workspace_bytes(int ndim, const int n[3], int nh) {
   TcPlan p{};

@@ -22,8 +22,8 @@ cudaError_t launch_direct_points(const scarf_srm_setup& s, const float* d_x, con
 // Geometry of one structured field in the factorised form:
 //   out[i*sr + j*ss + k*sc] = scale * Re sum_h R_h(i) S_h(j) C_h(k)
 // with (i, j, k) along the physical axes (ax_r, ax_s, ax_c): (x, y, z) by
-// default, (x, z, y) when the plan permutes, (x, z, y) with the single z
-// plane as j in 2D.
+// default ((x, z, y) in 2D, the single z plane as j); a permuting plan takes
+// the longest axis as k: (x, z, y) or (y, z, x).
 struct TcPlan {
   int n1, n2, n3;        // logical extents
   int ti, tj;            // row tile = ti x tj = 128 rows over (i, j)
@@ -50,8 +50,8 @@ constexpr int kTcVariantSingleTmemA = 2;  // one CTA per tile, A in tensor memor
 void tc_set_variant(int v);
 
 // tj_force > 0 fixes the row tile to (128 / tj_force) x tj_force.
-// permute: let the longer of y and z be the column axis (device fields of a
-// batch; the default layout keeps k = z, which the slab copy-out relies on).
+// permute: let the longest axis be the column axis (device-field entry
+// points; the default layout keeps k = z, which the slab copy-out relies on).
 bool tc_make_plan(int ndim, const int n[3], int nh, TcPlan* plan, int tj_force = 0, bool permute = false);
 // Harmonics accumulated in tensor memory before each FP32 drain (rounded up
 // to whole pipeline stages); 0 restores the default.

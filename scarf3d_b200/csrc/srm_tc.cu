@@ -1339,18 +1339,22 @@ void tc_set_chunk_harmonics(int harmonics) {
 bool tc_make_plan(int ndim, const int n[3], int nh, TcPlan* P, int tj_force, bool permute) {
   if (nh <= 0 || n[0] <= 0 || n[1] <= 0 || n[2] <= 0) return false;
   TcPlan p{};
-  // Rows (i, j) over x and one of y / z, columns k over the other: by default
-  // k = z (y in 2D, whose single z plane becomes j); with `permute` the longer
-  // of y and z becomes the column axis, for wider column tiles.
-  p.ax_r = 0;
-  if (ndim == 3) {
-    const bool swap = permute && n[1] > n[2];
-    p.ax_s = swap ? 2 : 1;
-    p.ax_c = swap ? 1 : 2;
-  } else {
-    p.ax_s = 2;
-    p.ax_c = 1;
+  // Rows (i, j) over two axes, columns k over the third. By default k = z
+  // (y in 2D, whose single z plane becomes j) and i = x. With `permute` the
+  // longest axis becomes the column axis (ties keep z, then y), for wide
+  // column tiles: generation and the per-instruction MMA cost amortise over
+  // more columns. The rows take the other two axes, the faster-varying one as
+  // i; with x as the column axis the field stores are strided, a small cost
+  // next to the sum.
+  int ax_c = (ndim == 3) ? 2 : 1;
+  if (permute) {
+    const int cand[3] = {ax_c, ax_c == 2 ? 1 : 2, 0};  // preference on ties
+    for (int c : cand)
+      if (c < (ndim == 3 ? 3 : 2) && n[c] > n[ax_c]) ax_c = c;
   }
+  p.ax_c = ax_c;
+  p.ax_r = (ax_c == 0) ? 1 : 0;
+  p.ax_s = (ax_c == 2) ? 1 : 2;
   const long long stride[3] = {1, n[0], static_cast<long long>(n[0]) * n[1]};
   p.n1 = n[p.ax_r];
   p.n2 = n[p.ax_s];

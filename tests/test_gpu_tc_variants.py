@@ -102,9 +102,9 @@ def test_unknown_variant_is_rejected():
         sb.set_tc_variant(7)
 
 
-@pytest.mark.parametrize("n", [[64, 200, 40], [96, 130, 33], [40, 257, 100]])
-def test_y_long_grids_take_y_as_the_column_axis(n):
-    # The device-field entry point lets the longer of y and z be the column
+@pytest.mark.parametrize("n", [[64, 200, 40], [96, 130, 33], [40, 257, 100], [257, 40, 64], [300, 96, 17]])
+def test_long_axis_grids_take_it_as_the_column_axis(n):
+    # The device-field entry point lets the longest axis be the column
     # axis: the field must still agree with the FP64 oracle in the caller's
     # x-fastest layout, for every kernel form.
     kw = dict(acf=0, nharm=600, seed=31, hurst=0.3, sigma=0.05, ds=40.0, cl=[1500.0, 1500.0, 1500.0])
