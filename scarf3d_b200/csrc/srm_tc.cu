@@ -613,6 +613,15 @@ __global__ void __launch_bounds__(kThreads, 1) srm_tc_kernel(const TcKernelArgs 
       int s = 0;
       uint32_t ph = 0, chunk = 0;
       bool issued_any = false;
+      // Stage slot's B image landed and its A tile generated. Both phases are
+      // probed back to back first (their round trips overlap); the bounded
+      // waits run only when one is still open.
+      auto stage_inputs_ready = [&](int sl, uint32_t par) -> bool {
+        const bool f = mbar_test_wait(&full[sl], par);
+        const bool g = mbar_test_wait(&agen[sl], par);
+        if (f && g) return true;
+        return mbar_wait_bounded(&full[sl], par, A.status) && mbar_wait_bounded(&agen[sl], par, A.status);
+      };
       for (uint32_t it = 0; ok; ++it) {
         const int q = it % kItemRing;
         if (!mbar_wait_bounded(&item_full[q], (it / kItemRing) & 1, A.status)) {
@@ -631,15 +640,22 @@ __global__ void __launch_bounds__(kThreads, 1) srm_tc_kernel(const TcKernelArgs 
             ok = false;
             break;
           }
-          tc_fence_after();
+          // Inputs of the chunk's first stage. Each later stage's inputs are
+          // checked between the two K halves of the stage before it, while
+          // the tensor core still holds queued MMAs: an issuing thread that
+          // checked them after its last MMA would leave the tensor pipe idle
+          // for the round trips of the checks.
+          if (!stage_inputs_ready(s, ph)) {
+            ok = false;
+            break;
+          }
           for (int k = c0; k < c1; ++k) {
-            if (!mbar_wait_bounded(&full[s], ph, A.status) || !mbar_wait_bounded(&agen[s], ph, A.status)) {
-              ok = false;
-              break;
-            }
             tc_fence_after();
             const uint32_t st = smem_u32(smem + s * A.stage_bytes);
             const uint32_t b_hi = st + A.off_b, b_lo = st + b_lo_off;
+            const int s_next = (s + 1 == S) ? 0 : s + 1;
+            const uint32_t ph_next = (s + 1 == S) ? (ph ^ 1u) : ph;
+            bool next_ok = true;
 #pragma unroll
             for (int kk = 0; kk < 2; ++kk) {
               const uint64_t dbh = umma_smem_desc(b_hi + 32 * kk, 16, 512, kSwizzle64);
@@ -658,12 +674,15 @@ __global__ void __launch_bounds__(kThreads, 1) srm_tc_kernel(const TcKernelArgs 
                 umma_f16(tmem_base, dah, dbl, w.f.idesc, 1u);
                 umma_f16(tmem_base, dal, dbh, w.f.idesc, 1u);
               }
+              if (kk == 0 && k + 1 < c1) next_ok = stage_inputs_ready(s_next, ph_next);
             }
             umma_commit(&empty[s]);
             issued_any = true;
-            if (++s == S) {
-              s = 0;
-              ph ^= 1;
+            s = s_next;
+            ph = ph_next;
+            if (!next_ok) {
+              ok = false;
+              break;
             }
           }
           if (!ok) break;
