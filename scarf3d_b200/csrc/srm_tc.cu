@@ -1023,6 +1023,14 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1) srm_tc_
       int s = 0;
       uint32_t ph = 0, chunk = 0;
       bool issued_any = false;
+      // This CTA's B half landed and both CTAs' A rows (and the odd CTA's B
+      // half, relayed by its forwarder) are in place.
+      auto stage_inputs_ready = [&](int sl, uint32_t par) -> bool {
+        const bool f = mbar_test_wait(&b_full[sl], par);
+        const bool g = mbar_test_wait_cluster(&agen[sl], par);
+        if (f && g) return true;
+        return mbar_wait_bounded(&b_full[sl], par, A.status) && mbar_wait_bounded_cluster(&agen[sl], par, A.status);
+      };
       for (uint32_t it = 0; ok; ++it) {
         int idx;
         if (!take_item(it, idx)) {
@@ -1039,16 +1047,20 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1) srm_tc_
             ok = false;
             break;
           }
-          tc_fence_after();
+          // As in the one-CTA form: the next stage's inputs are checked
+          // between the K halves of the current stage.
+          if (!stage_inputs_ready(s, ph)) {
+            ok = false;
+            break;
+          }
           for (int k = c0; k < c1; ++k) {
-            if (!mbar_wait_bounded(&b_full[s], ph, A.status) || !mbar_wait_bounded_cluster(&agen[s], ph, A.status)) {
-              ok = false;
-              break;
-            }
             tc_fence_after();
             const uint32_t st = smem_u32(smem + s * A.stage_bytes);
             const uint32_t a_hi = st + A.off_a, a_lo = a_hi + kATileBytes;
             const uint32_t b_hi = st + A.off_b, b_lo = st + b_lo_off;
+            const int s_next = (s + 1 == S) ? 0 : s + 1;
+            const uint32_t ph_next = (s + 1 == S) ? (ph ^ 1u) : ph;
+            bool next_ok = true;
 #pragma unroll
             for (int kk = 0; kk < 2; ++kk) {
               const uint64_t dah = umma_smem_desc(a_hi + 32 * kk, 16, 512, kSwizzle64);
@@ -1058,12 +1070,15 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1) srm_tc_
               umma_f16_pair(tmem_base, dah, dbh, w.f.idesc, (k > c0 || kk > 0) ? 1u : 0u);
               umma_f16_pair(tmem_base, dah, dbl, w.f.idesc, 1u);
               umma_f16_pair(tmem_base, dal, dbh, w.f.idesc, 1u);
+              if (kk == 0 && k + 1 < c1) next_ok = stage_inputs_ready(s_next, ph_next);
             }
             umma_commit_pair_both(&empty[s]);
             issued_any = true;
-            if (++s == S) {
-              s = 0;
-              ph ^= 1;
+            s = s_next;
+            ph = ph_next;
+            if (!next_ok) {
+              ok = false;
+              break;
             }
           }
           if (!ok) break;
