@@ -53,6 +53,22 @@ const PowTables& pow_tables() {
   static const PowTables t;
   return t;
 }
+// The device's split of the same transform: g^k, g^(k 2^11), g^(k 2^22).
+std::vector<uint32_t> device_pow_tables() {
+  std::vector<uint32_t> w;
+  w.reserve(2048 + 2048 + 512);
+  uint64_t step = Yarn2::kGen;
+  const int sizes[3] = {2048, 2048, 512};
+  for (int part = 0; part < 3; ++part) {
+    uint64_t v = 1;
+    for (int k = 0; k < sizes[part]; ++k) {
+      w.push_back(static_cast<uint32_t>(v));
+      v = Yarn2::mulmod(v, step);
+    }
+    for (int b = 0; b < 11; ++b) step = Yarn2::mulmod(step, step);  // step^(2^11)
+  }
+  return w;
+}
 }  // namespace
 
 uint32_t Yarn2::output(uint64_t r) {
@@ -452,8 +468,8 @@ bool ensure_sampler_device(DeviceSamplerState& D) {
     D.device = dev;
   }
   if (!D.tables) {
-    const PowTables& t = pow_tables();
-    if (sampler_upload_tables(t.lo.data(), t.hi.data()) != cudaSuccess) return false;
+    static const std::vector<uint32_t> t = device_pow_tables();
+    if (sampler_upload_tables(t.data()) != cudaSuccess) return false;
     D.tables = true;
   }
   return true;
@@ -601,7 +617,9 @@ int srm_sample_device_batch(int nfields, const scarf_srm_params* p, const scarf_
   // First pass of every field in one scan: each thread keeps up to `cap`
   // candidates in its own slot (cap sized from the expected count, with a
   // wide Poisson margin); a gather launch compacts them. The fields share
-  // ~300k threads (2 048 at least each), 256 to 65 536 pairs per thread.
+  // ~300k threads or more (2 048 at least each), 256 to 4 096 pairs per
+  // thread: each thread's pairs form one serial chain of generator steps, so
+  // longer chains leave the scan waiting on its slowest threads.
   const long long thread_goal = std::max<long long>(2048, 148LL * 2048 / nfields);
   std::vector<SamplerArgs> args(nfields);
   std::vector<long long> tbeg(nfields + 1, 0), sbeg(nfields + 1, 0);
@@ -611,7 +629,7 @@ int srm_sample_device_batch(int nfields, const scarf_srm_params* p, const scarf_
     A.q_begin = 0;
     A.q_count = first_pass_pairs(p[f], acc[f]);
     A.pairs_per_thread =
-        static_cast<int>(std::min<long long>(65536, std::max<long long>(256, A.q_count / thread_goal)));
+        static_cast<int>(std::min<long long>(4096, std::max<long long>(256, A.q_count / thread_goal)));
     A.nthreads = (A.q_count + A.pairs_per_thread - 1) / A.pairs_per_thread;
     const double lambda = A.pairs_per_thread * std::min(1.0, acc[f]);
     A.cap = static_cast<int>(std::ceil(1.25 * lambda + 6.0 * std::sqrt(lambda) + 8.0));
@@ -621,17 +639,18 @@ int srm_sample_device_batch(int nfields, const scarf_srm_params* p, const scarf_
   const long long T = tbeg[nfields];
   const int err = -2 - nfields;
   if (D.counts.ensure(sizeof(int) * T) != cudaSuccess || D.offsets.ensure(sizeof(long long) * T) != cudaSuccess ||
-      D.slots.ensure(sizeof(SampleEntry) * sbeg[nfields]) != cudaSuccess ||
+      D.slots.ensure(sizeof(unsigned long long) * sbeg[nfields]) != cudaSuccess ||
       D.batch_args.ensure(sizeof(SamplerArgs) * nfields) != cudaSuccess ||
       D.batch_tbeg.ensure(sizeof(long long) * (nfields + 1)) != cudaSuccess)
     return err;
   int* d_counts = static_cast<int*>(D.counts.p);
   long long* d_offsets = static_cast<long long*>(D.offsets.p);
-  SampleEntry* d_slots = static_cast<SampleEntry*>(D.slots.p);
+  unsigned long long* d_slots = static_cast<unsigned long long*>(D.slots.p);
   for (int f = 0; f < nfields; ++f) {
     args[f].counts = d_counts + tbeg[f];
     args[f].offsets = nullptr;
-    args[f].out = d_slots + sbeg[f];
+    args[f].out = nullptr;
+    args[f].keys = d_slots + sbeg[f];
   }
   if (cudaMemcpyAsync(D.batch_args.p, args.data(), sizeof(SamplerArgs) * nfields, cudaMemcpyHostToDevice, stream) !=
           cudaSuccess ||

@@ -125,16 +125,20 @@ struct SamplerArgs {
   int* counts;               // [nthreads]
   const long long* offsets;  // [nthreads]
   SampleEntry* out;
-  int cap;                   // batch mode 2: entries per thread slot (out + t * cap), counts kept in full
+  int cap;                   // batch mode 2: candidates per thread slot (keys + t * cap), counts kept in full
+  unsigned long long* keys;  // batch mode 2: candidate keys (pair index << 2 | flag)
 };
-cudaError_t sampler_upload_tables(const unsigned int* lo, const unsigned int* hi);
+// Output-transform tables of the generator: g^k (k < 2048), g^(k 2^11)
+// (k < 2048) and g^(k 2^22) (k < 512) mod 2^31 - 1, 4 608 words in that order.
+cudaError_t sampler_upload_tables(const unsigned int* pow3);
 cudaError_t launch_sampler(const SamplerArgs& args, cudaStream_t stream);
 // One pass for each of nfields fields in a single launch: d_fields[f] holds
 // field f's pass (its counts / offsets pointers already at the field's slice),
 // d_tbeg the prefix of the fields' thread counts (nfields + 1 entries).
 cudaError_t launch_sampler_batch(const SamplerArgs* d_fields, const long long* d_tbeg, int nfields, long long total,
                                  int write, cudaStream_t stream);
-// Compaction after a write = 2 batch pass (see SamplerArgs::cap).
+// Compaction after a write = 2 batch pass (see SamplerArgs::cap): each
+// kept key becomes a full entry, its draws regenerated from the stream.
 cudaError_t launch_sampler_gather(const SamplerArgs* d_fields, const long long* d_tbeg, int nfields, long long total,
                                   const long long* d_offsets, SampleEntry* d_dst, cudaStream_t stream);
 

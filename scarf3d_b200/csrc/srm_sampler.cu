@@ -15,6 +15,12 @@
 //
 // Two passes over the same range: the first counts candidates per thread,
 // the host turns the counts into offsets, the second writes them.
+//
+// The generator's output transform g^t mod m is evaluated from three tables
+// of exact residues, g^(t & 2047) * g^(((t >> 11) & 2047) * 2^11) *
+// g^((t >> 22) * 2^22), 18 KB that every block holds in shared memory: two
+// large tables in global memory made each draw two dependent random L2
+// reads, which bounded the scan.
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -28,8 +34,9 @@ constexpr uint64_t kMod = 2147483647ull;
 constexpr uint64_t kA1 = 1498809829ull;
 constexpr uint64_t kA2 = 1160990996ull;
 
-__device__ uint32_t g_pow_lo[1 << 16];  // g^k mod m, k < 2^16
-__device__ uint32_t g_pow_hi[1 << 15];  // g^(k 2^16) mod m, k < 2^15
+constexpr int kPow0 = 2048, kPow1 = 2048, kPow2 = 512;  // t < 2^31
+constexpr int kPowWords = kPow0 + kPow1 + kPow2;
+__device__ uint32_t g_pow[kPowWords];  // g^k, g^(k 2^11), g^(k 2^22) mod m
 
 __device__ __forceinline__ uint64_t mulmod(uint64_t a, uint64_t b) {
   uint64_t p = a * b;  // < 2^62
@@ -37,19 +44,37 @@ __device__ __forceinline__ uint64_t mulmod(uint64_t a, uint64_t b) {
   p = (p & kMod) + (p >> 31);
   return p >= kMod ? p - kMod : p;
 }
+// x mod m for x < 2m + 2 (unsigned wrap-around makes x - m huge when x < m).
+__device__ __forceinline__ uint32_t sub_m(uint32_t x) { return min(x, x - static_cast<uint32_t>(kMod)); }
+// a * b mod m for a, b < 2^31, in 32-bit operations: the 62-bit product
+// hi:lo folds once into (p >> 31) + (p & m) < 2^32 - 1, then at most two
+// subtractions of m.
+__device__ __forceinline__ uint32_t mulmod32(uint32_t a, uint32_t b) {
+  const uint32_t lo = a * b, hi = __umulhi(a, b);
+  const uint32_t f = __funnelshift_l(lo, hi, 1) + (lo & static_cast<uint32_t>(kMod));
+  return sub_m(sub_m(f));
+}
 __device__ __forceinline__ uint64_t addmod(uint64_t a, uint64_t b) {
   const uint64_t s = a + b;
   return s >= kMod ? s - kMod : s;
 }
 
+// The block's copy of g_pow in shared memory.
+__device__ __forceinline__ void load_pow(uint32_t* sp) {
+  for (int i = threadIdx.x; i < kPowWords; i += blockDim.x) sp[i] = g_pow[i];
+  __syncthreads();
+}
+
 struct Gen {
   uint64_t r0, r1;
+  const uint32_t* sp;  // shared-memory power tables
   __device__ __forceinline__ uint32_t next() {
-    const uint64_t t = addmod(mulmod(kA1, r0), mulmod(kA2, r1));
+    const uint32_t u = sub_m(mulmod32(static_cast<uint32_t>(kA1), static_cast<uint32_t>(r0)) +
+                             mulmod32(static_cast<uint32_t>(kA2), static_cast<uint32_t>(r1)));
     r1 = r0;
-    r0 = t;
-    if (t == 0) return 0u;
-    return static_cast<uint32_t>(mulmod(g_pow_lo[t & 0xFFFFu], g_pow_hi[t >> 16]));
+    r0 = u;
+    if (u == 0) return 0u;
+    return mulmod32(mulmod32(sp[u & 2047u], sp[kPow0 + ((u >> 11) & 2047u)]), sp[kPow0 + kPow1 + (u >> 22)]);
   }
   __device__ __forceinline__ void jump(uint64_t n) {
     uint64_t m00 = kA1, m01 = kA2, m10 = 1, m11 = 0;
@@ -99,14 +124,15 @@ __device__ __forceinline__ int classify(const SamplerArgs& A, float r1, float r2
 
 // Pairs [q0, q1) of local thread t of one field's pass: count (write = 0),
 // write the candidate entries at the thread's offset (write = 1), or write
-// up to A.cap of them into the thread's own slot out + t * cap while
-// counting them all (write = 2: one scan instead of two; a count above cap
-// tells the host to redo that field).
-__device__ __forceinline__ void sample_range(const SamplerArgs& A, long long t, int write) {
+// up to A.cap candidate keys (pair index << 2 | flag, 8 bytes) into the
+// thread's own slot keys + t * cap while counting them all (write = 2: one
+// scan instead of two; a count above cap tells the host to redo that field;
+// the gather launch rebuilds full entries from the keys).
+__device__ __forceinline__ void sample_range(const SamplerArgs& A, long long t, int write, const uint32_t* sp) {
   const long long q0 = A.q_begin + t * A.pairs_per_thread;
   long long q1 = q0 + A.pairs_per_thread;
   if (q1 > A.q_begin + A.q_count) q1 = A.q_begin + A.q_count;
-  Gen g{A.r0, A.r1};
+  Gen g{A.r0, A.r1, sp};
   g.jump(2ull * static_cast<uint64_t>(q0));
   int count = 0;
   long long slot = write == 1 ? A.offsets[t] : (write == 2 ? t * A.cap : 0);
@@ -117,7 +143,9 @@ __device__ __forceinline__ void sample_range(const SamplerArgs& A, long long t, 
     const int c = classify(A, r1, r2);
     if (c == 0) continue;
     ++count;
-    if (write && slot < slot_end) {
+    if (write == 2) {
+      if (slot < slot_end) A.keys[slot++] = (static_cast<unsigned long long>(q) << 2) | static_cast<unsigned>(c);
+    } else if (write && slot < slot_end) {
       SampleEntry e;
       e.q = q;
       e.flag = c;
@@ -132,15 +160,19 @@ __device__ __forceinline__ void sample_range(const SamplerArgs& A, long long t, 
 }
 
 __global__ void sampler_kernel(const SamplerArgs A) {
+  __shared__ uint32_t sp[kPowWords];
+  load_pow(sp);
   const long long t = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (t >= A.nthreads) return;
-  sample_range(A, t, A.write);
+  sample_range(A, t, A.write, sp);
 }
 
 // Passes of many fields in one launch: global thread t belongs to the field
 // f with tbeg[f] <= t < tbeg[f + 1] (binary search over the prefix).
 __global__ void sampler_batch_kernel(const SamplerArgs* fields, const long long* tbeg, int nfields,
                                      long long total, int write) {
+  __shared__ uint32_t sp[kPowWords];
+  load_pow(sp);
   const long long t = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (t >= total) return;
   int lo = 0, hi = nfields - 1;
@@ -150,13 +182,17 @@ __global__ void sampler_batch_kernel(const SamplerArgs* fields, const long long*
     else hi = mid - 1;
   }
   const SamplerArgs A = fields[lo];
-  sample_range(A, t - tbeg[lo], write);
+  sample_range(A, t - tbeg[lo], write, sp);
 }
 
 // Compacts the per-thread slots of a write = 2 pass: thread t's min(count,
-// cap) entries move to dst + offsets[t] (global thread index t).
+// cap) keys become entries at dst + offsets[t] (global thread index t), the
+// pair and the three after it drawn again by jumping a generator copy from
+// one candidate to the next.
 __global__ void sampler_gather_kernel(const SamplerArgs* fields, const long long* tbeg, int nfields, long long total,
                                       const long long* offsets, SampleEntry* dst) {
+  __shared__ uint32_t sp[kPowWords];
+  load_pow(sp);
   const long long t = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (t >= total) return;
   int lo = 0, hi = nfields - 1;
@@ -168,17 +204,29 @@ __global__ void sampler_gather_kernel(const SamplerArgs* fields, const long long
   const SamplerArgs& A = fields[lo];
   const long long tl = t - tbeg[lo];
   const int n = min(A.counts[tl], A.cap);
-  const SampleEntry* src = A.out + tl * A.cap;
+  const unsigned long long* src = A.keys + tl * A.cap;
   SampleEntry* o = dst + offsets[t];
-  for (int i = 0; i < n; ++i) o[i] = src[i];
+  Gen g{A.r0, A.r1, sp};
+  unsigned long long at = 0;  // draw index g stands at; keys ascend in q
+  for (int i = 0; i < n; ++i) {
+    const unsigned long long key = src[i];
+    const unsigned long long q = key >> 2;
+    g.jump(2ull * q - at);
+    at = 2ull * q;
+    SampleEntry e;
+    e.q = static_cast<long long>(q);
+    e.flag = static_cast<int>(key & 3u);
+    e.pad = 0;
+    Gen look = g;  // candidates may follow each other within 4 pairs
+    for (int k = 0; k < 8; ++k) e.r[k] = to_u01(look.next());
+    o[i] = e;
+  }
 }
 
 }  // namespace
 
-cudaError_t sampler_upload_tables(const uint32_t* lo, const uint32_t* hi) {
-  cudaError_t e = cudaMemcpyToSymbol(g_pow_lo, lo, sizeof(uint32_t) * (1u << 16));
-  if (e == cudaSuccess) e = cudaMemcpyToSymbol(g_pow_hi, hi, sizeof(uint32_t) * (1u << 15));
-  return e;
+cudaError_t sampler_upload_tables(const uint32_t* pow3) {
+  return cudaMemcpyToSymbol(g_pow, pow3, sizeof(uint32_t) * kPowWords);
 }
 
 cudaError_t launch_sampler_batch(const SamplerArgs* d_fields, const long long* d_tbeg, int nfields, long long total,
