@@ -61,7 +61,21 @@ def build(verbose_ptxas: bool = False) -> Path:
     if _needs(LIB, objs):
         _run([NVCC] + ARCH + ["-shared", "-cudart", "static", "-o", str(LIB)] + [str(o) for o in objs]
              + ["-lpthread"])
+    build_standalone()
     return LIB
+
+
+STANDALONE_SRC = PKG / "standalone" / "scarf3d_standalone.cpp"
+STANDALONE = PKG / "scarf3d_standalone"
+
+
+def build_standalone() -> Path:
+    """The keyword-file driver (counterpart of the reference's standalone
+    application), linked against the library next to it."""
+    if _needs(STANDALONE, [STANDALONE_SRC, LIB] + sorted((ROOT / "include").glob("*.h"))):
+        _run([CXX, "-O2", "-std=c++17", "-Wall"] + INCLUDES + [str(STANDALONE_SRC), f"-L{PKG}", "-lscarf3d_b200",
+              "-Wl,-rpath,$ORIGIN", "-o", str(STANDALONE)])
+    return STANDALONE
 
 
 def build_oracle() -> Path:

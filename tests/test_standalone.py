@@ -1,0 +1,139 @@
+"""The keyword-file driver (counterpart of the reference's standalone
+application, standalone/main.f90): input parsing, the reference's defaults,
+checks and messages on the CPU (--check mode, no device work), and on a GPU
+a full run whose random_field.bin must equal the library's own field."""
+import importlib.util
+import subprocess
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+ROOT = Path(__file__).resolve().parent.parent
+
+BASE = {
+    "dimension": "3",
+    "npts": "24 20 16",
+    "ds": "25.",
+    "cl": "2000. 2000. 1000.",
+    "sigma": "0.05",
+    "acf": "0",
+    "hurst": "0.5",
+    "seed": "1234",
+    "method": "1",
+}
+
+
+@pytest.fixture(scope="module")
+def exe():
+    spec = importlib.util.spec_from_file_location("scarf3d_b200_build", ROOT / "scarf3d_b200" / "build.py")
+    b = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(b)
+    if not b.LIB.exists():
+        pytest.skip("library not built")
+    return b.build_standalone()
+
+
+def write_input(path: Path, params: dict, extra: str = "") -> Path:
+    text = "".join(f"# {k}\n{v}\n" for k, v in params.items()) + extra
+    path.write_text(text)
+    return path
+
+
+def run(exe, *args, cwd=None):
+    return subprocess.run([str(exe), *map(str, args)], capture_output=True, text=True, cwd=cwd, timeout=300)
+
+
+def test_no_argument_asks_for_an_input_file(exe):
+    r = run(exe)
+    assert r.returncode == 0
+    assert "Please specify an input file!" in r.stdout
+
+
+def test_check_prints_the_summary(exe, tmp_path):
+    r = run(exe, "--check", write_input(tmp_path / "in.txt", BASE))
+    assert r.returncode == 0, r.stdout
+    assert "Summary of input parameters" in r.stdout
+    row = [ln for ln in r.stdout.splitlines() if ln.startswith(" Number of points")][0]
+    assert row.split("|")[1].split() == ["24", "20", "16"]
+    assert "Hurst exponent" in r.stdout
+    assert "MPI processes for I/O     |           2" in r.stdout  # default nwriters
+
+
+def test_list_directed_values(exe, tmp_path):
+    # Values may continue on the following lines, be separated by commas and
+    # use repeat counts, as Fortran list-directed input allows.
+    p = dict(BASE, npts="24,\n20 16", cl="3*1500.")
+    r = run(exe, "--check", write_input(tmp_path / "in.txt", p))
+    assert r.returncode == 0, r.stdout
+    row = [ln for ln in r.stdout.splitlines() if ln.startswith(" Correlation length")][0]
+    assert row.split("|")[1].split() == ["1500.000"] * 3
+    row = [ln for ln in r.stdout.splitlines() if ln.startswith(" Number of points")][0]
+    assert row.split("|")[1].split() == ["24", "20", "16"]
+
+
+def test_indented_descriptor_is_not_a_descriptor(exe, tmp_path):
+    # The reference compares the whole line (trailing blanks trimmed only).
+    p = dict(BASE)
+    del p["seed"]
+    r = run(exe, "--check", write_input(tmp_path / "in.txt", p, extra="  # seed\n1234\n"))
+    assert r.returncode == 1
+    assert "seed number (any integer not equal zero) not specified" in r.stdout
+
+
+@pytest.mark.parametrize("change,message", [
+    ({"dimension": "4"}, "dimension must be equal to 2 or 3"),
+    ({"npts": "24 0 16"}, "number of points must be larger than zero"),
+    ({"acf": "2"}, "accepted ACF are Von Karman (0) and Gaussian (1)"),
+    ({"mute": "-1."}, "mute parameter can be only positive"),
+    ({"taper": "-1."}, "taper parameter can be only positive"),
+    ({"rescale": "2"}, "rescale parameter can be only off (0) or on (1)"),
+    ({"nwriters": "0"}, "nwriters parameter can be only larger than zero"),
+    ({"sigma": "0."}, "standard deviation (sigma) must be larger than zero"),
+    ({"ds": "-25."}, "grid-step must be larger than zero"),
+    ({"seed": "0"}, "seed number (any integer not equal zero) not specified"),
+])
+def test_checks_and_messages(exe, tmp_path, change, message):
+    r = run(exe, "--check", write_input(tmp_path / "in.txt", dict(BASE, **change)))
+    assert r.returncode == 1
+    assert message in r.stdout
+
+
+def test_poi_outside_the_model(exe, tmp_path):
+    r = run(exe, "--check", write_input(tmp_path / "in.txt", BASE, extra="# poi\n100. -5. 30.\n"))
+    assert r.returncode == 1
+    assert "POI must be inside the model" in r.stdout
+
+
+def test_hurst_range_is_not_checked(exe, tmp_path):
+    # standalone/main.f90:333 tests hurst < 0 .and. hurst > 1, which no value
+    # satisfies; the driver keeps that behaviour.
+    r = run(exe, "--check", write_input(tmp_path / "in.txt", dict(BASE, hurst="1.7")))
+    assert r.returncode == 0
+
+
+@pytest.mark.gpu
+def test_run_writes_the_library_field(exe, tmp_path):
+    import scarf3d_b200 as sb
+    r = run(exe, write_input(tmp_path / "in.txt", BASE), cwd=tmp_path)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "Program completed successfully" in r.stdout
+    got = np.fromfile(tmp_path / "random_field.bin", dtype=np.float32)
+    n = [24, 20, 16]
+    assert got.size == np.prod(n)
+    sb.scarf_initialize(fs=[1, 1, 1], fe=n, ds=25.0, acf=0, cl=[2000.0, 2000.0, 1000.0], sigma=0.05, method=1,
+                        hurst=0.5)
+    try:
+        ref, stats = sb.scarf_execute(1234)
+    finally:
+        sb.scarf_finalize()
+    assert np.array_equal(got.view(np.uint32), np.asarray(ref, np.float32).view(np.uint32))
+    row = [ln for ln in r.stdout.splitlines() if "Discrete standard deviation" in ln][0]
+    assert abs(float(row.split("|")[1]) - stats[2]) < 1e-4
+
+
+@pytest.mark.gpu
+def test_fim_method_is_reported(exe, tmp_path):
+    r = run(exe, write_input(tmp_path / "in.txt", dict(BASE, method="0")), cwd=tmp_path)
+    assert r.returncode == 1
+    assert "set '# method' to 1 (SRM)" in r.stdout
