@@ -633,6 +633,9 @@ int srm_sample_device_batch(int nfields, const scarf_srm_params* p, const scarf_
     A.nthreads = (A.q_count + A.pairs_per_thread - 1) / A.pairs_per_thread;
     const double lambda = A.pairs_per_thread * std::min(1.0, acc[f]);
     A.cap = static_cast<int>(std::ceil(1.25 * lambda + 6.0 * std::sqrt(lambda) + 8.0));
+    // Test hook: a smaller slot forces the overflow path (fields redone with
+    // their own passes), which the margin above makes vanishingly rare.
+    if (const char* e = std::getenv("SCARF3D_B200_SAMPLER_SLOT_CAP")) A.cap = std::max(1, std::min(A.cap, std::atoi(e)));
     tbeg[f + 1] = tbeg[f] + A.nthreads;
     sbeg[f + 1] = sbeg[f] + A.nthreads * A.cap;
   }

@@ -116,6 +116,18 @@ def test_batched_device_sampler_matches_per_field_sampler():
         assert np.array_equal(t.view(np.uint32), ref.view(np.uint32))
 
 
+def test_batched_device_sampler_redoes_fields_whose_slots_overflowed(monkeypatch):
+    # One candidate slot per scan thread: most threads overflow, their fields
+    # are redone with their own passes, and the tables must not change.
+    fields = _batch_fields()
+    ref = sb.sample_device_batch([f[0] for f in fields], [f[1] for f in fields])
+    monkeypatch.setenv("SCARF3D_B200_SAMPLER_SLOT_CAP", "1")
+    got = sb.sample_device_batch([f[0] for f in fields], [f[1] for f in fields])
+    for t, r in zip(got[0], ref[0]):
+        assert np.array_equal(t.view(np.uint32), r.view(np.uint32))
+    assert list(got[1]) == list(ref[1])
+
+
 def test_batched_device_sampler_chains_further_passes():
     fields = _batch_fields()
     sb.check(sb.lib.scarf_set_sampler_pass_pairs(1_000_003))  # first passes run short
