@@ -119,3 +119,31 @@ def test_long_axis_grids_take_it_as_the_column_axis(n):
                        nc=[0.0] * 3, fc=fc)
     ref64 = oracle.sum_structured(oracle.setup(op), [1, 1, 1], n, 40.0, tab, f64=True)
     assert rel_rms(fields[0], ref64) <= 1e-5
+
+
+@pytest.mark.parametrize("nharm", [1, 15, 17])
+@pytest.mark.parametrize("fs,n", [
+    ([1, 1, 1], [1, 1, 1]),        # a single point
+    ([20, 5, 33], [1, 9, 1]),      # one line along y inside a larger domain
+    ([3, 40, 7], [33, 1, 1]),      # one line along x (x becomes the column axis)
+    ([9, 9, 1], [1, 1, 300]),      # one line along z, two column tiles
+    ([2, 60, 61], [2, 3, 5]),      # a corner block smaller than one row tile
+])
+def test_degenerate_blocks_and_tiny_harmonic_counts(fs, n, nharm):
+    # Blocks of one point or one line of a 64 x 64 x 320 domain (a rank's sub-block),
+    # with harmonic counts below, at and just above one 16-harmonic stage:
+    # every kernel form agrees bit for bit and with the FP64 oracle.
+    kw = dict(acf=0, nharm=nharm, seed=5, hurst=0.4, sigma=0.05, ds=50.0, cl=[800.0, 800.0, 800.0])
+    fc = [float(np.float32(m - 1) * np.float32(50.0)) for m in (64, 64, 320)]
+    p = sb.make_params(nc=[0.0, 0.0, 0.0], fc=fc, **kw)
+    s = sb.compute_setup(p)
+    tab, _ = sb.sample(p, s)
+    fields = [_run(v, s, fs, n, 50.0, tab) for v in VARIANTS]
+    for f in fields:
+        assert np.all(np.isfinite(f))
+        assert np.array_equal(f.view(np.uint32), fields[0].view(np.uint32))
+    op = oracle.params(acf=0, nharm=nharm, seed=5, hurst=0.4, sigma=0.05, ds=50.0, dh=50.0, cl=[800.0] * 3,
+                       nc=[0.0] * 3, fc=fc)
+    ref64 = oracle.sum_structured(oracle.setup(op), fs, n, 50.0, tab, f64=True)
+    # absolute bound: 1e-4 of sigma (the bench's 512^3 field sees ~1e-5)
+    assert float(np.max(np.abs(fields[0].astype(np.float64) - ref64))) <= 1e-4 * 0.05
