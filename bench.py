@@ -244,6 +244,12 @@ def run_batched(args, nfields=256):
     outs = [torch.empty(int(np.prod(f["n"])), dtype=torch.float32, device="cuda") for f in spec]
     entries = [dict(setup=f["setup"], fs=[1, 1, 1], n=f["n"], ds=f["ds"], d_table=d.data_ptr(), nh=len(t),
                     d_field=o.data_ptr()) for f, t, d, o in zip(spec, tabs, d_tabs, outs)]
+    tuned = None
+    if not args.no_autotune:
+        tuned = sb.tc_batch_autotune(entries, stream.cuda_stream)
+        sb.set_tc_variant(tuned["variant"])
+        for e in entries:
+            e["tile_j"] = tuned["tile_j"]
     batch = sb.TcBatch(entries, lambda nb: torch.empty(nb, dtype=torch.uint8, device="cuda"))
     batch.launch(stream.cuda_stream)
     batch.wait(stream.cuda_stream)
@@ -289,7 +295,10 @@ def run_batched(args, nfields=256):
     torch.cuda.synchronize()
     t_e2e = time.perf_counter() - t0
     del graph
+    sb.set_tc_variant(sb.TC_SINGLE)
     return {"fields": nfields, "work_pt_harm": work, "value": work / t_step, "unit": UNIT,
+            "plan": None if tuned is None else {"variant": ["pair", "single", "single_tmem_a"][tuned["variant"]],
+                                                "tile_j": tuned["tile_j"], "autotuned": True},
             "ms_per_step": t_step * 1e3, "graph_replayed": True, "sampling_s_device_assisted": t_sample,
             "rel_rms_vs_fp64_sampled_fields": errs,
             "e2e": {"value": work / t_e2e, "unit": UNIT, "s_per_step": t_e2e,
@@ -343,6 +352,17 @@ def run_b200(args, w):
 
     d_tab = torch.from_numpy(tab.reshape(-1).copy()).cuda()
     field = torch.empty(npts, dtype=torch.float32, device="cuda")
+    # Plans of this grid picked by the autotuner (before any timed region):
+    # the device-field plan of the timed step and the fixed-column plan that
+    # scarf_execute uses in the end-to-end leg.
+    tuned = None
+    if not args.no_autotune:
+        st0 = torch.cuda.current_stream().cuda_stream
+        tuned = {"device_field": sb.tc_autotune(s, fs, n, ds, d_tab.data_ptr(), nh, stream_handle=st0),
+                 "execute": sb.tc_autotune(s, fs, n, ds, d_tab.data_ptr(), nh, fixed_columns=True,
+                                           stream_handle=st0)}
+        sb.set_tc_autotune(1)
+    plan = sb.tc_plan_info(3, n, nh)
     wbytes = sb.tc_workspace_bytes(3, n, nh)
     work = torch.empty(wbytes, dtype=torch.uint8, device="cuda")
     stream = torch.cuda.current_stream()
@@ -452,6 +472,11 @@ def run_b200(args, w):
             "config": {"workload": workload_name(w), "grid_per_gpu": n, "global_grid": [nx, ny, nz * world],
                        "nharm": w["nharm"], "harmonics_kept": nh, "form": "tcgen05 FP16 hi/lo 3-product",
                        "l2": "inputs and output larger than L2 (tables 246 MB, field 537 MB per GPU)",
+                       "plan": {"variant": ["pair", "single", "single_tmem_a"][plan["variant"]],
+                                "tile": [128 // plan["tile_j"], plan["tile_j"]],
+                                "longest_axis_as_columns": bool(plan["permute"]),
+                                "autotuned": tuned is not None,
+                                "tuned": tuned},
                        "parallelism": f"z-slabs x{world}"},
             "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                          "frac": achieved / peak, "traffic": traffic,
@@ -482,6 +507,7 @@ def main():
     ap.add_argument("--grid", type=int, nargs=3, default=None, help="override the grid (profiling of small cases)")
     ap.add_argument("--nharm", type=int, default=None)
     ap.add_argument("--no-batched", action="store_true", help="skip the 256-field batched measurement")
+    ap.add_argument("--no-autotune", action="store_true", help="default plans instead of autotuned ones")
     args = ap.parse_args()
     w = dict(WORKLOAD)
     if args.grid:

@@ -110,6 +110,40 @@ int scarf_set_output_overlap(int items_per_slab);
 #define SCARF_TC_SINGLE_TMEM_A 2
 int scarf_set_tc_variant(int variant);
 
+/* Autotuning of the tensor-core form. No counterpart in the reference (its
+ * SRM has one CPU code path). A tuning times every candidate plan -- kernel
+ * form (SCARF_TC_*), row tile (128 / tile_j) x tile_j with tile_j in
+ * {2, 4, 8, 16}, and for device fields whether the longest axis is the
+ * column axis -- on the caller's grid and harmonic table (at most 2 048
+ * harmonics of it; table builds and kernel), on the current GPU, and records
+ * the fastest for the grid's shape bucket (extents rounded up to a multiple
+ * of 16, per GPU name and driver); the default plan is kept unless a
+ * candidate beats it by 3 %. With scarf_set_tc_autotune(1), plans made afterwards
+ * (scarf_srm_tc_workspace_bytes / scarf_srm_tc_structured, and
+ * scarf_execute for fixed_columns = 1 tunings) follow the recorded choice
+ * of their bucket; other buckets keep the default plans. Tuned plans compute
+ * the same sum; a different column axis changes how the per-axis factors
+ * combine, so results may differ at the rounding level (within the
+ * tensor-core tolerance). The tuning allocates its own device scratch. */
+typedef struct scarf_tc_tuning {
+  int variant; /* SCARF_TC_*                                     */
+  int tile_j;  /* row tile (128 / tile_j) x tile_j                */
+  int permute; /* 1: longest axis as column axis (device fields)  */
+  float ms;    /* kernel time of the chosen plan on the probe      */
+} scarf_tc_tuning;
+/* 0 = default plans (the initial state), 1 = follow recorded tunings. */
+int scarf_set_tc_autotune(int mode);
+/* Tunings are also appended to this text file and read from it now (NULL:
+ * memory only). */
+int scarf_set_tc_tune_cache(const char *path);
+/* The plan scarf_srm_tc_structured would use for this grid now (ms = 0;
+ * permute = 1 when the column axis is not z, or y in 2D). */
+int scarf_srm_tc_plan_info(int ndim, const int n[3], int nh, scarf_tc_tuning *out);
+/* Tune one structured grid (device table, nh rows); fixed_columns = 1 keeps
+ * z as the column axis (the layout scarf_execute uses). */
+int scarf_srm_tc_autotune(const scarf_srm_setup *s, const int fs[3], const int n[3], float ds, const float *d_table,
+                          int nh, int fixed_columns, void *stream, scarf_tc_tuning *out);
+
 /* Status-returning scarf_execute (c_binding.c:138-143); stats[8] as the
  * reference fills it (stats[4] host seconds, stats[5] device seconds). */
 int scarf_execute_ex(int seed, float *field, float stats[8], int flags);
@@ -192,6 +226,14 @@ int scarf_srm_tc_batch_launch(const scarf_tc_batch *batch, void *stream);
 /* Synchronises `stream` and reports a kernel-side pipeline failure. */
 int scarf_srm_tc_batch_wait(const scarf_tc_batch *batch, void *stream);
 void scarf_srm_tc_batch_destroy(scarf_tc_batch *batch);
+/* Times the batch's candidate plans (kernel form SCARF_TC_SINGLE or
+ * SCARF_TC_PAIR, tile_j in {2, 4, 8, 16} for every field) on the fields'
+ * own tables, overwriting their outputs, and returns the fastest (the
+ * default, one-CTA form with tile_j 8, unless beaten by 3 %): create the
+ * batch with each field's tile_j set to out->tile_j after
+ * scarf_set_tc_variant(out->variant). Synchronises `stream`; allocates its
+ * own device scratch. */
+int scarf_srm_tc_batch_autotune(const scarf_tc_field *fields, int nfields, void *stream, scarf_tc_tuning *out);
 
 /* Same tensor-core sum as scarf_srm_tc_structured, for callers that cannot
  * allocate device memory (their memory belongs to another allocator, or a

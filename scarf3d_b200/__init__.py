@@ -44,6 +44,8 @@ EXPORTED_SYMBOLS = (
     "scarf_srm_tc_noalloc_capacity_bytes", "scarf_srm_tc_structured_noalloc",
     "scarf_srm_tc_batch_workspace_bytes", "scarf_srm_tc_batch_create", "scarf_srm_tc_batch_launch",
     "scarf_srm_tc_batch_wait", "scarf_srm_tc_batch_destroy",
+    "scarf_set_tc_autotune", "scarf_set_tc_tune_cache", "scarf_srm_tc_autotune", "scarf_srm_tc_batch_autotune",
+    "scarf_srm_tc_plan_info",
     "scarf_field_stats_workspace_bytes", "scarf_field_stats",
 )
 
@@ -86,6 +88,12 @@ class TcField(ctypes.Structure):
     _fields_ = [("setup", ctypes.POINTER(SrmSetup)), ("fs", ctypes.c_int * 3), ("n", ctypes.c_int * 3),
                 ("ds", ctypes.c_float), ("d_table", ctypes.c_void_p), ("nh", ctypes.c_int),
                 ("d_field", ctypes.c_void_p), ("tile_j", ctypes.c_int)]
+
+
+class TcTuning(ctypes.Structure):
+    """scarf_tc_tuning: a tuned plan choice of the tensor-core form."""
+    _fields_ = [("variant", ctypes.c_int), ("tile_j", ctypes.c_int), ("permute", ctypes.c_int),
+                ("ms", ctypes.c_float)]
 
 
 def _load() -> ctypes.CDLL:
@@ -144,6 +152,13 @@ def _load() -> ctypes.CDLL:
         "scarf_srm_tc_noalloc_capacity_bytes": (c_size_t, []),
         "scarf_srm_tc_structured_noalloc": (c_int, [ctypes.POINTER(SrmSetup), ip, ip, c_float, c_void_p, c_int,
                                                     c_void_p, c_void_p]),
+        "scarf_set_tc_autotune": (c_int, [c_int]),
+        "scarf_srm_tc_plan_info": (c_int, [c_int, ip, c_int, ctypes.POINTER(TcTuning)]),
+        "scarf_set_tc_tune_cache": (c_int, [ctypes.c_char_p]),
+        "scarf_srm_tc_autotune": (c_int, [ctypes.POINTER(SrmSetup), ip, ip, c_float, c_void_p, c_int, c_int,
+                                          c_void_p, ctypes.POINTER(TcTuning)]),
+        "scarf_srm_tc_batch_autotune": (c_int, [ctypes.POINTER(TcField), c_int, c_void_p,
+                                                ctypes.POINTER(TcTuning)]),
         "scarf_field_stats_workspace_bytes": (c_size_t, [c_ll]),
         "scarf_field_stats": (c_int, [c_void_p, c_ll, c_void_p, c_size_t, fp, fp, c_void_p]),
     }
@@ -375,6 +390,34 @@ def set_tc_variant(variant: int):
     check(lib.scarf_set_tc_variant(int(variant)))
 
 
+def set_tc_autotune(mode: int):
+    """0: default plans; 1: plans follow recorded tunings of their shape bucket."""
+    check(lib.scarf_set_tc_autotune(int(mode)))
+
+
+def set_tc_tune_cache(path):
+    """Append tunings to (and read them from) this text file; None: memory only."""
+    check(lib.scarf_set_tc_tune_cache(None if path is None else str(path).encode()))
+
+
+def tc_autotune(s: "SrmSetup", fs, n, ds: float, d_table: int, nh: int, fixed_columns: bool = False,
+                stream_handle: int | None = None) -> dict:
+    """Time the candidate plans of one grid on the device table `d_table`
+    (device pointer, nh rows) and record the fastest for its shape bucket."""
+    t = TcTuning()
+    check(lib.scarf_srm_tc_autotune(ctypes.byref(s), _iptr(fs), _iptr(n), float(ds), ctypes.c_void_p(int(d_table)),
+                                    int(nh), int(bool(fixed_columns)), ctypes.c_void_p(stream_handle or 0),
+                                    ctypes.byref(t)))
+    return {"variant": t.variant, "tile_j": t.tile_j, "permute": t.permute, "ms": t.ms}
+
+
+def tc_plan_info(ndim: int, n, nh: int) -> dict:
+    """The plan the device-field tensor-core entry points would use now."""
+    t = TcTuning()
+    check(lib.scarf_srm_tc_plan_info(int(ndim), _iptr(n), int(nh), ctypes.byref(t)))
+    return {"variant": t.variant, "tile_j": t.tile_j, "permute": t.permute}
+
+
 def set_output_overlap(items_per_slab: int = 1):
     """scarf_execute: copy finished field slabs (about items_per_slab work
     items each; 1 = default size) to the host while the kernel runs, or the
@@ -394,6 +437,32 @@ def tc_workspace_bytes(ndim: int, n, nh: int) -> int:
     return int(lib.scarf_srm_tc_workspace_bytes(int(ndim), _iptr(n), int(nh)))
 
 
+def _tc_field_array(entries, setups):
+    arr = (TcField * len(entries))()
+    for k, e in enumerate(entries):
+        f = arr[k]
+        f.setup = ctypes.pointer(setups[k])
+        for c in range(3):
+            f.fs[c] = int(e["fs"][c])
+            f.n[c] = int(e["n"][c])
+        f.ds = float(e["ds"])
+        f.d_table = ctypes.c_void_p(int(e["d_table"]))
+        f.nh = int(e["nh"])
+        f.d_field = ctypes.c_void_p(int(e["d_field"]))
+        f.tile_j = int(e.get("tile_j", 0))
+    return arr
+
+
+def tc_batch_autotune(entries, stream_handle: int | None = None) -> dict:
+    """Time the candidate plans of a batch (the TcBatch entries; outputs are
+    overwritten) and return the fastest {variant, tile_j, ms}."""
+    setups = [e["setup"] for e in entries]
+    arr = _tc_field_array(entries, setups)
+    t = TcTuning()
+    check(lib.scarf_srm_tc_batch_autotune(arr, len(entries), ctypes.c_void_p(stream_handle or 0), ctypes.byref(t)))
+    return {"variant": t.variant, "tile_j": t.tile_j, "ms": t.ms}
+
+
 class TcBatch:
     """Batched tensor-core launch over many structured fields.
 
@@ -405,18 +474,7 @@ class TcBatch:
 
     def __init__(self, entries, alloc):
         self._setups = [e["setup"] for e in entries]
-        arr = (TcField * len(entries))()
-        for k, e in enumerate(entries):
-            f = arr[k]
-            f.setup = ctypes.pointer(self._setups[k])
-            for c in range(3):
-                f.fs[c] = int(e["fs"][c])
-                f.n[c] = int(e["n"][c])
-            f.ds = float(e["ds"])
-            f.d_table = ctypes.c_void_p(int(e["d_table"]))
-            f.nh = int(e["nh"])
-            f.d_field = ctypes.c_void_p(int(e["d_field"]))
-            f.tile_j = int(e.get("tile_j", 0))
+        arr = _tc_field_array(entries, self._setups)
         self._arr = arr
         self.bytes = int(lib.scarf_srm_tc_batch_workspace_bytes(arr, len(entries)))
         if self.bytes == 0:

@@ -11,7 +11,10 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <fstream>
+#include <map>
 #include <mutex>
+#include <sstream>
 #include <new>
 #include <string>
 #include <thread>
@@ -335,7 +338,11 @@ int execute_impl(int seed, float* field, float stats[8], int flags) {
   if (g_obj.structured) {
     const bool use_tc = (g_cfg.form != SCARF_FORM_DIRECT);
     TcPlan plan{};
-    if (use_tc && nh > 0 && tc_make_plan(s.ndim, n, nh, &plan)) {
+    TcChoice tuned{};
+    const bool have_tuned = use_tc && nh > 0 && tc_tuned_choice(s.ndim, n, true, &tuned);
+    const bool planned = have_tuned ? tc_make_plan(s.ndim, n, nh, &plan, tuned.tile_j, false, tuned.variant)
+                                    : tc_make_plan(s.ndim, n, nh, &plan);
+    if (use_tc && nh > 0 && planned) {
       SCARF_CUDA(g_res.work.ensure(plan.bytes));
       // Without rescale or taper the field is final when the kernel stores
       // it: copy it out slab by slab while the kernel still runs.
@@ -817,18 +824,39 @@ int scarf_srm_direct_points(const scarf_srm_setup* s, const float* d_x, const fl
 }
 
 // Device-field entry points let the longest axis be the column axis
-// (wider column tiles); the same rule sizes their workspace.
+// (wider column tiles), or follow a tuned choice for the grid's bucket when
+// tuned plans are enabled; the same rule sizes their workspace.
+}  // extern "C"
+namespace {
+bool device_field_plan(int ndim, const int n[3], int nh, TcPlan* p) {
+  TcChoice c{};
+  if (n[0] > 0 && n[1] > 0 && n[2] > 0 && tc_tuned_choice(ndim, n, false, &c))
+    return tc_make_plan(ndim, n, nh, p, c.tile_j, c.permute != 0, c.variant);
+  return tc_make_plan(ndim, n, nh, p, 0, true);
+}
+}  // namespace
+extern "C" {
 size_t scarf_srm_tc_workspace_bytes(int ndim, const int n[3], int nh) {
   TcPlan p{};
-  if (!n || !tc_make_plan(ndim, n, nh, &p, 0, true)) return 0;
+  if (!n || !device_field_plan(ndim, n, nh, &p)) return 0;
   return p.bytes;
+}
+
+int scarf_srm_tc_plan_info(int ndim, const int n[3], int nh, scarf_tc_tuning* out) {
+  TcPlan p{};
+  if (!n || !out || !device_field_plan(ndim, n, nh, &p)) return fail(SCARF_ERR_ARG, "invalid grid for the tensor-core form");
+  out->variant = p.pair ? SCARF_TC_PAIR : (p.tmem_a ? SCARF_TC_SINGLE_TMEM_A : SCARF_TC_SINGLE);
+  out->tile_j = p.tj;
+  out->permute = p.ax_c != (ndim == 3 ? 2 : 1) ? 1 : 0;
+  out->ms = 0.0f;
+  return SCARF_OK;
 }
 
 int scarf_srm_tc_structured(const scarf_srm_setup* s, const int fs[3], const int n[3], float ds, const float* d_table,
                             int nh, float* d_field, void* d_work, size_t work_bytes, void* stream) {
   if (!s || !fs || !n || !d_field || !d_table || nh <= 0 || !d_work) return fail(SCARF_ERR_ARG, "invalid argument");
   TcPlan p{};
-  if (!tc_make_plan(s->ndim, n, nh, &p, 0, true)) return fail(SCARF_ERR_ARG, "invalid grid for the tensor-core form");
+  if (!device_field_plan(s->ndim, n, nh, &p)) return fail(SCARF_ERR_ARG, "invalid grid for the tensor-core form");
   if (work_bytes < p.bytes) return fail(SCARF_ERR_ARG, "workspace too small: %zu < %zu", work_bytes, p.bytes);
   if (reinterpret_cast<uintptr_t>(d_work) & 255u) return fail(SCARF_ERR_ARG, "workspace must be 256-byte aligned");
   std::lock_guard<std::mutex> lk(g_mu);
@@ -979,6 +1007,263 @@ int scarf_field_stats(const float* d_field, long long n, void* d_work, size_t wo
   SCARF_CUDA(cudaStreamSynchronize(st));
   *mean = mv[0];
   *var = mv[1];
+  return SCARF_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------- autotune --
+// Plan choices of the tensor-core form measured on this GPU: kernel form,
+// row tile (128 / tile_j) x tile_j and column axis, per shape bucket (grid
+// extents rounded up to a multiple of 16; the key also names the GPU and the
+// driver). Entries live in memory and, when a cache file is set, one line
+// each in that file ("key variant tile_j permute ms").
+namespace {
+struct TuneState {
+  std::mutex mu;
+  int mode = 0;  // 0: the default plans; 1: tuned choices where a bucket has one
+  std::string path;
+  std::map<std::string, scarf::TcChoice> entries;
+};
+TuneState g_tune;
+
+// GPU name and driver version of the current device, looked up once per
+// device (a properties query costs milliseconds; plans are made per call).
+std::string device_tag() {
+  static std::mutex mu;
+  static std::map<int, std::string> tags;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) {
+    cudaGetLastError();
+    return "unknown";
+  }
+  std::lock_guard<std::mutex> lk(mu);
+  const auto it = tags.find(dev);
+  if (it != tags.end()) return it->second;
+  int drv = 0;
+  cudaDeviceProp prop{};
+  if (cudaGetDeviceProperties(&prop, dev) != cudaSuccess) {
+    cudaGetLastError();
+    return "unknown";
+  }
+  cudaDriverGetVersion(&drv);
+  std::string name = prop.name;
+  for (char& c : name)
+    if (c == ' ' || c == ':') c = '_';
+  return tags[dev] = name + "_drv" + std::to_string(drv);
+}
+
+std::string bucket_key(int ndim, const int n[3], bool fixed_columns) {
+  std::ostringstream k;
+  k << device_tag() << ':' << ndim << ':';
+  for (int a = 0; a < 3; ++a) k << (a ? "x" : "") << (n[a] + 15) / 16 * 16;
+  k << (fixed_columns ? ":z" : ":p");
+  return k.str();
+}
+
+void load_cache_locked(const std::string& path) {
+  std::ifstream f(path);
+  std::string line;
+  while (std::getline(f, line)) {
+    std::istringstream is(line);
+    std::string key;
+    scarf::TcChoice c{};
+    if (is >> key >> c.variant >> c.tile_j >> c.permute >> c.ms) g_tune.entries[key] = c;
+  }
+}
+
+void store_locked(const std::string& key, const scarf::TcChoice& c) {
+  g_tune.entries[key] = c;
+  if (g_tune.path.empty()) return;
+  std::ofstream f(g_tune.path, std::ios::app);
+  f << key << ' ' << c.variant << ' ' << c.tile_j << ' ' << c.permute << ' ' << c.ms << '\n';
+}
+
+// Time of one plan on the caller's data, table builds and kernel (the
+// fastest of three runs after a warm-up run), or a negative value when the
+// plan cannot run.
+float time_plan(const scarf_srm_setup& s, const int fs[3], const int n[3], float ds, const float* d_table, int nh,
+                float* d_field, void* d_work, const TcPlan& p, cudaStream_t st, cudaEvent_t e0, cudaEvent_t e1) {
+  int* d_status = reinterpret_cast<int*>(static_cast<char*>(d_work) + p.off_status);
+  float best = -1.0f;
+  for (int rep = 0; rep < 4; ++rep) {
+    float ms = -1.0f;
+    if (cudaMemsetAsync(d_status, 0, sizeof(int), st) != cudaSuccess || cudaEventRecord(e0, st) != cudaSuccess ||
+        launch_tc_structured(s, fs, n, ds, d_table, nh, d_field, d_work, p, d_status, st) != cudaSuccess ||
+        cudaEventRecord(e1, st) != cudaSuccess) {
+      cudaGetLastError();
+      return -1.0f;
+    }
+    int h = 1;
+    if (cudaMemcpyAsync(&h, d_status, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess || h != 0 || cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) {
+      cudaGetLastError();
+      return -1.0f;
+    }
+    if (rep > 0 && (best < 0.0f || ms < best)) best = ms;
+  }
+  return best;
+}
+}  // namespace
+
+namespace scarf {
+bool tc_tuned_choice(int ndim, const int n[3], bool fixed_columns, TcChoice* c) {
+  std::lock_guard<std::mutex> lk(g_tune.mu);
+  if (g_tune.mode == 0 || g_tune.entries.empty()) return false;
+  const auto it = g_tune.entries.find(bucket_key(ndim, n, fixed_columns));
+  if (it == g_tune.entries.end()) return false;
+  *c = it->second;
+  return true;
+}
+}  // namespace scarf
+
+extern "C" {
+
+int scarf_set_tc_autotune(int mode) {
+  if (mode != 0 && mode != 1) return fail(SCARF_ERR_ARG, "autotune mode must be 0 or 1");
+  std::lock_guard<std::mutex> lk(g_tune.mu);
+  g_tune.mode = mode;
+  return SCARF_OK;
+}
+
+int scarf_set_tc_tune_cache(const char* path) {
+  std::lock_guard<std::mutex> lk(g_tune.mu);
+  g_tune.path = path ? path : "";
+  if (!g_tune.path.empty()) load_cache_locked(g_tune.path);
+  return SCARF_OK;
+}
+
+int scarf_srm_tc_autotune(const scarf_srm_setup* s, const int fs[3], const int n[3], float ds, const float* d_table,
+                          int nh, int fixed_columns, void* stream, scarf_tc_tuning* out) {
+  if (!s || !fs || !n || !d_table || nh <= 0 || !out) return fail(SCARF_ERR_ARG, "invalid argument");
+  if (n[0] <= 0 || n[1] <= 0 || n[2] <= 0) return fail(SCARF_ERR_ARG, "empty grid");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  // Whole stages of at most 2 048 harmonics: enough for the pipeline to
+  // reach its steady state, short enough to try every candidate.
+  const int nh_probe = std::min(nh, 2048);
+  const int forms[3] = {SCARF_TC_SINGLE, SCARF_TC_PAIR, SCARF_TC_SINGLE_TMEM_A};
+  const int tiles[4] = {2, 4, 8, 16};
+  std::vector<TcPlan> plans;
+  std::vector<scarf::TcChoice> choices;
+  for (int v : forms)
+    for (int tj : tiles)
+      for (int perm = 0; perm < (fixed_columns ? 1 : 2); ++perm) {
+        TcPlan p{};
+        if (!tc_make_plan(s->ndim, n, nh_probe, &p, tj, perm != 0, v)) continue;
+        if (perm == 1 && !plans.empty()) {  // the longest axis may already be z: same plan
+          const TcPlan& q = plans.back();
+          if (q.ax_c == p.ax_c && q.tj == p.tj && q.pair == p.pair && q.tmem_a == p.tmem_a) continue;
+        }
+        plans.push_back(p);
+        choices.push_back(scarf::TcChoice{v, tj, perm, 0.0f});
+      }
+  size_t work = 0;
+  for (const TcPlan& p : plans) work = std::max(work, p.bytes);
+  const size_t npts = static_cast<size_t>(n[0]) * n[1] * n[2];
+  void* d_work = nullptr;
+  float* d_field = nullptr;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  auto release = [&]() {
+    if (d_work) cudaFree(d_work);
+    if (d_field) cudaFree(d_field);
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+  };
+  if (cudaMalloc(&d_work, work) != cudaSuccess || cudaMalloc(&d_field, sizeof(float) * npts) != cudaSuccess ||
+      cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
+    cudaGetLastError();
+    release();
+    return fail(SCARF_ERR_NOMEM, "autotune: device allocation failed");
+  }
+  int best = -1;
+  for (size_t c = 0; c < plans.size(); ++c) {
+    choices[c].ms = time_plan(*s, fs, n, ds, d_table, nh_probe, d_field, d_work, plans[c], st, e0, e1);
+    if (choices[c].ms > 0.0f && (best < 0 || choices[c].ms < choices[best].ms)) best = static_cast<int>(c);
+  }
+  release();
+  if (best < 0) return fail(SCARF_ERR_CUDA, "autotune: no candidate plan ran");
+  // The default plan stays unless a candidate beats it by 3 %: probe timings
+  // of a few milliseconds carry about that much noise.
+  TcPlan dp{};
+  if (tc_make_plan(s->ndim, n, nh_probe, &dp, 0, fixed_columns == 0, SCARF_TC_SINGLE)) {
+    for (size_t c = 0; c < plans.size(); ++c) {
+      const TcPlan& q = plans[c];
+      if (q.ax_c == dp.ax_c && q.tj == dp.tj && q.pair == dp.pair && q.tmem_a == dp.tmem_a && choices[c].ms > 0.0f &&
+          choices[best].ms > 0.97f * choices[c].ms)
+        best = static_cast<int>(c);
+    }
+  }
+  const scarf::TcChoice& b = choices[best];
+  {
+    std::lock_guard<std::mutex> lk(g_tune.mu);
+    store_locked(bucket_key(s->ndim, n, fixed_columns != 0), b);
+  }
+  out->variant = b.variant;
+  out->tile_j = b.tile_j;
+  out->permute = b.permute;
+  out->ms = b.ms;
+  return SCARF_OK;
+}
+
+int scarf_srm_tc_batch_autotune(const scarf_tc_field* fields, int nfields, void* stream, scarf_tc_tuning* out) {
+  if (!out || !batch_fields_valid(fields, nfields)) return fail(SCARF_ERR_ARG, "invalid argument");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const int forms[2] = {SCARF_TC_SINGLE, SCARF_TC_PAIR};
+  const int tiles[4] = {2, 4, 8, 16};
+  std::lock_guard<std::mutex> lk(g_mu);  // the kernel form is global while a batch is planned
+  const int saved = tc_get_variant();
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
+    cudaGetLastError();
+    if (e0) cudaEventDestroy(e0);
+    return fail(SCARF_ERR_CUDA, "autotune: event creation failed");
+  }
+  scarf::TcChoice best{-1, 0, 1, 0.0f}, deflt{-1, 0, 1, 0.0f};
+  for (int v : forms) {
+    tc_set_variant(v);
+    for (int tj : tiles) {
+      auto in = batch_inputs(fields, nfields);
+      for (auto& e : in) e.tj = tj;
+      TcBatchPlan bp;
+      if (!tc_batch_plan(in.data(), nfields, &bp)) continue;
+      void* d_work = nullptr;
+      if (cudaMalloc(&d_work, bp.bytes) != cudaSuccess) {
+        cudaGetLastError();
+        continue;
+      }
+      float ms = -1.0f;
+      if (tc_batch_upload(in.data(), bp, d_work) == cudaSuccess) {
+        const int* d_status = reinterpret_cast<const int*>(static_cast<const char*>(d_work) + bp.off_status);
+        for (int rep = 0; rep < 4; ++rep) {  // a warm-up run, then the fastest of three
+          int h = 1;
+          float t = -1.0f;
+          if (cudaEventRecord(e0, st) != cudaSuccess || tc_batch_launch(bp, d_work, st) != cudaSuccess ||
+              cudaEventRecord(e1, st) != cudaSuccess ||
+              cudaMemcpyAsync(&h, d_status, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+              cudaStreamSynchronize(st) != cudaSuccess || h != 0 || cudaEventElapsedTime(&t, e0, e1) != cudaSuccess) {
+            ms = -1.0f;
+            break;
+          }
+          if (rep > 0 && (ms < 0.0f || t < ms)) ms = t;
+        }
+      }
+      cudaGetLastError();
+      cudaFree(d_work);
+      if (ms > 0.0f && (best.variant < 0 || ms < best.ms)) best = scarf::TcChoice{v, tj, 1, ms};
+      if (ms > 0.0f && v == SCARF_TC_SINGLE && tj == 8) deflt = scarf::TcChoice{v, tj, 1, ms};
+    }
+  }
+  // As for single grids: the default (one-CTA form, 16 x 8 row tiles) stays
+  // unless a candidate beats it by 3 %.
+  if (deflt.variant >= 0 && best.ms > 0.97f * deflt.ms) best = deflt;
+  tc_set_variant(saved);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (best.variant < 0) return fail(SCARF_ERR_CUDA, "autotune: no candidate batch plan ran");
+  out->variant = best.variant;
+  out->tile_j = best.tile_j;
+  out->permute = 1;
+  out->ms = best.ms;
   return SCARF_OK;
 }
 

@@ -48,11 +48,26 @@ constexpr int kTcVariantPair = 0;         // cta_group::2 pairs, A in shared mem
 constexpr int kTcVariantSingle = 1;       // one CTA per tile, A in shared memory (default)
 constexpr int kTcVariantSingleTmemA = 2;  // one CTA per tile, A in tensor memory
 void tc_set_variant(int v);
+int tc_get_variant();
 
 // tj_force > 0 fixes the row tile to (128 / tj_force) x tj_force.
 // permute: let the longest axis be the column axis (device-field entry
 // points; the default layout keeps k = z, which the slab copy-out relies on).
-bool tc_make_plan(int ndim, const int n[3], int nh, TcPlan* plan, int tj_force = 0, bool permute = false);
+// variant >= 0 selects the kernel form (kTcVariant*) instead of the global one.
+bool tc_make_plan(int ndim, const int n[3], int nh, TcPlan* plan, int tj_force = 0, bool permute = false,
+                  int variant = -1);
+
+// ---- autotuning (tc_tune.cpp) ----
+// A tuned plan choice for one shape bucket (grid extents rounded up to a
+// multiple of 16): kernel form, row tile (128 / tile_j) x tile_j, and whether
+// the longest axis is the column axis.
+struct TcChoice {
+  int variant, tile_j, permute;
+  float ms;
+};
+// The tuned choice for a grid when tuned plans are enabled and its bucket has
+// an entry (fixed_columns: the caller keeps k = z, as scarf_execute does).
+bool tc_tuned_choice(int ndim, const int n[3], bool fixed_columns, TcChoice* c);
 // Harmonics accumulated in tensor memory before each FP32 drain (rounded up
 // to whole pipeline stages); 0 restores the default.
 void tc_set_chunk_harmonics(int harmonics);

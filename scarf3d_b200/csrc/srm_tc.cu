@@ -1364,13 +1364,15 @@ void launch_tc_kernel(const TcKernelArgs& A, bool tmem_a, bool pair, int nsm, si
 
 }  // namespace
 
+int tc_get_variant() { return g_variant; }
+
 void tc_set_variant(int v) { g_variant = v; }
 
 void tc_set_chunk_harmonics(int harmonics) {
   g_chunk_stages = harmonics > 0 ? (harmonics + kStageHarm - 1) / kStageHarm : kDefaultChunkStages;
 }
 
-bool tc_make_plan(int ndim, const int n[3], int nh, TcPlan* P, int tj_force, bool permute) {
+bool tc_make_plan(int ndim, const int n[3], int nh, TcPlan* P, int tj_force, bool permute, int variant) {
   if (nh <= 0 || n[0] <= 0 || n[1] <= 0 || n[2] <= 0) return false;
   TcPlan p{};
   // Rows (i, j) over two axes, columns k over the third. By default k = z
@@ -1406,8 +1408,9 @@ bool tc_make_plan(int ndim, const int n[3], int nh, TcPlan* P, int tj_force, boo
   p.ti = kRows / p.tj;
   p.bi = (p.n1 + p.ti - 1) / p.ti;
   p.bj = (p.n2 + p.tj - 1) / p.tj;
-  p.pair = g_variant == kTcVariantPair ? 1 : 0;
-  p.tmem_a = g_variant == kTcVariantSingleTmemA ? 1 : 0;
+  const int form = (variant >= 0) ? variant : g_variant;
+  p.pair = form == kTcVariantPair ? 1 : 0;
+  p.tmem_a = form == kTcVariantSingleTmemA ? 1 : 0;
   p.pair_i = (p.pair && p.bj == 1) ? 1 : 0;  // one row block along j (2D): pair along i
   p.bix = (p.pair && p.pair_i) ? (p.bi + 1) / 2 : p.bi;
   p.bjx = (p.pair && !p.pair_i) ? (p.bj + 1) / 2 : p.bj;

@@ -58,6 +58,8 @@ int main(void) {
   printf("scarf_srm_params.size %zu\n", sizeof(scarf_srm_params));
   printf("scarf_srm_setup.size %zu\n", sizeof(scarf_srm_setup));
   P(scarf_srm_setup, m); P(scarf_srm_setup, ier_full);
+  P(scarf_tc_tuning, variant); P(scarf_tc_tuning, tile_j); P(scarf_tc_tuning, permute); P(scarf_tc_tuning, ms);
+  printf("scarf_tc_tuning.size %zu\n", sizeof(scarf_tc_tuning));
   return 0;
 }
 """)
@@ -72,6 +74,9 @@ int main(void) {
     assert int(got["scarf_srm_setup.size"]) == ctypes.sizeof(sb.SrmSetup)
     assert int(got["scarf_srm_setup.m"]) == sb.SrmSetup.m.offset
     assert int(got["scarf_srm_setup.ier_full"]) == sb.SrmSetup.ier_full.offset
+    for fname, _ in sb.TcTuning._fields_:
+        assert int(got[f"scarf_tc_tuning.{fname}"]) == getattr(sb.TcTuning, fname).offset, fname
+    assert int(got["scarf_tc_tuning.size"]) == ctypes.sizeof(sb.TcTuning)
 
 
 def test_cpp_wrapper_compiles(tmp_path):
