@@ -62,7 +62,21 @@ def build(verbose_ptxas: bool = False) -> Path:
         _run([NVCC] + ARCH + ["-shared", "-cudart", "static", "-o", str(LIB)] + [str(o) for o in objs]
              + ["-lpthread"])
     build_standalone()
+    build_fbind()
     return LIB
+
+
+FBIND_SRC = PKG / "fbind" / "scarf3d_fbind.cpp"
+FBIND = PKG / "libscarf3d_b200_fbind.so"
+
+
+def build_fbind() -> Path:
+    """The reference's Fortran BIND(C) routine names (struct_initialize,
+    execute, ...) as a separate shim over the library."""
+    if _needs(FBIND, [FBIND_SRC, LIB] + sorted((ROOT / "include").glob("*.h"))):
+        _run([CXX, "-O2", "-std=c++17", "-Wall", "-shared", "-fPIC"] + INCLUDES + [str(FBIND_SRC), f"-L{PKG}",
+              "-lscarf3d_b200", "-Wl,-rpath,$ORIGIN", "-o", str(FBIND)])
+    return FBIND
 
 
 STANDALONE_SRC = PKG / "standalone" / "scarf3d_standalone.cpp"
