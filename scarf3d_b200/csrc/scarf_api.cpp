@@ -391,18 +391,21 @@ int execute_impl(int seed, float* field, float stats[8], int flags) {
       SCARF_CUDA(cudaMemsetAsync(d_field, 0, sizeof(float) * npts, st));
     }
   }
-  rc = check_device_status(d_status, st);
-  if (rc) return rc;
-  if (nh > 0) collect_kernel_time();
-
   // Statistics (scarflib_srm.f90:877-895): single set, so the Chan merge
-  // returns (var, mean) unchanged; std = sqrt(var) in FP32.
+  // returns (var, mean) unchanged; std = sqrt(var) in FP32. They are
+  // enqueued behind the sum, and the sum's status word comes back with them
+  // in one synchronisation (after a failed sum the statistics are dropped).
   double* d_part = static_cast<double*>(g_res.stats.p);
   float* d_out = reinterpret_cast<float*>(static_cast<char*>(g_res.stats.p) + stats_partials_bytes(0));
   SCARF_CUDA(launch_field_stats(d_field, npts, d_part, d_out, st));
   float mv[2];
+  int dev_status = 0;
+  SCARF_CUDA(cudaMemcpyAsync(&dev_status, d_status, sizeof(int), cudaMemcpyDeviceToHost, st));
   SCARF_CUDA(cudaMemcpyAsync(mv, d_out, sizeof(mv), cudaMemcpyDeviceToHost, st));
   SCARF_CUDA(cudaStreamSynchronize(st));
+  if (dev_status != 0)
+    return fail(SCARF_ERR_DEVICE, "device pipeline reported status %d (bounded wait expired)", dev_status);
+  if (nh > 0) collect_kernel_time();
   stats[0] = s.info0;
   stats[1] = s.info1;
   stats[2] = sqrtf(mv[1]);
