@@ -223,8 +223,17 @@ int scarf_srm_tc_batch_create(const scarf_tc_field *fields, int nfields, void *d
 /* Enqueues the batch on `stream` (table builds + one persistent kernel);
  * makes no synchronising or allocating call. */
 int scarf_srm_tc_batch_launch(const scarf_tc_batch *batch, void *stream);
-/* Synchronises `stream` and reports a kernel-side pipeline failure. */
+/* Synchronises `stream` and reports a kernel-side pipeline failure. With host
+ * outputs set, it first copies each field to its host buffer as soon as
+ * the launch has stored that field, while the launch computes the others. */
 int scarf_srm_tc_batch_wait(const scarf_tc_batch *batch, void *stream);
+/* host_fields[f] (nfields host buffers of n[0]*n[1]*n[2] floats, page-locked
+ * for full copy speed; NULL turns the copy-out off): every
+ * scarf_srm_tc_batch_wait after a launch copies the fields there, field by
+ * field as they complete (the launch raises one host-mapped flag per field).
+ * Re-uploads the descriptors (synchronous; call outside stream capture).
+ * No counterpart in the reference. */
+int scarf_srm_tc_batch_set_host_outputs(scarf_tc_batch *batch, float *const *host_fields);
 void scarf_srm_tc_batch_destroy(scarf_tc_batch *batch);
 /* Times the batch's candidate plans (kernel form SCARF_TC_SINGLE or
  * SCARF_TC_PAIR, tile_j in {2, 4, 8, 16} for every field) on the fields'

@@ -43,7 +43,7 @@ EXPORTED_SYMBOLS = (
     "scarf_srm_direct_points", "scarf_srm_tc_workspace_bytes", "scarf_srm_tc_structured",
     "scarf_srm_tc_noalloc_capacity_bytes", "scarf_srm_tc_structured_noalloc",
     "scarf_srm_tc_batch_workspace_bytes", "scarf_srm_tc_batch_create", "scarf_srm_tc_batch_launch",
-    "scarf_srm_tc_batch_wait", "scarf_srm_tc_batch_destroy",
+    "scarf_srm_tc_batch_wait", "scarf_srm_tc_batch_destroy", "scarf_srm_tc_batch_set_host_outputs",
     "scarf_set_tc_autotune", "scarf_set_tc_tune_cache", "scarf_srm_tc_autotune", "scarf_srm_tc_batch_autotune",
     "scarf_srm_tc_plan_info",
     "scarf_field_stats_workspace_bytes", "scarf_field_stats",
@@ -149,6 +149,7 @@ def _load() -> ctypes.CDLL:
         "scarf_srm_tc_batch_launch": (c_int, [c_void_p, c_void_p]),
         "scarf_srm_tc_batch_wait": (c_int, [c_void_p, c_void_p]),
         "scarf_srm_tc_batch_destroy": (None, [c_void_p]),
+        "scarf_srm_tc_batch_set_host_outputs": (c_int, [c_void_p, c_void_p]),
         "scarf_srm_tc_noalloc_capacity_bytes": (c_size_t, []),
         "scarf_srm_tc_structured_noalloc": (c_int, [ctypes.POINTER(SrmSetup), ip, ip, c_float, c_void_p, c_int,
                                                     c_void_p, c_void_p]),
@@ -486,6 +487,18 @@ class TcBatch:
 
     def launch(self, stream_handle: int | None = None):
         check(lib.scarf_srm_tc_batch_launch(self._h, ctypes.c_void_p(stream_handle or 0)))
+
+    def set_host_outputs(self, host_ptrs):
+        """Host buffers (addresses, one per field, page-locked for full speed)
+        that wait() fills field by field as the launch completes them; None
+        turns the copy-out off."""
+        if host_ptrs is None:
+            check(lib.scarf_srm_tc_batch_set_host_outputs(self._h, None))
+            self._host = None
+            return
+        arr = (ctypes.c_void_p * len(host_ptrs))(*[int(p) for p in host_ptrs])
+        check(lib.scarf_srm_tc_batch_set_host_outputs(self._h, arr))
+        self._host = arr
 
     def wait(self, stream_handle: int | None = None):
         check(lib.scarf_srm_tc_batch_wait(self._h, ctypes.c_void_p(stream_handle or 0)))

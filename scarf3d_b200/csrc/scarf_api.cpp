@@ -882,6 +882,18 @@ int scarf_srm_tc_structured(const scarf_srm_setup* s, const int fs[3], const int
 struct scarf_tc_batch {
   scarf::TcBatchPlan plan;
   void* d_work = nullptr;
+  // Kept for re-uploads of the descriptors (host outputs on or off).
+  std::vector<scarf_srm_setup> setups;
+  std::vector<scarf::TcBatchInput> in;
+  // Overlapped copy-out to host buffers (scarf_srm_tc_batch_set_host_outputs).
+  std::vector<float*> host;
+  int* flags = nullptr;      // host-mapped, one per field
+  int* flags_dev = nullptr;  // their device address
+  cudaStream_t copy_stream = nullptr;
+  ~scarf_tc_batch() {
+    if (flags) cudaFreeHost(flags);
+    if (copy_stream) cudaStreamDestroy(copy_stream);
+  }
 };
 
 namespace {
@@ -935,12 +947,42 @@ int scarf_srm_tc_batch_create(const scarf_tc_field* fields, int nfields, void* d
     return fail(SCARF_ERR_ARG, "workspace too small: %zu < %zu", work_bytes, need);
   }
   b->d_work = d_work;
-  const cudaError_t e = tc_batch_upload(in.data(), b->plan, d_work);
+  b->setups.resize(nfields);
+  b->in = in;
+  for (int f = 0; f < nfields; ++f) {
+    b->setups[f] = *fields[f].setup;
+    b->in[f].s = &b->setups[f];
+  }
+  const cudaError_t e = tc_batch_upload(b->in.data(), b->plan, d_work);
   if (e != cudaSuccess) {
     delete b;
     return cuda_fail(e, "tc_batch_upload");
   }
   *batch = b;
+  return SCARF_OK;
+}
+
+int scarf_srm_tc_batch_set_host_outputs(scarf_tc_batch* batch, float* const* host_fields) {
+  if (!batch) return fail(SCARF_ERR_ARG, "NULL batch");
+  const int nf = batch->plan.nfields;
+  if (host_fields) {
+    for (int f = 0; f < nf; ++f)
+      if (!host_fields[f]) return fail(SCARF_ERR_ARG, "host output %d is NULL", f);
+    if (!batch->flags) {
+      void* h = nullptr;
+      SCARF_CUDA(cudaHostAlloc(&h, sizeof(int) * nf, cudaHostAllocMapped));
+      batch->flags = static_cast<int*>(h);
+      void* d = nullptr;
+      SCARF_CUDA(cudaHostGetDevicePointer(&d, h, 0));
+      batch->flags_dev = static_cast<int*>(d);
+    }
+    if (!batch->copy_stream) SCARF_CUDA(cudaStreamCreateWithFlags(&batch->copy_stream, cudaStreamNonBlocking));
+    std::memset(batch->flags, 0, sizeof(int) * nf);
+    batch->host.assign(host_fields, host_fields + nf);
+  } else {
+    batch->host.clear();
+  }
+  SCARF_CUDA(tc_batch_upload(batch->in.data(), batch->plan, batch->d_work, host_fields ? batch->flags_dev : nullptr));
   return SCARF_OK;
 }
 
@@ -957,8 +999,39 @@ int scarf_srm_tc_batch_launch(const scarf_tc_batch* batch, void* stream) {
 
 int scarf_srm_tc_batch_wait(const scarf_tc_batch* batch, void* stream) {
   if (!batch) return fail(SCARF_ERR_ARG, "NULL batch");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (!batch->host.empty()) {
+    // Copy each field to its host buffer as soon as its flag rises, while
+    // the launch computes the others; whatever is left when the stream
+    // has finished (a failed launch) is copied then.
+    const int nf = batch->plan.nfields;
+    volatile int* flags = batch->flags;
+    std::vector<char> copied(nf, 0);
+    int left = nf;
+    bool idle = false;
+    for (uint32_t spins = 0; left > 0;) {
+      bool progress = false;
+      for (int f = 0; f < nf; ++f) {
+        if (copied[f] || (!idle && !flags[f])) continue;
+        const size_t bytes = sizeof(float) * static_cast<size_t>(batch->in[f].n[0]) * batch->in[f].n[1] *
+                             batch->in[f].n[2];
+        SCARF_CUDA(cudaMemcpyAsync(batch->host[f], batch->in[f].d_field, bytes, cudaMemcpyDeviceToHost,
+                                   batch->copy_stream));
+        copied[f] = 1;
+        --left;
+        progress = true;
+      }
+      if (!progress && (++spins & 1023u) == 0 && cudaStreamQuery(st) != cudaErrorNotReady) {
+        cudaGetLastError();
+        idle = true;
+      }
+      if (!progress) cpu_relax();
+    }
+    SCARF_CUDA(cudaStreamSynchronize(batch->copy_stream));
+    std::memset(batch->flags, 0, sizeof(int) * nf);
+  }
   const int* d_status = reinterpret_cast<const int*>(static_cast<const char*>(batch->d_work) + batch->plan.off_status);
-  const int rc = check_device_status(d_status, static_cast<cudaStream_t>(stream));
+  const int rc = check_device_status(d_status, st);
   if (!rc) collect_kernel_time();
   return rc;
 }

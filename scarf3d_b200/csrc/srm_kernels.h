@@ -109,15 +109,18 @@ struct TcBatchPlan {
   int nfields = 0, num_items = 0, ti = 0, tj = 0, ntile_max = 0, tmem_a = 0, pair = 0;
   size_t smem_rs = 0, smem_c = 0;  // shared memory of the factored table builders (largest field)
   int max_stages = 0;              // largest stage count of the fields
-  size_t off_fields = 0, off_jobs = 0, off_items = 0, off_status = 0, bytes = 0;
+  size_t off_fields = 0, off_jobs = 0, off_items = 0, off_done = 0, off_status = 0, bytes = 0;
   std::vector<TcPlan> plans;
   std::vector<size_t> field_off;
 };
 // Workspace bytes (0 if the fields cannot share one launch).
 size_t tc_batch_plan(const TcBatchInput* in, int nfields, TcBatchPlan* out);
 // Host -> device upload of descriptors, table jobs and the work list
-// (synchronous; not for use inside stream capture).
-cudaError_t tc_batch_upload(const TcBatchInput* in, const TcBatchPlan& plan, void* d_work);
+// (synchronous; not for use inside stream capture). With done_flags_dev
+// (device address of nfields host-mapped ints) each field raises its flag
+// once all of its items are stored.
+cudaError_t tc_batch_upload(const TcBatchInput* in, const TcBatchPlan& plan, void* d_work,
+                            int* done_flags_dev = nullptr);
 // Enqueue only: status/queue reset, table builds, persistent kernel.
 cudaError_t tc_batch_launch(const TcBatchPlan& plan, void* d_work, cudaStream_t stream,
                             cudaEvent_t ev_main0 = nullptr, cudaEvent_t ev_main1 = nullptr);

@@ -67,6 +67,12 @@ struct TcField {
   const float2* simg;   // [bj][stages][16][tj]
   const uint8_t* cimg;  // [bn][stages][part][hi,lo][ntile_n / parts * 64 B]
   float* field;
+  // Completion signal of a batch field (null when unused): every epilogue
+  // warp of every item adds one to done_cnt after its last chunk; the
+  // arrival that reaches done_expect sets the host-mapped done_flag.
+  int* done_cnt;
+  volatile int* done_flag;
+  int done_expect;
 };
 
 struct TcKernelArgs {
@@ -445,6 +451,18 @@ __device__ __forceinline__ void signal_slab(const TcKernelArgs& A, const TcField
   }
 }
 
+// The field's last item is stored: the last epilogue warp to arrive raises
+// the field's host flag. System-scope fences order the field stores before
+// the count and the count before the flag, as for slabs.
+__device__ __forceinline__ void signal_field(const TcField& f, int lane) {
+  __threadfence_system();
+  __syncwarp();
+  if (lane == 0 && atomicAdd(f.done_cnt, 1) == f.done_expect - 1) {
+    __threadfence_system();
+    *f.done_flag = 1;
+  }
+}
+
 // A operand of one stage into shared memory: row r of the tile (the
 // (ii, jj) point of the row block), kGenHarm harmonics from h0, FP16 hi and lo
 // images in the 64-B-swizzled K-major layout.
@@ -731,6 +749,7 @@ __global__ void __launch_bounds__(kThreads, 1) srm_tc_kernel(const TcKernelArgs 
         __syncwarp();
         if (lane == 0) mbar_arrive(acce);
         if (last && A.slab_cnt) signal_slab(A, w.f, w.ib, w.jb, w.nt, lane);
+        if (last && w.f.done_flag) signal_field(w.f, lane);
       }
     }
   } else if (warp >= kGenWarp0) {
@@ -1161,6 +1180,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1) srm_tc_
         __syncwarp();
         if (lane == 0) mbar_arrive_cluster(acce0);
         if (last && A.slab_cnt) signal_slab(A, w.f, ib, jb, w.nt, lane);
+        if (last && w.f.done_flag) signal_field(w.f, lane);
       }
     }
   } else if (warp >= kGenWarp0) {
@@ -1531,6 +1551,8 @@ size_t tc_batch_plan(const TcBatchInput* in, int nfields, TcBatchPlan* out) {
   bp.num_items = static_cast<int>(items);
   bp.off_items = off;
   off = align(off + sizeof(int2) * static_cast<size_t>(items));
+  bp.off_done = off;
+  off = align(off + sizeof(int) * static_cast<size_t>(nfields));
   bp.off_status = off;
   off = align(off + 256);
   bp.bytes = off;
@@ -1538,7 +1560,7 @@ size_t tc_batch_plan(const TcBatchInput* in, int nfields, TcBatchPlan* out) {
   return bp.bytes;
 }
 
-cudaError_t tc_batch_upload(const TcBatchInput* in, const TcBatchPlan& bp, void* d_work) {
+cudaError_t tc_batch_upload(const TcBatchInput* in, const TcBatchPlan& bp, void* d_work, int* done_flags_dev) {
   uint8_t* work = static_cast<uint8_t*>(d_work);
   std::vector<TcField> fields(bp.nfields);
   std::vector<TableJob> jobs(bp.nfields);
@@ -1548,6 +1570,11 @@ cudaError_t tc_batch_upload(const TcBatchInput* in, const TcBatchPlan& bp, void*
     jobs[f] = make_job(*in[f].s, in[f].fs, in[f].ds, in[f].d_table, in[f].nh, bp.plans[f], work + bp.field_off[f]);
     fields[f] = make_field(*in[f].s, bp.plans[f], jobs[f], in[f].d_field);
     const int nit = bp.plans[f].bix * bp.plans[f].bjx * bp.plans[f].bn;
+    if (done_flags_dev) {
+      fields[f].done_cnt = reinterpret_cast<int*>(work + bp.off_done) + f;
+      fields[f].done_flag = done_flags_dev + f;
+      fields[f].done_expect = (bp.plans[f].pair ? 8 : 4) * nit;  // epilogue warps per item
+    }
     for (int l = 0; l < nit; ++l) items.push_back(make_int2(f, l));
   }
   // Longest items first (the dynamic queue then balances the tail).
@@ -1571,6 +1598,8 @@ cudaError_t tc_batch_launch(const TcBatchPlan& bp, void* d_work, cudaStream_t st
   TableJob none{};
   int* status = reinterpret_cast<int*>(work + bp.off_status);
   cudaError_t e = cudaMemsetAsync(status, 0, 2 * sizeof(int), stream);
+  if (e != cudaSuccess) return e;
+  e = cudaMemsetAsync(work + bp.off_done, 0, sizeof(int) * bp.nfields, stream);  // field completion counts
   if (e != cudaSuccess) return e;
   launch_table_builders(none, jobs, bp.nfields, bp.max_stages, bp.smem_rs, bp.smem_c, nsm, stream);
   e = cudaGetLastError();

@@ -92,6 +92,41 @@ def test_batch_replays_from_a_cuda_graph():
     del g
 
 
+def test_batch_copies_fields_to_host_buffers_as_they_complete():
+    # Host outputs: wait() copies every field to its page-locked host buffer
+    # (field by field as the launch raises its flags), eagerly and from a
+    # graph replay, twice in a row; None turns the copy-out off again.
+    fields = _fields(nh_base=90)
+    batch = sb.TcBatch(_entries(fields), _alloc)
+    batch.launch()
+    batch.wait()
+    ref = [f["field"].cpu().clone() for f in fields]
+    hosts = [torch.full((f["field"].numel(),), float("nan"), dtype=torch.float32, pin_memory=True) for f in fields]
+    batch.set_host_outputs([h.data_ptr() for h in hosts])
+    batch.launch()
+    batch.wait()
+    for h, r in zip(hosts, ref):
+        assert torch.equal(h, r)
+    s = torch.cuda.Stream()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g, stream=s):
+        batch.launch(torch.cuda.current_stream().cuda_stream)
+    for _ in range(2):
+        for h in hosts:
+            h.fill_(float("nan"))
+        g.replay()
+        batch.wait(torch.cuda.current_stream().cuda_stream)
+        for h, r in zip(hosts, ref):
+            assert torch.equal(h, r)
+    del g
+    batch.set_host_outputs(None)
+    for h in hosts:
+        h.fill_(float("nan"))
+    batch.launch()
+    batch.wait()
+    assert all(torch.isnan(h).all() for h in hosts)
+
+
 def test_batch_rejects_mixed_row_tiles():
     fields = _fields()[:2]
     entries = _entries(fields)
