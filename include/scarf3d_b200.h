@@ -113,7 +113,7 @@ int scarf_set_tc_variant(int variant);
 /* Autotuning of the tensor-core form. No counterpart in the reference (its
  * SRM has one CPU code path). A tuning times every candidate plan -- kernel
  * form (SCARF_TC_*), row tile (128 / tile_j) x tile_j with tile_j in
- * {2, 4, 8, 16}, and for device fields whether the longest axis is the
+ * {1, 2, 4, 8, 16}, and for device fields whether the longest axis is the
  * column axis -- on the caller's grid and harmonic table (at most 2 048
  * harmonics of it; table builds and kernel), on the current GPU, and records
  * the fastest for the grid's shape bucket (extents rounded up to a multiple
@@ -236,9 +236,9 @@ int scarf_srm_tc_batch_wait(const scarf_tc_batch *batch, void *stream);
 int scarf_srm_tc_batch_set_host_outputs(scarf_tc_batch *batch, float *const *host_fields);
 void scarf_srm_tc_batch_destroy(scarf_tc_batch *batch);
 /* Times the batch's candidate plans (kernel form SCARF_TC_SINGLE or
- * SCARF_TC_PAIR, tile_j in {2, 4, 8, 16} for every field) on the fields'
+ * SCARF_TC_PAIR, tile_j in {1, 2, 4, 8, 16} for every field) on the fields'
  * own tables, overwriting their outputs, and returns the fastest (the
- * default, one-CTA form with tile_j 8, unless beaten by 3 %): create the
+ * default, one-CTA form with the automatic tile_j, unless beaten by 3 %): create the
  * batch with each field's tile_j set to out->tile_j after
  * scarf_set_tc_variant(out->variant). Synchronises `stream`; allocates its
  * own device scratch. */

@@ -1218,7 +1218,7 @@ int scarf_srm_tc_autotune(const scarf_srm_setup* s, const int fs[3], const int n
   // reach its steady state, short enough to try every candidate.
   const int nh_probe = std::min(nh, 2048);
   const int forms[3] = {SCARF_TC_SINGLE, SCARF_TC_PAIR, SCARF_TC_SINGLE_TMEM_A};
-  const int tiles[4] = {2, 4, 8, 16};
+  const int tiles[5] = {1, 2, 4, 8, 16};
   std::vector<TcPlan> plans;
   std::vector<scarf::TcChoice> choices;
   for (int v : forms)
@@ -1285,7 +1285,7 @@ int scarf_srm_tc_batch_autotune(const scarf_tc_field* fields, int nfields, void*
   if (!out || !batch_fields_valid(fields, nfields)) return fail(SCARF_ERR_ARG, "invalid argument");
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   const int forms[2] = {SCARF_TC_SINGLE, SCARF_TC_PAIR};
-  const int tiles[4] = {2, 4, 8, 16};
+  const int tiles[5] = {1, 2, 4, 8, 16};
   std::lock_guard<std::mutex> lk(g_mu);  // the kernel form is global while a batch is planned
   const int saved = tc_get_variant();
   cudaEvent_t e0 = nullptr, e1 = nullptr;
@@ -1295,6 +1295,13 @@ int scarf_srm_tc_batch_autotune(const scarf_tc_field* fields, int nfields, void*
     return fail(SCARF_ERR_CUDA, "autotune: event creation failed");
   }
   scarf::TcChoice best{-1, 0, 1, 0.0f}, deflt{-1, 0, 1, 0.0f};
+  int auto_tj = 8;  // the row tile the batch would get with tile_j = 0
+  {
+    auto in0 = batch_inputs(fields, nfields);
+    for (auto& e : in0) e.tj = 0;
+    TcBatchPlan bp0;
+    if (tc_batch_plan(in0.data(), nfields, &bp0)) auto_tj = bp0.tj;
+  }
   for (int v : forms) {
     tc_set_variant(v);
     for (int tj : tiles) {
@@ -1326,11 +1333,11 @@ int scarf_srm_tc_batch_autotune(const scarf_tc_field* fields, int nfields, void*
       cudaGetLastError();
       cudaFree(d_work);
       if (ms > 0.0f && (best.variant < 0 || ms < best.ms)) best = scarf::TcChoice{v, tj, 1, ms};
-      if (ms > 0.0f && v == SCARF_TC_SINGLE && tj == 8) deflt = scarf::TcChoice{v, tj, 1, ms};
+      if (ms > 0.0f && v == SCARF_TC_SINGLE && tj == auto_tj) deflt = scarf::TcChoice{v, tj, 1, ms};
     }
   }
-  // As for single grids: the default (one-CTA form, 16 x 8 row tiles) stays
-  // unless a candidate beats it by 3 %.
+  // As for single grids: the default (one-CTA form, automatic row tile)
+  // stays unless a candidate beats it by 3 %.
   if (deflt.variant >= 0 && best.ms > 0.97f * deflt.ms) best = deflt;
   tc_set_variant(saved);
   cudaEventDestroy(e0);

@@ -40,9 +40,13 @@ def _case(n, nharm=600):
 
 
 def _tc(s, n, tab):
+    return _tc_nd(s, n, tab, 3)
+
+
+def _tc_nd(s, n, tab, ndim):
     d_tab = torch.from_numpy(np.ascontiguousarray(tab.reshape(-1))).cuda()
     out = torch.full((int(np.prod(n)),), float("nan"), dtype=torch.float32, device="cuda")
-    wb = sb.tc_workspace_bytes(3, n, len(tab))
+    wb = sb.tc_workspace_bytes(ndim, n, len(tab))
     work = torch.empty(wb, dtype=torch.uint8, device="cuda")
     import ctypes
     from srm_cases import iarr
@@ -62,7 +66,7 @@ def test_tuning_is_recorded_and_followed(tmp_path):
     d_tab = torch.from_numpy(np.ascontiguousarray(tab.reshape(-1))).cuda()
     t = sb.tc_autotune(s, [1, 1, 1], n, 40.0, d_tab.data_ptr(), len(tab))
     assert t["variant"] in (sb.TC_SINGLE, sb.TC_PAIR, sb.TC_SINGLE_TMEM_A)
-    assert t["tile_j"] in (2, 4, 8, 16) and t["ms"] > 0.0
+    assert t["tile_j"] in (1, 2, 4, 8, 16) and t["ms"] > 0.0
     default = sb.tc_plan_info(3, n, len(tab))
     other_default = sb.tc_plan_info(3, [200, 48, 72], len(tab))
     sb.set_tc_autotune(1)
@@ -93,7 +97,7 @@ def test_every_candidate_plan_computes_the_field():
         key = cache.read_text().split()[0]
         fields = []
         for variant in (sb.TC_SINGLE, sb.TC_PAIR, sb.TC_SINGLE_TMEM_A):
-            for tj in (2, 4, 8, 16):
+            for tj in (1, 2, 4, 8, 16):
                 for perm in (0, 1):
                     cache.write_text(f"{key} {variant} {tj} {perm} 1.0\n")
                     sb.set_tc_tune_cache(cache)
@@ -164,7 +168,7 @@ def test_batch_tuning_returns_a_plan_that_runs():
     b.wait()
     ref = [o.cpu().numpy().copy() for o in outs]
     t = sb.tc_batch_autotune(entries)
-    assert t["variant"] in (sb.TC_SINGLE, sb.TC_PAIR) and t["tile_j"] in (2, 4, 8, 16) and t["ms"] > 0
+    assert t["variant"] in (sb.TC_SINGLE, sb.TC_PAIR) and t["tile_j"] in (1, 2, 4, 8, 16) and t["ms"] > 0
     sb.set_tc_variant(t["variant"])
     for e in entries:
         e["tile_j"] = t["tile_j"]
@@ -175,3 +179,24 @@ def test_batch_tuning_returns_a_plan_that_runs():
     b2.wait()
     for o, r in zip(outs, ref):
         assert np.array_equal(o.cpu().numpy().view(np.uint32), r.view(np.uint32))
+
+
+def test_two_dimensional_grid_tuning():
+    # 2-D grids: the single z plane is the row-slow axis, so row tiles with
+    # tile_j > 1 waste rows; the tuner must offer tile_j = 1 (the default).
+    n = [300, 200, 1]
+    fc = [float(np.float32(v - 1) * np.float32(40.0)) for v in n[:2]] + [0.0]
+    kw = dict(KW, cl=[1500.0, 1500.0, 0.0])
+    p = sb.make_params(nc=[0.0, 0.0, 0.0], fc=fc, nharm=300, **kw)
+    s = sb.compute_setup(p)
+    tab, _ = sb.sample(p, s)
+    d_tab = torch.from_numpy(np.ascontiguousarray(tab.reshape(-1))).cuda()
+    default = sb.tc_plan_info(2, n, len(tab))
+    assert default["tile_j"] == 1
+    t = sb.tc_autotune(s, [1, 1, 1], n, 40.0, d_tab.data_ptr(), len(tab))
+    sb.set_tc_autotune(1)
+    field = _tc_nd(s, n, tab, 2)
+    op = oracle.params(nharm=300, dh=40.0, nc=[0.0] * 3, fc=fc, **kw)
+    ref64 = oracle.sum_structured(oracle.setup(op), [1, 1, 1], n, 40.0, tab, f64=True)
+    assert rel_rms(field, ref64) <= 1e-5
+    assert t["tile_j"] in (1, 2, 4, 8, 16)
