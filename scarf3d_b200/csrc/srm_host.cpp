@@ -4,12 +4,15 @@
 #include "srm_host.h"
 
 #include <cuda_runtime.h>
+#include <unistd.h>
 
 #include <algorithm>
 #include <atomic>
 #include <cmath>
+#include <condition_variable>
 #include <cstdlib>
 #include <cstring>
+#include <functional>
 #include <memory>
 #include <mutex>
 #include <thread>
@@ -206,6 +209,105 @@ int host_threads() {
   return static_cast<int>(std::max(1u, std::min(hc, 64u)));
 }
 
+// ------------------------------------------------------ host worker pool --
+namespace {
+
+// Persistent host workers for the sampler's short parallel loops (field
+// walks, table rows, rejection rounds): creating threads per loop costs tens
+// of microseconds per thread, more than a 20 000-row loop itself. A job is a
+// shared object with its own task counter, so a worker that wakes late for a
+// finished job finds no task left and never calls a stale function; the
+// caller takes tasks too and waits only for tasks, never for workers.
+class HostPool {
+ public:
+  // Runs fn(0) .. fn(ntasks - 1) on at most `width` threads (the caller's
+  // included) and returns when all have returned. Jobs from several caller
+  // threads run one after another; fn must not start another job.
+  void run(int ntasks, int width, const std::function<void(int)>& fn) {
+    if (ntasks <= 0) return;
+    width = std::min(width, ntasks);
+    if (width <= 1) {
+      for (int i = 0; i < ntasks; ++i) fn(i);
+      return;
+    }
+    std::lock_guard<std::mutex> serial(run_mu_);
+    auto job = std::make_shared<Job>();
+    job->fn = &fn;
+    job->ntasks = ntasks;
+    job->slots = width - 1;
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      for (; nworkers_ < width - 1; ++nworkers_) std::thread([this] { worker_loop(); }).detach();
+      job_ = job;
+      ++gen_;
+    }
+    cv_.notify_all();
+    work(*job);
+    std::unique_lock<std::mutex> lk(mu_);
+    done_cv_.wait(lk, [&] { return job->done.load() == job->ntasks; });
+    job_.reset();
+  }
+
+ private:
+  struct Job {
+    const std::function<void(int)>* fn = nullptr;
+    int ntasks = 0;
+    std::atomic<int> slots{0}, next{0}, done{0};
+  };
+
+  void work(Job& j) {
+    for (int i = j.next.fetch_add(1); i < j.ntasks; i = j.next.fetch_add(1)) {
+      (*j.fn)(i);
+      if (j.done.fetch_add(1) + 1 == j.ntasks) {
+        std::lock_guard<std::mutex> lk(mu_);
+        done_cv_.notify_all();
+      }
+    }
+  }
+
+  void worker_loop() {
+    unsigned long long seen = 0;
+    for (;;) {
+      std::shared_ptr<Job> job;
+      {
+        std::unique_lock<std::mutex> lk(mu_);
+        cv_.wait(lk, [&] { return gen_ != seen; });
+        seen = gen_;
+        job = job_;
+      }
+      if (job && job->slots.fetch_sub(1) > 0) work(*job);
+    }
+  }
+
+  std::mutex run_mu_, mu_;
+  std::condition_variable cv_, done_cv_;
+  std::shared_ptr<Job> job_;
+  unsigned long long gen_ = 0;
+  int nworkers_ = 0;  // detached threads; they live as long as the process
+};
+
+// One pool per process: a child made by fork() has none of its parent's
+// workers (and may hold copies of locked mutexes), so it starts a new pool;
+// the parent's object is left as it is.
+HostPool& host_pool() {
+  static std::mutex mu;
+  static HostPool* pool = nullptr;
+  static pid_t owner = 0;
+  std::lock_guard<std::mutex> lk(mu);
+  const pid_t pid = getpid();
+  if (!pool || owner != pid) {
+    pool = new HostPool();
+    owner = pid;
+  }
+  return *pool;
+}
+
+}  // namespace
+
+void parallel_tasks(int ntasks, int width, const std::function<void(int)>& fn) {
+  host_pool().run(ntasks, width, fn);
+}
+
 // ------------------------------------------------------------- sampler -----
 namespace {
 
@@ -298,23 +400,18 @@ int walk_parallel(const scarf_srm_params& p, const scarf_srm_setup& s, int threa
   base.seed(p.seed);
 
   auto fill = [&](int64_t first_pair, std::vector<float>& r, std::vector<uint8_t>& acc, std::vector<float>& uu) {
-    std::vector<std::thread> pool;
-    pool.reserve(threads);
-    for (int t = 0; t < threads; ++t) {
-      pool.emplace_back([&, t]() {
-        Yarn2 g = base;
-        g.jump(2ull * static_cast<uint64_t>(first_pair + t * chunk));
-        for (int64_t q = t * chunk; q < (t + 1) * chunk; ++q) {
-          const float r1 = g.next_u01(), r2 = g.next_u01();
-          r[2 * q] = r1;
-          r[2 * q + 1] = r2;
-          float u;
-          acc[q] = accept(r1, r2, s, p.acf, &u) ? 1 : 0;
-          uu[q] = u;
-        }
-      });
-    }
-    for (auto& th : pool) th.join();
+    parallel_tasks(threads, threads, [&](int t) {
+      Yarn2 g = base;
+      g.jump(2ull * static_cast<uint64_t>(first_pair + t * chunk));
+      for (int64_t q = t * chunk; q < (t + 1) * chunk; ++q) {
+        const float r1 = g.next_u01(), r2 = g.next_u01();
+        r[2 * q] = r1;
+        r[2 * q + 1] = r2;
+        float u;
+        acc[q] = accept(r1, r2, s, p.acf, &u) ? 1 : 0;
+        uu[q] = u;
+      }
+    });
   };
 
   int64_t cur_first = 0;
@@ -538,6 +635,7 @@ struct DeviceWalk {
   int kept = 0, l = 0;
 
   bool walk() {
+    if (draws.empty()) draws.reserve(p->nharm);
     for (; l < p->nharm; ++l) {
       for (;;) {
         while (ei < nent && ent[ei].q < pos) ++ei;
@@ -717,15 +815,7 @@ int srm_sample_device_batch(int nfields, const scarf_srm_params* p, const scarf_
     w.nent = overflow[f] ? 0 : static_cast<size_t>(ebeg[f + 1] - ebeg[f]);
     if (overflow[f]) w.pass_end = 0;
   }
-  const int nthr = std::max(1, std::min(host_threads(), nfields));
-  std::atomic<int> next{0};
-  auto worker = [&]() {
-    for (int f = next.fetch_add(1); f < nfields; f = next.fetch_add(1)) done[f] = walks[f].walk() ? 1 : 0;
-  };
-  std::vector<std::thread> pool;
-  for (int t = 1; t < nthr; ++t) pool.emplace_back(worker);
-  worker();
-  for (auto& th : pool) th.join();
+  parallel_tasks(nfields, host_threads(), [&](int f) { done[f] = walks[f].walk() ? 1 : 0; });
   long long open_total = 0;
   for (int f = 0; f < nfields; ++f) {
     DeviceWalk& w = walks[f];
@@ -744,25 +834,17 @@ int srm_sample_device_batch(int nfields, const scarf_srm_params* p, const scarf_
   // threads in blocks of rows; each row depends on its own draw only.
   std::vector<long long> rbeg(nfields + 1, 0);
   for (int f = 0; f < nfields; ++f) rbeg[f + 1] = rbeg[f] + walks[f].kept;
-  constexpr long long kRowBlock = 2048;
+  constexpr long long kRowBlock = 512;
   const long long nblocks = (rbeg[nfields] + kRowBlock - 1) / kRowBlock;
-  std::atomic<long long> next_block{0};
-  auto rows = [&]() {
-    for (long long b = next_block.fetch_add(1); b < nblocks; b = next_block.fetch_add(1)) {
-      const long long r0 = b * kRowBlock, r1 = std::min(rbeg[nfields], r0 + kRowBlock);
-      int f = static_cast<int>(std::upper_bound(rbeg.begin(), rbeg.end(), r0) - rbeg.begin()) - 1;
-      for (long long r = r0; r < r1; ++r) {
-        while (r >= rbeg[f + 1]) ++f;
-        const long long i = r - rbeg[f];
-        harmonic_row(walks[f].draws[i], s[f].ndim, p[f].cl, tables[f] + 5 * i);
-      }
+  parallel_tasks(static_cast<int>(nblocks), host_threads(), [&](int b) {
+    const long long r0 = b * kRowBlock, r1 = std::min(rbeg[nfields], r0 + kRowBlock);
+    int f = static_cast<int>(std::upper_bound(rbeg.begin(), rbeg.end(), r0) - rbeg.begin()) - 1;
+    for (long long r = r0; r < r1; ++r) {
+      while (r >= rbeg[f + 1]) ++f;
+      const long long i = r - rbeg[f];
+      harmonic_row(walks[f].draws[i], s[f].ndim, p[f].cl, tables[f] + 5 * i);
     }
-  };
-  const int nrow_thr = static_cast<int>(std::max<long long>(1, std::min<long long>(host_threads(), nblocks)));
-  std::vector<std::thread> rpool;
-  for (int t = 1; t < nrow_thr; ++t) rpool.emplace_back(rows);
-  rows();
-  for (auto& th : rpool) th.join();
+  });
   if (uncertain) *uncertain = open_total;
   return 0;
 }

@@ -4,6 +4,7 @@
 
 #include <cstddef>
 #include <cstdint>
+#include <functional>
 #include <vector>
 
 #include "scarf3d_b200.h"
@@ -90,5 +91,9 @@ int srm_sample_device_batch(int nfields, const scarf_srm_params* p, const scarf_
 void set_device_sampler_pass_cap(long long pairs);
 
 int host_threads();
+
+// Runs fn(0) .. fn(ntasks - 1) on at most `width` host threads (the caller's
+// included) from a persistent worker pool; returns when all have returned.
+void parallel_tasks(int ntasks, int width, const std::function<void(int)>& fn);
 
 }  // namespace scarf

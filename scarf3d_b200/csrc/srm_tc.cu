@@ -24,6 +24,8 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdlib>
+#include <cstring>
 #include <numeric>
 #include <vector>
 
@@ -335,6 +337,122 @@ __global__ void tc_build_c_factored(const TableJob j0, const TableJob* jobs) {
   }
 }
 
+// The same factored builders with a warp, not a block, per harmonic (R/S)
+// or per 4-harmonic chunk (C): each warp keeps its own factor tables and
+// synchronises with __syncwarp only. Small fields have few entries per
+// harmonic (a 64-point axis: 40 sincos and 128 entries), so a block per
+// harmonic leaves most threads waiting at its two barriers; with a warp per
+// harmonic four harmonics are in flight per block. Every entry is computed
+// by the same FP64 operations as above, so the images are bit-identical.
+constexpr int kBuilderWarps = 4;
+
+__global__ void __launch_bounds__(32 * kBuilderWarps) tc_build_rs_warps(const TableJob j0, const TableJob* jobs) {
+  extern __shared__ double2 fsh[];
+  const TableJob& T = jobs ? jobs[blockIdx.y] : j0;
+  const int nr = T.bi * T.ti, ns = T.bj * T.tj;
+  const int nur = (nr + 15) / 16, nus = (ns + 15) / 16;
+  const int nfac = nur + nus + 32;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  double2* ur = fsh + warp * nfac;
+  double2* vr = ur + nur;
+  double2* us = vr + 16;
+  double2* vs = us + nus;
+  const double offr = T.off[T.ax_r], offs = T.off[T.ax_s];
+  for (int h = blockIdx.x * kBuilderWarps + warp; h < T.stages * kStageHarm; h += gridDim.x * kBuilderWarps) {
+    const bool valid = h < T.nh;
+    double kv[3] = {0.0, 0.0, 0.0}, c = 0.0, a = 0.0, b = 0.0;
+    if (valid) harmonic_k(T, h, kv, c, a, b);
+    const double kr = kv[T.ax_r], ks = kv[T.ax_s];
+    __syncwarp();  // the previous harmonic's entries are written
+    for (int e = lane; e < nfac; e += 32) {
+      if (e < nur) {
+        ur[e] = expi(kr * ((16.0 * e + offr) * T.ds) + c);
+      } else if (e < nur + 16) {
+        vr[e - nur] = expi(kr * ((e - nur) * T.ds));
+      } else if (e < nur + 16 + nus) {
+        us[e - nur - 16] = expi(ks * ((16.0 * (e - nur - 16) + offs) * T.ds));
+      } else {
+        vs[e - nur - 16 - nus] = expi(ks * ((e - nur - 16 - nus) * T.ds));
+      }
+    }
+    __syncwarp();
+    const int k = h / kStageHarm, hp = h - k * kStageHarm;
+    for (int e = lane; e < nr + ns; e += 32) {
+      const bool is_r = e < nr;
+      const int idx = is_r ? e : e - nr;
+      const int tw = is_r ? T.ti : T.tj;
+      const int blk = idx / tw, t = idx - blk * tw;
+      float2 out = make_float2(0.0f, 0.0f);
+      if (valid && idx < (is_r ? T.n1 : T.n2)) {
+        if (is_r) {
+          const double2 z = cmul(ur[idx >> 4], vr[idx & 15]);
+          out = make_float2(static_cast<float>(b * z.x + a * z.y), static_cast<float>(b * z.y - a * z.x));
+        } else {
+          const double2 z = cmul(us[idx >> 4], vs[idx & 15]);
+          out = make_float2(static_cast<float>(z.x), static_cast<float>(z.y));
+        }
+      }
+      const size_t q = ((static_cast<size_t>(blk) * T.stages + k) * kStageHarm + hp) * tw + t;
+      (is_r ? T.rimg : T.simg)[q] = out;
+    }
+  }
+}
+
+__global__ void __launch_bounds__(32 * kBuilderWarps) tc_build_c_warps(const TableJob j0, const TableJob* jobs) {
+  extern __shared__ double2 fsh[];
+  const TableJob& T = jobs ? jobs[blockIdx.y] : j0;
+  const int ncol = T.bn * T.ntile_n;
+  const int nu = (ncol + 15) / 16;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  double2* u4 = fsh + warp * 4 * (nu + 16);  // [4][nu]
+  double2* v4 = u4 + 4 * nu;                 // [4][16]
+  const double offc = T.off[T.ax_c];
+  const int part_rows = T.ntile_n / T.parts;
+  for (int j = blockIdx.x * kBuilderWarps + warp; j < T.stages * 4; j += gridDim.x * kBuilderWarps) {
+    const int k = j >> 2, chunk = j & 3;
+    bool valid[4];
+    double kc[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int h = k * kStageHarm + chunk * 4 + u;
+      valid[u] = h < T.nh;
+      double kv[3] = {0.0, 0.0, 0.0}, c, a, b;
+      if (valid[u]) harmonic_k(T, h, kv, c, a, b);
+      kc[u] = kv[T.ax_c];
+    }
+    __syncwarp();  // the previous chunk's entries are written
+    for (int e = lane; e < 4 * (nu + 16); e += 32) {
+      const int u = e / (nu + 16), r = e - u * (nu + 16);
+      if (r < nu) u4[u * nu + r] = expi(kc[u] * ((16.0 * r + offc) * T.ds));
+      else v4[u * 16 + (r - nu)] = expi(kc[u] * ((r - nu) * T.ds));
+    }
+    __syncwarp();
+    for (int col = lane; col < ncol; col += 32) {
+      const int nb = col / T.ntile_n, row = col - nb * T.ntile_n;
+      const int part = row / part_rows, prow = row - part * part_rows;
+      __half2 hi[4], lo[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        float cs32 = 0.0f, sn32 = 0.0f;
+        if (valid[u] && col < T.n3) {
+          const double2 z = cmul(u4[u * nu + (col >> 4)], v4[u * 16 + (col & 15)]);
+          cs32 = static_cast<float>(z.x);
+          sn32 = static_cast<float>(z.y);
+        }
+        hi[u] = __floats2half2_rn(cs32, sn32);
+        const float2 hf = __half22float2(hi[u]);
+        lo[u] = __floats2half2_rn(cs32 - hf.x, sn32 - hf.y);
+      }
+      uint8_t* base = T.cimg + ((static_cast<size_t>(nb) * T.stages + k) * T.parts + part) *
+                                   (2u * part_rows * kRowBytes);
+      const uint32_t off = swz64(static_cast<uint32_t>(prow), static_cast<uint32_t>(chunk));
+      *reinterpret_cast<uint4*>(base + off) = *reinterpret_cast<const uint4*>(hi);
+      *reinterpret_cast<uint4*>(base + static_cast<size_t>(part_rows) * kRowBytes + off) =
+          *reinterpret_cast<const uint4*>(lo);
+    }
+  }
+}
+
 // Shared memory of the factored builders for a plan (image widths as
 // make_job sets them, padded to whole row blocks).
 size_t factor_smem_rs(const TcPlan& p) {
@@ -355,12 +473,30 @@ void launch_table_builders(const TableJob& T, const TableJob* jobs, int nfields,
                            size_t smem_c, int nsm, cudaStream_t stream) {
   const int per_field = std::max(1, nsm * 64 / std::max(1, nfields));
   const int grid_old = std::max(1, std::min(64, nsm * 8 / std::max(1, nfields)));
-  if (smem_rs <= static_cast<size_t>(kFactorSmem))
+  // Builder form: warps while each warp's factor tables fit (default), else
+  // blocks, else direct; SCARF3D_B200_TABLE_BUILDER=block|direct forces a
+  // form (the forms are compared in tests).
+  static const int forced = [] {
+    const char* e = std::getenv("SCARF3D_B200_TABLE_BUILDER");
+    if (!e) return 0;
+    if (!std::strcmp(e, "block")) return 1;
+    if (!std::strcmp(e, "direct")) return 2;
+    return 0;
+  }();
+  const size_t warps_limit = static_cast<size_t>(kFactorSmem) / kBuilderWarps;
+  if (forced == 0 && smem_rs <= warps_limit)
+    tc_build_rs_warps<<<dim3(std::min((max_stages * kStageHarm + kBuilderWarps - 1) / kBuilderWarps, per_field),
+                             nfields),
+                        32 * kBuilderWarps, kBuilderWarps * smem_rs, stream>>>(T, jobs);
+  else if (forced <= 1 && smem_rs <= static_cast<size_t>(kFactorSmem))
     tc_build_rs_factored<<<dim3(std::min(max_stages * kStageHarm, per_field), nfields), 128, smem_rs, stream>>>(
         T, jobs);
   else
     tc_build_rs<<<dim3(jobs ? grid_old : nsm * 8, nfields), 256, 0, stream>>>(T, jobs);
-  if (smem_c <= static_cast<size_t>(kFactorSmem))
+  if (forced == 0 && smem_c <= warps_limit)
+    tc_build_c_warps<<<dim3(std::min((max_stages * 4 + kBuilderWarps - 1) / kBuilderWarps, per_field), nfields),
+                       32 * kBuilderWarps, kBuilderWarps * smem_c, stream>>>(T, jobs);
+  else if (forced <= 1 && smem_c <= static_cast<size_t>(kFactorSmem))
     tc_build_c_factored<<<dim3(std::min(max_stages * 4, per_field), nfields), 128, smem_c, stream>>>(T, jobs);
   else
     tc_build_c<<<dim3(jobs ? grid_old : nsm * 8, nfields), 256, 0, stream>>>(T, jobs);
