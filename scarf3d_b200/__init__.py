@@ -481,6 +481,9 @@ class TcBatch:
         if self.bytes == 0:
             raise ScarfError(SCARF_ERR_ARG, "fields cannot share one batched launch")
         self.work = alloc(self.bytes)
+        # held by the instance: module globals may already be gone when a
+        # batch is collected at interpreter exit
+        self._destroy = lib.scarf_srm_tc_batch_destroy
         self._h = ctypes.c_void_p()
         check(lib.scarf_srm_tc_batch_create(arr, len(entries), ctypes.c_void_p(self.work.data_ptr()), self.bytes,
                                             ctypes.byref(self._h)))
@@ -503,8 +506,13 @@ class TcBatch:
     def wait(self, stream_handle: int | None = None):
         check(lib.scarf_srm_tc_batch_wait(self._h, ctypes.c_void_p(stream_handle or 0)))
 
-    def __del__(self):
+    def close(self):
+        """Releases the batch's host-side state (its workspace belongs to the
+        caller's allocation); later calls raise."""
         h = getattr(self, "_h", None)
         if h:
-            lib.scarf_srm_tc_batch_destroy(h)
-            self._h = None
+            self._destroy(h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        self.close()
