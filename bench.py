@@ -448,9 +448,14 @@ def run_b200(args, w):
     for _ in range(max(1, args.warmup)):
         sb.check(sb.lib.scarf_execute_ex(w["seed"], fptr, sptr_stats, 0))
     barrier()
+    host_s, device_s = [], []
     t0 = time.perf_counter()
     for _ in range(args.steps):
         sb.check(sb.lib.scarf_execute_ex(w["seed"], fptr, sptr_stats, 0))
+        # stats[4]: host time (setup + harmonic sampling); stats[5]: device
+        # time from the table upload to the last byte of the field on the host
+        host_s.append(float(stats[4]))
+        device_s.append(float(stats[5]))
     t_e2e = max_over_ranks(time.perf_counter() - t0)
     if world > 1:
         # Chan merge of (n, mean, var) across ranks (scarflib_common.f90:823-875).
@@ -491,7 +496,8 @@ def run_b200(args, w):
             "accuracy": acc,
             "batched": batched,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(nh * 20),
-                    "d2h_bytes_per_step": int(npts * 4 + 8), "ms_per_step": t_e2e / args.steps * 1e3},
+                    "d2h_bytes_per_step": int(npts * 4 + 8), "ms_per_step": t_e2e / args.steps * 1e3,
+                    "host_sampling_ms": float(np.mean(host_s)) * 1e3, "device_ms": float(np.mean(device_s)) * 1e3},
             "gpu_launches": 3 * args.steps,
             "clocks": clocks,
             "cpu_baseline": cpu,
