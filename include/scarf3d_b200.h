@@ -83,6 +83,26 @@ int scarf_set_host_threads(int nthreads);
  * such duration in milliseconds. */
 int scarf_set_kernel_timing(int enable);
 float scarf_last_kernel_ms(void);
+/* Cap on the device memory the library allocates for itself (tables,
+ * staging fields, sampler and tuning scratch), summed over all devices;
+ * 0 = no cap (default). A call that would pass the cap fails with
+ * SCARF_ERR_NOMEM and leaves the library usable; buffers the caller passes
+ * in (device fields, batch workspaces) do not count. Buffers are kept
+ * between calls and only grow, so the cap bounds the high-water mark. */
+int scarf_set_device_memory_cap(size_t bytes);
+/* Device bytes the library holds now. */
+size_t scarf_device_memory_in_use(void);
+/* Frees the device buffers the library keeps between calls (they are
+ * allocated again on demand); waits for the library's device work first. */
+int scarf_release_device_memory(void);
+/* Self-test of the bounded waits inside every pipeline kernel: `blocks`
+ * blocks (1..1024) wait on an mbarrier that nothing arrives on, through the
+ * same bounded wait (limit 2 s) the pipeline kernels use. Returns SCARF_OK
+ * when a wait ran out and wrote the timeout code into the status word, as
+ * designed; *device_status (if non-NULL) receives the status word and
+ * *waited_s (if non-NULL) the longest wait in seconds. Nothing faults: the
+ * context stays usable. No counterpart in the reference. */
+int scarf_selftest_wait_limit(int blocks, int *device_status, double *waited_s);
 /* Harmonics accumulated in tensor memory before each FP32 drain of the
  * tensor-core form (0 = default, 512). The tensor core's FP32 accumulation
  * does not round to nearest, so its error grows with this length. */

@@ -34,7 +34,9 @@ EXPORTED_SYMBOLS = (
     # extended (include/scarf3d_b200.h)
     "scarf_last_error", "scarf_set_nharm", "scarf_get_nharm", "scarf_set_form",
     "scarf_set_uniform_source", "scarf_set_stream", "scarf_set_host_threads", "scarf_set_kernel_timing",
-    "scarf_last_kernel_ms", "scarf_set_tc_chunk", "scarf_set_tc_variant", "scarf_set_output_overlap",
+    "scarf_last_kernel_ms", "scarf_set_device_memory_cap", "scarf_device_memory_in_use",
+    "scarf_release_device_memory",
+    "scarf_selftest_wait_limit", "scarf_set_tc_chunk", "scarf_set_tc_variant", "scarf_set_output_overlap",
     "scarf_execute_ex",
     "scarf_srm_compute_setup", "scarf_srm_sample", "scarf_srm_sample_device", "scarf_srm_sample_device_batch",
     "scarf_set_sampler",
@@ -123,6 +125,10 @@ def _load() -> ctypes.CDLL:
         "scarf_set_host_threads": (c_int, [c_int]),
         "scarf_set_kernel_timing": (c_int, [c_int]),
         "scarf_last_kernel_ms": (c_float, []),
+        "scarf_set_device_memory_cap": (c_int, [c_size_t]),
+        "scarf_device_memory_in_use": (c_size_t, []),
+        "scarf_release_device_memory": (c_int, []),
+        "scarf_selftest_wait_limit": (c_int, [c_int, ctypes.POINTER(c_int), ctypes.POINTER(ctypes.c_double)]),
         "scarf_set_tc_chunk": (c_int, [c_int]),
         "scarf_set_tc_variant": (c_int, [c_int]),
         "scarf_set_output_overlap": (c_int, [c_int]),
@@ -389,6 +395,31 @@ def set_tc_variant(variant: int):
     """Tensor-core kernel form for plans made afterwards: TC_SINGLE (default),
     TC_PAIR (CTA pairs with cta_group::2 MMAs) or TC_SINGLE_TMEM_A."""
     check(lib.scarf_set_tc_variant(int(variant)))
+
+
+def set_device_memory_cap(nbytes: int):
+    """Cap on the device memory the library allocates for itself (0: none);
+    calls that would pass it raise ScarfError(SCARF_ERR_NOMEM)."""
+    check(lib.scarf_set_device_memory_cap(int(nbytes)))
+
+
+def device_memory_in_use() -> int:
+    return int(lib.scarf_device_memory_in_use())
+
+
+def release_device_memory():
+    """Frees the device buffers the library keeps between calls."""
+    check(lib.scarf_release_device_memory())
+
+
+def selftest_wait_limit(blocks: int = 4) -> dict:
+    """Runs the bounded-wait self-test (blocks wait on an mbarrier that nothing
+    arrives on); returns the status word and the longest wait in seconds.
+    Raises when the waits did not report the timeout as designed."""
+    st = ctypes.c_int(-1)
+    waited = ctypes.c_double(0.0)
+    check(lib.scarf_selftest_wait_limit(int(blocks), ctypes.byref(st), ctypes.byref(waited)))
+    return {"status": st.value, "waited_s": waited.value}
 
 
 def set_tc_autotune(mode: int):

@@ -41,7 +41,21 @@ int fail(int code, const char* fmt, ...) {
 }
 
 int cuda_fail(cudaError_t e, const char* what) {
+  if (e == cudaErrorMemoryAllocation) {
+    cudaGetLastError();  // a failed cudaMalloc leaves no sticky error
+    return fail(SCARF_ERR_NOMEM, "%s: %s (library device memory in use: %zu bytes)", what, cudaGetErrorString(e),
+                scarf::device_memory_in_use());
+  }
   return fail(SCARF_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+
+// A device-sampler failure: out of device memory (or over the library's
+// cap) when an allocation on this thread said so, else a CUDA error.
+int sampler_fail(const char* what) {
+  if (scarf::take_device_alloc_failure())
+    return fail(SCARF_ERR_NOMEM, "%s: out of device memory (library device memory in use: %zu bytes)", what,
+                scarf::device_memory_in_use());
+  return fail(SCARF_ERR_CUDA, "%s: CUDA error", what);
 }
 
 #define SCARF_CUDA(call)                                   \
@@ -94,15 +108,15 @@ struct DeviceBuf {
   size_t bytes = 0;
   cudaError_t ensure(size_t need) {
     if (need <= bytes) return cudaSuccess;
-    if (p) cudaFree(p);
+    scarf::device_free(p, bytes);
     p = nullptr;
     bytes = 0;
-    cudaError_t e = cudaMalloc(&p, need);
+    const cudaError_t e = static_cast<cudaError_t>(scarf::device_alloc(&p, need));
     if (e == cudaSuccess) bytes = need;
     return e;
   }
   void release() {
-    if (p) cudaFree(p);
+    scarf::device_free(p, bytes);
     p = nullptr;
     bytes = 0;
   }
@@ -274,6 +288,7 @@ int execute_impl(int seed, float* field, float stats[8], int flags) {
   if (!field || !stats) return fail(SCARF_ERR_ARG, "field and stats must not be NULL");
   int rc = ensure_resources();
   if (rc) return rc;
+  scarf::take_device_alloc_failure();
   cudaStream_t st = g_cfg.stream;
   for (int i = 0; i < 8; ++i) stats[i] = 0.0f;
 
@@ -289,7 +304,7 @@ int execute_impl(int seed, float* field, float stats[8], int flags) {
   const bool on_gpu = !g_cfg.src.srng && g_cfg.sampler != SCARF_SAMPLER_HOST;
   const int nh = on_gpu ? srm_sample_device(p, s, table.data(), &pairs, st, nullptr)
                         : srm_sample(p, s, &g_cfg.src, threads, table.data(), &pairs);
-  if (nh == -2) return fail(SCARF_ERR_CUDA, "device sampler: CUDA error");
+  if (nh == -2) return sampler_fail("device sampler");
   if (nh < 0)
     return fail(SCARF_ERR_ARG,
                 "rejection sampling infeasible: acceptance rate %.3g < %.1g (domain too small for the correlation "
@@ -732,12 +747,13 @@ int scarf_set_sampler_pass_pairs(long long pairs) {
 int scarf_srm_sample_device(const scarf_srm_params* p, const scarf_srm_setup* s, float* table, int* n_kept,
                             long long* pairs_used, long long* host_decided, void* stream) {
   if (!p || !s || !table) return fail(SCARF_ERR_ARG, "NULL argument");
+  scarf::take_device_alloc_failure();
   long long used = 0, open = 0;
   const int kept = srm_sample_device(*p, *s, table, &used, stream, &open);
   if (kept == -1)
     return fail(SCARF_ERR_ARG, "rejection sampling infeasible: acceptance rate %.3g < %.1g", acceptance_rate(*s),
                 kMinAcceptance);
-  if (kept < 0) return fail(SCARF_ERR_CUDA, "device sampler: CUDA error");
+  if (kept < 0) return sampler_fail("device sampler");
   if (n_kept) *n_kept = kept;
   if (pairs_used) *pairs_used = used;
   if (host_decided) *host_decided = open;
@@ -751,9 +767,10 @@ int scarf_srm_sample_device_batch(int nfields, const scarf_srm_params* p, const 
     return fail(SCARF_ERR_ARG, "invalid argument");
   for (int f = 0; f < nfields; ++f)
     if (!tables[f]) return fail(SCARF_ERR_ARG, "tables[%d] is NULL", f);
+  scarf::take_device_alloc_failure();
   long long open = 0;
   const int rc = srm_sample_device_batch(nfields, p, s, tables, n_kept, pairs_used, stream, &open);
-  if (rc <= -2 - nfields) return fail(SCARF_ERR_CUDA, "batched device sampler: CUDA error");
+  if (rc <= -2 - nfields) return sampler_fail("batched device sampler");
   if (rc < 0) {
     const int f = -1 - rc;
     return fail(SCARF_ERR_ARG, "field %d: rejection sampling infeasible: acceptance rate %.3g < %.1g", f,
@@ -1044,6 +1061,48 @@ int scarf_set_kernel_timing(int enable) {
   return SCARF_OK;
 }
 
+int scarf_set_device_memory_cap(size_t bytes) {
+  scarf::set_device_memory_cap(bytes);
+  return SCARF_OK;
+}
+
+size_t scarf_device_memory_in_use(void) { return scarf::device_memory_in_use(); }
+
+int scarf_release_device_memory(void) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (g_res.device >= 0) {
+    int dev = 0;
+    SCARF_CUDA(cudaGetDevice(&dev));
+    SCARF_CUDA(cudaSetDevice(g_res.device));
+    SCARF_CUDA(cudaDeviceSynchronize());
+    g_res.release();
+    SCARF_CUDA(cudaSetDevice(dev));
+  }
+  scarf::release_sampler_device_memory();
+  return SCARF_OK;
+}
+
+int scarf_selftest_wait_limit(int blocks, int* device_status, double* waited_s) {
+  if (blocks < 1 || blocks > 1024) return fail(SCARF_ERR_ARG, "blocks must be in 1..1024 (got %d)", blocks);
+  void* d = nullptr;
+  const cudaError_t ea = static_cast<cudaError_t>(scarf::device_alloc(&d, 16));
+  if (ea != cudaSuccess) return cuda_fail(ea, "self-test scratch");
+  struct Scratch {
+    void* p;
+    ~Scratch() { scarf::device_free(p, 16); }
+  } scratch{d};
+  int status = -1;
+  unsigned long long waited = 0;
+  bool timed_out = false;
+  SCARF_CUDA(scarf::run_wait_limit_probe(blocks, d, g_cfg.stream, &status, &waited, &timed_out));
+  if (device_status) *device_status = status;
+  if (waited_s) *waited_s = static_cast<double>(waited) * 1e-9;
+  if (!timed_out)
+    return fail(SCARF_ERR_DEVICE, "bounded-wait self-test: status word %d after the waits, not the timeout code",
+                status);
+  return SCARF_OK;
+}
+
 float scarf_last_kernel_ms(void) { return g_last_kernel_ms; }
 
 int scarf_set_tc_chunk(int harmonics) {
@@ -1240,12 +1299,13 @@ int scarf_srm_tc_autotune(const scarf_srm_setup* s, const int fs[3], const int n
   float* d_field = nullptr;
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   auto release = [&]() {
-    if (d_work) cudaFree(d_work);
-    if (d_field) cudaFree(d_field);
+    scarf::device_free(d_work, work);
+    scarf::device_free(d_field, sizeof(float) * npts);
     if (e0) cudaEventDestroy(e0);
     if (e1) cudaEventDestroy(e1);
   };
-  if (cudaMalloc(&d_work, work) != cudaSuccess || cudaMalloc(&d_field, sizeof(float) * npts) != cudaSuccess ||
+  if (scarf::device_alloc(&d_work, work) != cudaSuccess ||
+      scarf::device_alloc(reinterpret_cast<void**>(&d_field), sizeof(float) * npts) != cudaSuccess ||
       cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
     cudaGetLastError();
     release();
@@ -1310,7 +1370,7 @@ int scarf_srm_tc_batch_autotune(const scarf_tc_field* fields, int nfields, void*
       TcBatchPlan bp;
       if (!tc_batch_plan(in.data(), nfields, &bp)) continue;
       void* d_work = nullptr;
-      if (cudaMalloc(&d_work, bp.bytes) != cudaSuccess) {
+      if (scarf::device_alloc(&d_work, bp.bytes) != cudaSuccess) {
         cudaGetLastError();
         continue;
       }
@@ -1331,7 +1391,7 @@ int scarf_srm_tc_batch_autotune(const scarf_tc_field* fields, int nfields, void*
         }
       }
       cudaGetLastError();
-      cudaFree(d_work);
+      scarf::device_free(d_work, bp.bytes);
       if (ms > 0.0f && (best.variant < 0 || ms < best.ms)) best = scarf::TcChoice{v, tj, 1, ms};
       if (ms > 0.0f && v == SCARF_TC_SINGLE && tj == auto_tj) deflt = scarf::TcChoice{v, tj, 1, ms};
     }

@@ -487,6 +487,50 @@ double acceptance_rate(const scarf_srm_setup& s) {
   return static_cast<double>(s.intg_band) * s.cnst / width;
 }
 
+// ------------------------------------------------ device memory accounting --
+namespace {
+std::atomic<size_t> g_dev_in_use{0};
+std::atomic<size_t> g_dev_cap{0};  // 0: no cap
+thread_local bool t_alloc_failed = false;
+}  // namespace
+
+int device_alloc(void** p, size_t bytes) {
+  *p = nullptr;
+  const size_t cap = g_dev_cap.load();
+  size_t used = g_dev_in_use.load();
+  do {
+    if (cap && bytes > cap - std::min(cap, used)) {
+      t_alloc_failed = true;
+      return cudaErrorMemoryAllocation;
+    }
+  } while (!g_dev_in_use.compare_exchange_weak(used, used + bytes));
+  const cudaError_t e = cudaMalloc(p, bytes);
+  if (e != cudaSuccess) {
+    g_dev_in_use -= bytes;
+    *p = nullptr;
+    if (e == cudaErrorMemoryAllocation) {
+      t_alloc_failed = true;
+      cudaGetLastError();
+    }
+  }
+  return e;
+}
+
+bool take_device_alloc_failure() {
+  const bool f = t_alloc_failed;
+  t_alloc_failed = false;
+  return f;
+}
+
+void device_free(void* p, size_t bytes) {
+  if (!p) return;
+  cudaFree(p);
+  g_dev_in_use -= bytes;
+}
+
+void set_device_memory_cap(size_t bytes) { g_dev_cap = bytes; }
+size_t device_memory_in_use() { return g_dev_in_use.load(); }
+
 // ------------------------------------------------- device-assisted sampler --
 namespace {
 
@@ -495,12 +539,17 @@ struct DevBuf {
   size_t bytes = 0;
   cudaError_t ensure(size_t need) {
     if (need <= bytes) return cudaSuccess;
-    if (p) cudaFree(p);
+    device_free(p, bytes);
     p = nullptr;
     bytes = 0;
-    const cudaError_t e = cudaMalloc(&p, need);
+    const cudaError_t e = static_cast<cudaError_t>(device_alloc(&p, need));
     if (e == cudaSuccess) bytes = need;
     return e;
+  }
+  void release() {
+    device_free(p, bytes);
+    p = nullptr;
+    bytes = 0;
   }
 };
 
@@ -556,11 +605,24 @@ long long first_pass_pairs(const scarf_srm_params& p, double acc) {
   return capped_pairs(static_cast<long long>(p.nharm * (1.0 / acc + 3.0) * 1.1) + 4096);
 }
 
+}  // namespace
+
+void release_sampler_device_memory() {
+  std::lock_guard<std::mutex> lk(g_dev_sampler_mu);
+  DeviceSamplerState& D = g_dev_sampler;
+  for (DevBuf* b : {&D.counts, &D.offsets, &D.entries, &D.slots, &D.batch_args, &D.batch_tbeg}) b->release();
+}
+
+namespace {
+
 // Uploads the pow tables once per device (caller holds g_dev_sampler_mu).
 bool ensure_sampler_device(DeviceSamplerState& D) {
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) return false;
   if (D.device != dev) {
+    // the previous device's buffers (freed through unified addressing)
+    for (DevBuf* b : {&D.counts, &D.offsets, &D.entries, &D.slots, &D.batch_args, &D.batch_tbeg}) b->release();
+    if (D.host_entries) cudaFreeHost(D.host_entries);
     D = DeviceSamplerState();
     D.device = dev;
   }

@@ -92,6 +92,21 @@ void set_device_sampler_pass_cap(long long pairs);
 
 int host_threads();
 
+// Device allocations of the library's own buffers (tables, staging fields,
+// scratch), counted over all devices against the cap that
+// scarf_set_device_memory_cap sets (0: none). device_alloc returns a
+// cudaError_t value: cudaErrorMemoryAllocation when the request would pass
+// the cap, without calling the driver.
+int device_alloc(void** p, size_t bytes);
+void device_free(void* p, size_t bytes);
+void set_device_memory_cap(size_t bytes);
+size_t device_memory_in_use();
+// Whether a device_alloc on the calling thread ran out of memory (or into
+// the cap) since the last call; clears the flag.
+bool take_device_alloc_failure();
+// Frees the device sampler's scratch buffers (they grow again on demand).
+void release_sampler_device_memory();
+
 // Runs fn(0) .. fn(ntasks - 1) on at most `width` host threads (the caller's
 // included) from a persistent worker pool; returns when all have returned.
 void parallel_tasks(int ntasks, int width, const std::function<void(int)>& fn);

@@ -149,6 +149,13 @@ struct SamplerArgs {
 // Output-transform tables of the generator: g^k (k < 2048), g^(k 2^11)
 // (k < 2048) and g^(k 2^22) (k < 512) mod 2^31 - 1, 4 608 words in that order.
 cudaError_t sampler_upload_tables(const unsigned int* pow3);
+
+// Bounded-wait self-test (srm_selftest.cu): `blocks` blocks wait on an
+// mbarrier that nothing arrives on; d_scratch is 16 device bytes. On return
+// *status is the status word the waits wrote, *waited_ns the longest wait,
+// and *timed_out whether a wait ran out and said so.
+cudaError_t run_wait_limit_probe(int blocks, void* d_scratch, cudaStream_t stream, int* status,
+                                 unsigned long long* waited_ns, bool* timed_out);
 cudaError_t launch_sampler(const SamplerArgs& args, cudaStream_t stream);
 // One pass for each of nfields fields in a single launch: d_fields[f] holds
 // field f's pass (its counts / offsets pointers already at the field's slice),

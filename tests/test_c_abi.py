@@ -155,3 +155,14 @@ def test_package_refuses_to_load_without_its_library():
     r = subprocess.run([sys.executable, "-c", "import scarf3d_b200"], cwd=str(ROOT), env=env, capture_output=True,
                        text=True)
     assert r.returncode != 0 and "no CPU fallback" in r.stderr
+
+
+def test_device_memory_cap_and_selftest_arguments_without_a_gpu():
+    assert sb.device_memory_in_use() == 0
+    sb.set_device_memory_cap(1 << 20)
+    sb.set_device_memory_cap(0)
+    st = ctypes.c_int(-1)
+    waited = ctypes.c_double(-1.0)
+    assert sb.lib.scarf_selftest_wait_limit(0, ctypes.byref(st), ctypes.byref(waited)) == sb.SCARF_ERR_ARG
+    assert sb.lib.scarf_selftest_wait_limit(2000, None, None) == sb.SCARF_ERR_ARG
+    assert "blocks" in sb.last_error()
