@@ -15,8 +15,7 @@ namespace scarf {
 // Device-side status codes written into the caller-visible status word.
 enum DevStatus : int {
   kDevOk = 0,
-  kDevTimeout = 1,     // a bounded wait ran out (pipeline stalled)
-  kDevBadShape = 2,    // launch received an inconsistent shape
+  kDevTimeout = 1,  // a bounded wait ran out (pipeline stalled)
 };
 
 // Upper bound for any single wait inside a kernel, in nanoseconds of
