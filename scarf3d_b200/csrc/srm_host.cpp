@@ -12,6 +12,7 @@
 #include <condition_variable>
 #include <cstdlib>
 #include <cstring>
+#include <exception>
 #include <functional>
 #include <memory>
 #include <mutex>
@@ -221,8 +222,9 @@ namespace {
 class HostPool {
  public:
   // Runs fn(0) .. fn(ntasks - 1) on at most `width` threads (the caller's
-  // included) and returns when all have returned. Jobs from several caller
-  // threads run one after another; fn must not start another job.
+  // included) and returns when all have returned; the first exception a task
+  // threw is rethrown then. Jobs from several caller threads run one after
+  // another; fn must not start another job.
   void run(int ntasks, int width, const std::function<void(int)>& fn) {
     if (ntasks <= 0) return;
     width = std::min(width, ntasks);
@@ -246,6 +248,7 @@ class HostPool {
     std::unique_lock<std::mutex> lk(mu_);
     done_cv_.wait(lk, [&] { return job->done.load() == job->ntasks; });
     job_.reset();
+    if (job->error) std::rethrow_exception(job->error);
   }
 
  private:
@@ -253,11 +256,18 @@ class HostPool {
     const std::function<void(int)>* fn = nullptr;
     int ntasks = 0;
     std::atomic<int> slots{0}, next{0}, done{0};
+    std::mutex error_mu;
+    std::exception_ptr error;  // the first exception a task threw
   };
 
   void work(Job& j) {
     for (int i = j.next.fetch_add(1); i < j.ntasks; i = j.next.fetch_add(1)) {
-      (*j.fn)(i);
+      try {
+        (*j.fn)(i);
+      } catch (...) {
+        std::lock_guard<std::mutex> lk(j.error_mu);
+        if (!j.error) j.error = std::current_exception();
+      }
       if (j.done.fetch_add(1) + 1 == j.ntasks) {
         std::lock_guard<std::mutex> lk(mu_);
         done_cv_.notify_all();

@@ -7,6 +7,7 @@
 #include <atomic>
 #include <cstdio>
 #include <cstring>
+#include <stdexcept>
 #include <thread>
 #include <vector>
 
@@ -116,6 +117,24 @@ int main() {
     for (int n : {0, 1, 3, 64, 1000})
       for (int i = 0; i < n; ++i) want1 += 1 + i, want2 += 2 + i;
   expect(s1 == want1 && s2 == want2, "worker pool ran a task other than once", -1);
+
+  // A task that throws: every other task still runs, and the caller gets the
+  // exception once all have returned.
+  {
+    std::vector<int> hit(200, 0);
+    bool caught = false;
+    try {
+      scarf::parallel_tasks(200, 6, [&](int i) {
+        hit[i] = 1;
+        if (i == 17) throw std::runtime_error("task 17");
+      });
+    } catch (const std::runtime_error& e) {
+      caught = std::strcmp(e.what(), "task 17") == 0;
+    }
+    int ran = 0;
+    for (int h : hit) ran += h;
+    expect(caught && ran == 200, "a throwing task lost other tasks or its exception", -1);
+  }
 
   std::printf("%d cases, %d failures\n", c, failures);
   return failures ? 1 : 0;
