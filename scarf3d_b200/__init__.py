@@ -356,15 +356,28 @@ def sample_device(p: SrmParams, s: SrmSetup, stream_handle: int | None = None):
     return tab[: kept.value].copy(), used.value, open_.value
 
 
-def sample_device_batch(params, setups, stream_handle: int | None = None):
+def sample_device_batch(params, setups, stream_handle: int | None = None, out=None):
     """Device-assisted sampler for many fields in one pass of launches:
-    (list of tables, list of pairs used, pairs decided on the host)."""
+    (list of tables, list of pairs used, pairs decided on the host). Each
+    table is a view of its kept rows. `out` optionally gives the arrays to
+    write into, one per field: float32, C-contiguous, at least nharm x 5
+    (for example views of one page-locked buffer, ready for one upload)."""
     n = len(params)
     if len(setups) != n:
         raise ValueError("params and setups differ in length")
     p_arr = (SrmParams * n)(*params)
     s_arr = (SrmSetup * n)(*setups)
-    tabs = [np.zeros((max(p.nharm, 1), 5), np.float32) for p in params]
+    if out is None:
+        tabs = [np.empty((max(p.nharm, 1), 5), np.float32) for p in params]
+    else:
+        if len(out) != n:
+            raise ValueError("out must hold one array per field")
+        tabs = []
+        for p, t in zip(params, out):
+            t = np.asarray(t)
+            if t.dtype != np.float32 or not t.flags.c_contiguous or t.size < 5 * max(p.nharm, 1):
+                raise ValueError("each out array must be C-contiguous float32 with room for nharm x 5 values")
+            tabs.append(t.reshape(-1)[: 5 * max(p.nharm, 1)].reshape(-1, 5))
     ptrs = (ctypes.c_void_p * n)(*[t.ctypes.data for t in tabs])
     kept = (ctypes.c_int * n)()
     used = (ctypes.c_longlong * n)()
@@ -373,7 +386,7 @@ def sample_device_batch(params, setups, stream_handle: int | None = None):
                                             ctypes.cast(ptrs, ctypes.c_void_p), kept,
                                             ctypes.cast(used, ctypes.c_void_p), ctypes.byref(open_),
                                             ctypes.c_void_p(stream_handle or 0)))
-    return [t[: kept[i]].copy() for i, t in enumerate(tabs)], list(used), open_.value
+    return [t[: kept[i]] for i, t in enumerate(tabs)], list(used), open_.value
 
 
 def set_sampler(where: int):

@@ -166,3 +166,14 @@ def test_device_memory_cap_and_selftest_arguments_without_a_gpu():
     assert sb.lib.scarf_selftest_wait_limit(0, ctypes.byref(st), ctypes.byref(waited)) == sb.SCARF_ERR_ARG
     assert sb.lib.scarf_selftest_wait_limit(2000, None, None) == sb.SCARF_ERR_ARG
     assert "blocks" in sb.last_error()
+
+
+def test_batch_sampler_output_arrays_are_validated():
+    ps = [sb.make_params(nc=[0.0] * 3, fc=[1000.0] * 3, nharm=n, acf=0, seed=1, hurst=0.3, sigma=0.05, ds=50.0,
+                         cl=[500.0] * 3) for n in (7, 13)]
+    ss = [sb.SrmSetup(), sb.SrmSetup()]
+    for bad in ([np.zeros(35, np.float64), np.zeros(65, np.float32)],  # wrong type
+                [np.zeros(30, np.float32), np.zeros(65, np.float32)],  # too small
+                [np.zeros(35, np.float32)]):                           # one array short
+        with pytest.raises(ValueError):
+            sb.sample_device_batch(ps, ss, out=bad)

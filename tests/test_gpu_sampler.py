@@ -116,6 +116,23 @@ def test_batched_device_sampler_matches_per_field_sampler():
         assert np.array_equal(t.view(np.uint32), ref.view(np.uint32))
 
 
+def test_batched_device_sampler_writes_into_caller_arrays():
+    # Tables written in place into views of one buffer equal those of
+    # library-allocated arrays; the views keep the rows beyond `kept` untouched.
+    fields = _batch_fields()
+    ps, ss = [f[0] for f in fields], [f[1] for f in fields]
+    ref, ref_used, _ = sb.sample_device_batch(ps, ss)
+    offs = np.concatenate([[0], np.cumsum([5 * p.nharm + 20 for p in ps])])
+    buf = np.full(int(offs[-1]), -7.0, np.float32)
+    views = [buf[offs[i]:offs[i + 1]] for i in range(len(ps))]
+    got, used, _ = sb.sample_device_batch(ps, ss, out=views)
+    assert list(used) == list(ref_used)
+    for i, (g, r) in enumerate(zip(got, ref)):
+        assert np.array_equal(g.view(np.uint32), r.view(np.uint32))
+        assert np.shares_memory(g, buf)
+        assert np.all(buf[offs[i] + 5 * ps[i].nharm:offs[i + 1]] == -7.0)
+
+
 def test_batched_device_sampler_redoes_fields_whose_slots_overflowed(monkeypatch):
     # One candidate slot per scan thread: most threads overflow, their fields
     # are redone with their own passes, and the tables must not change.
