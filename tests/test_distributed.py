@@ -90,3 +90,36 @@ def test_two_rank_slabs_reproduce_single_rank_field_and_stats():
     assert np.array_equal(whole, full)  # decomposition invariance, bit for bit
     assert abs(gv / oracle.variance(full) - 1) < 1e-5
     assert abs(gm - oracle.mean(full)) <= 1e-6 * np.sqrt(gv)
+
+
+def _leaving_worker(rank, world, port, out):
+    # Rank 1 leaves between steps (after the group is up, before the merge);
+    # rank 0 must get an error from its next collective, not wait for good.
+    import datetime
+    import time
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=5))
+    if rank == 1:
+        os._exit(0)
+    t0 = time.monotonic()
+    try:
+        merge_stats_across_ranks(1.0, 0.0, 10)
+        out.put(("merged", time.monotonic() - t0))
+    except Exception as e:  # noqa: BLE001 - any error is the expected outcome
+        out.put(("error", time.monotonic() - t0, type(e).__name__))
+    os._exit(0)
+
+
+def test_a_rank_that_leaves_makes_the_merge_fail_instead_of_hang():
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_leaving_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = q.get(timeout=120)
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    assert res[0] == "error", res
+    assert res[1] < 60.0  # bounded by the process group's timeout
