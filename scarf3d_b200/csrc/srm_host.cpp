@@ -569,10 +569,15 @@ struct DeviceSamplerState {
   DevBuf counts, offsets, entries, slots, batch_args, batch_tbeg;
   SampleEntry* host_entries = nullptr;  // page-locked staging of candidate entries
   long long host_entries_cap = 0;
+  cudaStream_t side = nullptr;        // gathers and copies beside the scans
+  std::vector<cudaEvent_t> events;    // end of each group's scan
 };
 DeviceSamplerState g_dev_sampler;
 std::mutex g_dev_sampler_mu;
 long long g_pass_pairs_cap = 0;  // 0: size passes from the acceptance rate
+// Scan launches of a batch: the host's walks and table rows of one group run
+// while the following groups scan.
+constexpr int kSamplerGroups = 8;
 
 // Host decision for a pair the device left open (glibc spectrum).
 bool host_accept(const scarf_srm_setup& s, int acf, float r1, float r2) {
@@ -825,54 +830,56 @@ int srm_sample_device_batch(int nfields, const scarf_srm_params* p, const scarf_
     args[f].out = nullptr;
     args[f].keys = d_slots + sbeg[f];
   }
+  // Groups of consecutive fields, balanced by their first-pass pairs. Each
+  // group's scan is its own launch on `stream`; while later groups scan, the
+  // host copies the finished group's counts, gathers its candidates on the
+  // side stream, walks its fields and fills their table rows, so the host
+  // work of all but the last group runs under the scans. tbeg_rel holds the
+  // thread offsets relative to each group's first thread, group after group
+  // (group g's fields [gbeg[g], gbeg[g+1]) at entries gbeg[g] + g ...).
+  const int G = std::max(1, std::min(nfields, kSamplerGroups));
+  std::vector<int> gbeg(G + 1, nfields);
+  gbeg[0] = 0;
+  {
+    double all = 0.0, run = 0.0;
+    for (int f = 0; f < nfields; ++f) all += static_cast<double>(args[f].q_count);
+    int g = 1;
+    for (int f = 0; f < nfields && g < G; ++f) {
+      run += static_cast<double>(args[f].q_count);
+      if (run >= all * g / G) gbeg[g++] = f + 1;
+    }
+  }
+  std::vector<long long> tbeg_rel(nfields + G, 0);
+  for (int g = 0; g < G; ++g)
+    for (int f = gbeg[g]; f <= gbeg[g + 1]; ++f) tbeg_rel[f + g] = tbeg[f] - tbeg[gbeg[g]];
+  if (D.batch_tbeg.ensure(sizeof(long long) * (nfields + G)) != cudaSuccess) return err;
+  if (!D.side && cudaStreamCreateWithFlags(&D.side, cudaStreamNonBlocking) != cudaSuccess) {
+    D.side = nullptr;
+    return err;
+  }
+  while (static_cast<int>(D.events.size()) < G) {
+    cudaEvent_t e = nullptr;
+    if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) return err;
+    D.events.push_back(e);
+  }
   if (cudaMemcpyAsync(D.batch_args.p, args.data(), sizeof(SamplerArgs) * nfields, cudaMemcpyHostToDevice, stream) !=
           cudaSuccess ||
-      cudaMemcpyAsync(D.batch_tbeg.p, tbeg.data(), sizeof(long long) * (nfields + 1), cudaMemcpyHostToDevice,
+      cudaMemcpyAsync(D.batch_tbeg.p, tbeg_rel.data(), sizeof(long long) * (nfields + G), cudaMemcpyHostToDevice,
                       stream) != cudaSuccess)
     return err;
   const SamplerArgs* d_args = static_cast<const SamplerArgs*>(D.batch_args.p);
   const long long* d_tbeg = static_cast<const long long*>(D.batch_tbeg.p);
-  if (launch_sampler_batch(d_args, d_tbeg, nfields, T, 2, stream) != cudaSuccess) return err;
-  std::vector<int> counts(T);
-  if (cudaMemcpyAsync(counts.data(), d_counts, sizeof(int) * T, cudaMemcpyDeviceToHost, stream) != cudaSuccess ||
-      cudaStreamSynchronize(stream) != cudaSuccess)
-    return err;
-  std::vector<long long> offsets(T);
-  std::vector<long long> ebeg(nfields + 1, 0);  // entry range of each field
-  std::vector<char> overflow(nfields, 0);       // a slot overflowed: the field is redone alone
-  long long total = 0;
-  for (int f = 0; f < nfields; ++f) {
-    for (long long t = tbeg[f]; t < tbeg[f + 1]; ++t) {
-      offsets[t] = total;
-      if (counts[t] > args[f].cap) overflow[f] = 1;
-      total += std::min(counts[t], args[f].cap);
-    }
-    ebeg[f + 1] = total;
-  }
-  if (total > 0) {
-    if (D.entries.ensure(sizeof(SampleEntry) * total) != cudaSuccess) return err;
-    if (D.host_entries_cap < total) {
-      if (D.host_entries) cudaFreeHost(D.host_entries);
-      D.host_entries = nullptr;
-      D.host_entries_cap = 0;
-      void* h = nullptr;
-      if (cudaHostAlloc(&h, sizeof(SampleEntry) * total, cudaHostAllocDefault) != cudaSuccess) return err;
-      D.host_entries = static_cast<SampleEntry*>(h);
-      D.host_entries_cap = total;
-    }
-    if (cudaMemcpyAsync(d_offsets, offsets.data(), sizeof(long long) * T, cudaMemcpyHostToDevice, stream) !=
-            cudaSuccess ||
-        launch_sampler_gather(d_args, d_tbeg, nfields, T, d_offsets, static_cast<SampleEntry*>(D.entries.p),
-                              stream) != cudaSuccess ||
-        cudaMemcpyAsync(D.host_entries, D.entries.p, sizeof(SampleEntry) * total, cudaMemcpyDeviceToHost, stream) !=
-            cudaSuccess ||
-        cudaStreamSynchronize(stream) != cudaSuccess)
+  for (int g = 0; g < G; ++g) {
+    const int f0 = gbeg[g], f1 = gbeg[g + 1];
+    if (f1 > f0 &&
+        launch_sampler_batch(d_args + f0, d_tbeg + f0 + g, f1 - f0, tbeg[f1] - tbeg[f0], 2, stream) != cudaSuccess)
       return err;
+    if (cudaEventRecord(D.events[g], stream) != cudaSuccess) return err;
   }
-  const SampleEntry* entries = D.host_entries;
-  // Host walks over the first passes, fields spread over host threads (each
-  // walk is independent); a field whose first pass ran short then continues
-  // with its own device passes, one field at a time.
+
+  std::vector<int> counts(T);
+  std::vector<long long> offsets(T);        // relative to the group's first entry
+  std::vector<char> overflow(nfields, 0);   // a slot overflowed: the field is redone alone
   std::vector<DeviceWalk> walks(nfields);
   std::vector<char> done(nfields, 0);
   for (int f = 0; f < nfields; ++f) {
@@ -882,13 +889,90 @@ int srm_sample_device_batch(int nfields, const scarf_srm_params* p, const scarf_
     w.table = tables[f];
     w.acc = acc[f];
     w.pass_end = args[f].q_count;
-    // an overflowed field starts over with its own passes (empty first pass)
-    w.ent = overflow[f] ? nullptr : entries + ebeg[f];
-    w.nent = overflow[f] ? 0 : static_cast<size_t>(ebeg[f + 1] - ebeg[f]);
-    if (overflow[f]) w.pass_end = 0;
   }
-  parallel_tasks(nfields, host_threads(), [&](int f) { done[f] = walks[f].walk() ? 1 : 0; });
+  // Table rows from the kept draws (libm trig per row), spread over host
+  // threads in blocks of rows; each row depends on its own draw only.
+  auto fill_rows = [&](const std::vector<int>& fields) {
+    std::vector<long long> rbeg(fields.size() + 1, 0);
+    for (size_t i = 0; i < fields.size(); ++i) rbeg[i + 1] = rbeg[i] + walks[fields[i]].kept;
+    constexpr long long kRowBlock = 512;
+    const long long nblocks = (rbeg.back() + kRowBlock - 1) / kRowBlock;
+    parallel_tasks(static_cast<int>(nblocks), host_threads(), [&](int b) {
+      const long long r0 = b * kRowBlock, r1 = std::min(rbeg.back(), r0 + kRowBlock);
+      size_t i = static_cast<size_t>(std::upper_bound(rbeg.begin(), rbeg.end(), r0) - rbeg.begin()) - 1;
+      for (long long r = r0; r < r1; ++r) {
+        while (r >= rbeg[i + 1]) ++i;
+        const int f = fields[i];
+        const long long k = r - rbeg[i];
+        harmonic_row(walks[f].draws[k], s[f].ndim, p[f].cl, tables[f] + 5 * k);
+      }
+    });
+  };
+  for (int g = 0; g < G; ++g) {
+    const int f0 = gbeg[g], f1 = gbeg[g + 1];
+    if (f1 == f0) continue;
+    const long long t0 = tbeg[f0], Tg = tbeg[f1] - t0;
+    if (cudaStreamWaitEvent(D.side, D.events[g], 0) != cudaSuccess ||
+        cudaMemcpyAsync(counts.data() + t0, d_counts + t0, sizeof(int) * Tg, cudaMemcpyDeviceToHost, D.side) !=
+            cudaSuccess ||
+        cudaStreamSynchronize(D.side) != cudaSuccess)
+      return err;
+    std::vector<long long> ebeg(f1 - f0 + 1, 0);  // entry range of each field of the group
+    long long total = 0;
+    for (int f = f0; f < f1; ++f) {
+      for (long long t = tbeg[f]; t < tbeg[f + 1]; ++t) {
+        offsets[t] = total;
+        if (counts[t] > args[f].cap) overflow[f] = 1;
+        total += std::min(counts[t], args[f].cap);
+      }
+      ebeg[f - f0 + 1] = total;
+    }
+    if (total > 0) {
+      // The previous group's gather and copy have finished (side stream
+      // synchronised) and its walks are done, so both buffers may be reused.
+      if (D.entries.ensure(sizeof(SampleEntry) * total) != cudaSuccess) return err;
+      if (D.host_entries_cap < total) {
+        if (D.host_entries) cudaFreeHost(D.host_entries);
+        D.host_entries = nullptr;
+        D.host_entries_cap = 0;
+        void* h = nullptr;
+        if (cudaHostAlloc(&h, sizeof(SampleEntry) * total, cudaHostAllocDefault) != cudaSuccess) return err;
+        D.host_entries = static_cast<SampleEntry*>(h);
+        D.host_entries_cap = total;
+      }
+      if (cudaMemcpyAsync(d_offsets + t0, offsets.data() + t0, sizeof(long long) * Tg, cudaMemcpyHostToDevice,
+                          D.side) != cudaSuccess ||
+          launch_sampler_gather(d_args + f0, d_tbeg + f0 + g, f1 - f0, Tg, d_offsets + t0,
+                                static_cast<SampleEntry*>(D.entries.p), D.side) != cudaSuccess ||
+          cudaMemcpyAsync(D.host_entries, D.entries.p, sizeof(SampleEntry) * total, cudaMemcpyDeviceToHost,
+                          D.side) != cudaSuccess ||
+          cudaStreamSynchronize(D.side) != cudaSuccess)
+        return err;
+    }
+    // Walks over the group's first passes, fields spread over host threads
+    // (each walk is independent). An overflowed field starts over later with
+    // its own passes (empty first pass).
+    for (int f = f0; f < f1; ++f) {
+      DeviceWalk& w = walks[f];
+      w.ent = overflow[f] ? nullptr : D.host_entries + ebeg[f - f0];
+      w.nent = overflow[f] ? 0 : static_cast<size_t>(ebeg[f - f0 + 1] - ebeg[f - f0]);
+      if (overflow[f]) w.pass_end = 0;
+    }
+    parallel_tasks(f1 - f0, host_threads(), [&](int i) { done[f0 + i] = walks[f0 + i].walk() ? 1 : 0; });
+    std::vector<int> finished;
+    for (int f = f0; f < f1; ++f) {
+      // the staging buffer belongs to the next group now
+      walks[f].ent = nullptr;
+      walks[f].nent = 0;
+      walks[f].ei = 0;
+      if (done[f]) finished.push_back(f);
+    }
+    fill_rows(finished);
+  }
+  // Fields whose first pass ran short (or overflowed) continue with their own
+  // device passes, one field at a time, once every group's scan is done.
   long long open_total = 0;
+  std::vector<int> rest;
   for (int f = 0; f < nfields; ++f) {
     DeviceWalk& w = walks[f];
     if (!done[f]) {
@@ -897,26 +981,13 @@ int srm_sample_device_batch(int nfields, const scarf_srm_params* p, const scarf_
       A.offsets = nullptr;
       A.out = nullptr;
       if (!w.finish(D, A, stream)) return err;
+      rest.push_back(f);
     }
     if (kept) kept[f] = w.kept;
     if (pairs_used) pairs_used[f] = w.pos;
     open_total += w.open;
   }
-  // Table rows from the kept draws (libm trig per row), spread over host
-  // threads in blocks of rows; each row depends on its own draw only.
-  std::vector<long long> rbeg(nfields + 1, 0);
-  for (int f = 0; f < nfields; ++f) rbeg[f + 1] = rbeg[f] + walks[f].kept;
-  constexpr long long kRowBlock = 512;
-  const long long nblocks = (rbeg[nfields] + kRowBlock - 1) / kRowBlock;
-  parallel_tasks(static_cast<int>(nblocks), host_threads(), [&](int b) {
-    const long long r0 = b * kRowBlock, r1 = std::min(rbeg[nfields], r0 + kRowBlock);
-    int f = static_cast<int>(std::upper_bound(rbeg.begin(), rbeg.end(), r0) - rbeg.begin()) - 1;
-    for (long long r = r0; r < r1; ++r) {
-      while (r >= rbeg[f + 1]) ++f;
-      const long long i = r - rbeg[f];
-      harmonic_row(walks[f].draws[i], s[f].ndim, p[f].cl, tables[f] + 5 * i);
-    }
-  });
+  fill_rows(rest);
   if (uncertain) *uncertain = open_total;
   return 0;
 }
