@@ -107,3 +107,30 @@ def test_infeasible_rejection_sampling_is_refused():
     rc = sb.lib.scarf_srm_sample(ctypes.byref(pp), ctypes.byref(s), tab.ctypes.data_as(ctypes.c_void_p), None, None)
     assert rc == sb.SCARF_ERR_ARG
     assert "acceptance rate" in sb.last_error()
+
+
+def test_threaded_sampler_after_fork():
+    # The threaded host sampler runs on a persistent worker pool; a child
+    # made by fork() has none of the parent's workers and must build its own
+    # (a pool inherited as is would wait for threads that do not exist).
+    import os
+    fc = [float(np.float32(127) * np.float32(50.0))] * 3
+    p = sb.make_params(nc=[0.0] * 3, fc=fc, nharm=2000, acf=0, seed=7, hurst=0.3, sigma=0.05, ds=50.0,
+                       cl=[2000.0] * 3)
+    s = sb.compute_setup(p)
+    sb.lib.scarf_set_host_threads(4)
+    try:
+        ref, _ = sb.sample(p, s)  # the parent's pool now has workers
+        pid = os.fork()
+        if pid == 0:  # child: same table, then leave without running pytest's teardown
+            try:
+                tab, _ = sb.sample(p, s)
+                os._exit(0 if np.array_equal(tab.view(np.uint32), ref.view(np.uint32)) else 3)
+            except BaseException:  # noqa: BLE001
+                os._exit(4)
+        _, status = os.waitpid(pid, 0)
+        assert os.waitstatus_to_exitcode(status) == 0
+        again, _ = sb.sample(p, s)  # and the parent's pool still works
+        assert np.array_equal(again.view(np.uint32), ref.view(np.uint32))
+    finally:
+        sb.lib.scarf_set_host_threads(0)
