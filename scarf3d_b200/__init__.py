@@ -375,8 +375,10 @@ def sample_device_batch(params, setups, stream_handle: int | None = None, out=No
         tabs = []
         for p, t in zip(params, out):
             t = np.asarray(t)
-            if t.dtype != np.float32 or not t.flags.c_contiguous or t.size < 5 * max(p.nharm, 1):
-                raise ValueError("each out array must be C-contiguous float32 with room for nharm x 5 values")
+            if (t.dtype != np.float32 or not t.flags.c_contiguous or not t.flags.writeable
+                    or t.size < 5 * max(p.nharm, 1)):
+                raise ValueError("each out array must be writeable, C-contiguous float32 with room for "
+                                 "nharm x 5 values")
             tabs.append(t.reshape(-1)[: 5 * max(p.nharm, 1)].reshape(-1, 5))
     ptrs = (ctypes.c_void_p * n)(*[t.ctypes.data for t in tabs])
     kept = (ctypes.c_int * n)()

@@ -172,8 +172,11 @@ def test_batch_sampler_output_arrays_are_validated():
     ps = [sb.make_params(nc=[0.0] * 3, fc=[1000.0] * 3, nharm=n, acf=0, seed=1, hurst=0.3, sigma=0.05, ds=50.0,
                          cl=[500.0] * 3) for n in (7, 13)]
     ss = [sb.SrmSetup(), sb.SrmSetup()]
+    ro = np.zeros(35, np.float32)
+    ro.flags.writeable = False
     for bad in ([np.zeros(35, np.float64), np.zeros(65, np.float32)],  # wrong type
                 [np.zeros(30, np.float32), np.zeros(65, np.float32)],  # too small
+                [ro, np.zeros(65, np.float32)],                        # read-only
                 [np.zeros(35, np.float32)]):                           # one array short
         with pytest.raises(ValueError):
             sb.sample_device_batch(ps, ss, out=bad)
