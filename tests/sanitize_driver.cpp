@@ -204,7 +204,7 @@ scarf_srm_params params_of(const Case& k, int seed_offset) {
 // host sampler: tables bit for bit, kept counts and pairs consumed equal.
 int check_device_batches(const char* what) {
   int batches = 0;
-  for (int nf : {1, 2, 3, 5, 9, 17}) {
+  for (int nf : {1, 2, 3, 5, 9, 17, 40}) {
     std::vector<scarf_srm_params> P;
     std::vector<scarf_srm_setup> S(nf);
     for (int f = 0; f < nf; ++f) {

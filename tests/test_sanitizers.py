@@ -38,4 +38,4 @@ def test_host_code_is_clean_under_asan_and_ubsan(driver):
                        env={"ASAN_OPTIONS": "detect_leaks=0", "UBSAN_OPTIONS": "print_stacktrace=1",
                             "PATH": "/usr/bin:/bin"})
     assert r.returncode == 0, r.stdout + r.stderr
-    assert "5 cases, 18 device-sampler batches, 0 failures" in r.stdout
+    assert "5 cases, 21 device-sampler batches, 0 failures" in r.stdout
