@@ -180,3 +180,21 @@ def test_batch_sampler_output_arrays_are_validated():
                 [np.zeros(35, np.float32)]):                           # one array short
         with pytest.raises(ValueError):
             sb.sample_device_batch(ps, ss, out=bad)
+
+
+def test_tensor_core_plan_and_workspace_without_a_gpu():
+    # 512^3 x 20 000 harmonics, default plan: one CTA, 16 x 8 row tiles, z the
+    # column axis in 256-wide tiles; 1 250 stages of 16 harmonics. The R, S
+    # and C images are 32 x 16 rows, 64 x 8 rows and 2 x 256 columns (hi and lo
+    # halves of 64-byte rows) per stage, 8 bytes per R/S entry: 81.92 MB each,
+    # plus 256 bytes of status and queue words.
+    assert sb.tc_plan_info(3, [512, 512, 512], 20000) == {"variant": sb.TC_SINGLE, "tile_j": 8, "permute": 0}
+    stages = 20000 // 16
+    image = stages * 16 * 512 * 8
+    assert sb.tc_workspace_bytes(3, [512, 512, 512], 20000) == 3 * image + 256
+    # one more stage adds one stage of each image
+    per_stage = 16 * 512 * 8 * 3
+    assert (sb.tc_workspace_bytes(3, [512, 512, 512], 20016) - sb.tc_workspace_bytes(3, [512, 512, 512], 20000)
+            == per_stage)
+    # 2-D grids keep one row of j per tile (tile_j 1)
+    assert sb.tc_plan_info(2, [300, 200, 1], 300)["tile_j"] == 1
