@@ -269,10 +269,13 @@ int scarf_srm_tc_batch_autotune(const scarf_tc_field *fields, int nfields, void 
  * per-step cudaMalloc/cudaFree synchronisation is unacceptable). No
  * counterpart in the reference. Scratch lives in a fixed device array of
  * scarf_srm_tc_noalloc_capacity_bytes() (64 MiB) that every GPU loading the
- * library holds until exit; larger grids/harmonic counts return
- * SCARF_ERR_ARG. The first call on a device looks up the array's device
- * address, so make it before any stream capture. All calls on a device share
- * the array: calls that overlap on the GPU race and must be serialised. */
+ * library holds until exit; a grid and harmonic count whose
+ * scarf_srm_tc_workspace_bytes() exceeds it returns SCARF_ERR_ARG. The plan
+ * is the one scarf_srm_tc_structured runs (tuned plans included). The first
+ * call in each device context looks up the array's device address. Every
+ * call reads its status word back and synchronises `stream`. All calls on a
+ * device share the array: calls that overlap on the GPU race and must be
+ * serialised. */
 size_t scarf_srm_tc_noalloc_capacity_bytes(void);
 int scarf_srm_tc_structured_noalloc(const scarf_srm_setup *s, const int fs[3], const int n[3], float ds,
                                     const float *d_table, int nh, float *d_field, void *stream);

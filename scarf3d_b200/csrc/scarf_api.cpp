@@ -847,14 +847,14 @@ int scarf_srm_direct_points(const scarf_srm_setup* s, const float* d_x, const fl
 // (wider column tiles), or follow a tuned choice for the grid's bucket when
 // tuned plans are enabled; the same rule sizes their workspace.
 }  // extern "C"
-namespace {
+namespace scarf {
 bool device_field_plan(int ndim, const int n[3], int nh, TcPlan* p) {
   TcChoice c{};
   if (n[0] > 0 && n[1] > 0 && n[2] > 0 && tc_tuned_choice(ndim, n, false, &c))
     return tc_make_plan(ndim, n, nh, p, c.tile_j, c.permute != 0, c.variant);
   return tc_make_plan(ndim, n, nh, p, 0, true);
 }
-}  // namespace
+}  // namespace scarf
 extern "C" {
 size_t scarf_srm_tc_workspace_bytes(int ndim, const int n[3], int nh) {
   TcPlan p{};

@@ -68,6 +68,11 @@ struct TcChoice {
 // The tuned choice for a grid when tuned plans are enabled and its bucket has
 // an entry (fixed_columns: the caller keeps k = z, as scarf_execute does).
 bool tc_tuned_choice(int ndim, const int n[3], bool fixed_columns, TcChoice* c);
+// Plan of the device-field entry points (scarf_srm_tc_structured and the
+// allocation-free variant): a tuned choice for the grid's bucket when tuned
+// plans are enabled, else the default plan with the longest axis as columns.
+// The same rule sizes scarf_srm_tc_workspace_bytes.
+bool device_field_plan(int ndim, const int n[3], int nh, TcPlan* p);
 // Harmonics accumulated in tensor memory before each FP32 drain (rounded up
 // to whole pipeline stages); 0 restores the default.
 void tc_set_chunk_harmonics(int harmonics);

@@ -19,8 +19,17 @@
 // other's tables -- serialise them.
 //
 // The device address of the array is looked up with cudaGetSymbolAddress the
-// first time the entry point runs on each device (with that device current);
-// that first call should therefore be made before any stream capture begins.
+// first time the entry point runs in each device context (with that device
+// current) and cached under the context's process-unique id, so a
+// cudaDeviceReset, or another driver-API context made current on the same
+// device, makes the next call look the address up again instead of using a
+// stale one. Each call copies its status word back and synchronises its
+// stream, so it cannot be recorded into a CUDA graph.
+//
+// The plan (kernel form, row tile, column axis) follows the same rule as
+// scarf_srm_tc_structured, tuned plans included, so both entry points run the
+// same plan and scarf_srm_tc_workspace_bytes gives the scratch this one needs.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -41,24 +50,62 @@ namespace {
 constexpr size_t kNoAllocScratchBytes = SCARF_NOALLOC_SCRATCH_BYTES;
 constexpr int kMaxDevices = 64;
 std::mutex g_noalloc_mu;
-void* g_noalloc_ptr[kMaxDevices] = {};
+struct ScratchSlot {
+  unsigned long long ctx_id;  // process-unique id of the context the address belongs to
+  void* ptr;
+};
+ScratchSlot g_noalloc_slot[kMaxDevices] = {};
 
-// Device address of g_noalloc_scratch on the current device (set-up on the
-// first call per device). In host code the symbol itself is only a host-side
-// stand-in and must never be passed to a kernel.
+using CtxGetCurrentFn = CUresult (*)(CUcontext*);
+using CtxGetIdFn = CUresult (*)(CUcontext, unsigned long long*);
+
+// Unique id of the current context (0 when it cannot be read). The driver
+// routines are fetched through the runtime, so the library does not link
+// libcuda itself.
+unsigned long long current_context_id() {
+  static CtxGetCurrentFn get_current = nullptr;
+  static CtxGetIdFn get_id = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &f, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_current = reinterpret_cast<CtxGetCurrentFn>(f);
+    f = nullptr;
+    if (cudaGetDriverEntryPointByVersion("cuCtxGetId", &f, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_id = reinterpret_cast<CtxGetIdFn>(f);
+  });
+  if (!get_current || !get_id) return 0;
+  CUcontext ctx = nullptr;
+  unsigned long long id = 0;
+  if (get_current(&ctx) != CUDA_SUCCESS || !ctx) return 0;
+  if (get_id(ctx, &id) != CUDA_SUCCESS) return 0;
+  return id;
+}
+
+// Device address of g_noalloc_scratch in the current context. In host code
+// the symbol itself is only a host-side stand-in and must never be passed to
+// a kernel. The lookup (set-up) runs once per device context: when the
+// context's id cannot be read it runs on every call instead.
 cudaError_t scratch_address(void** out) {
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
   if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
   std::lock_guard<std::mutex> lk(g_noalloc_mu);
-  if (!g_noalloc_ptr[dev]) {
-    void* p = nullptr;
-    e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (e != cudaSuccess) return e;
-    g_noalloc_ptr[dev] = p;
+  unsigned long long id = current_context_id();
+  if (id != 0 && g_noalloc_slot[dev].ptr && g_noalloc_slot[dev].ctx_id == id) {
+    *out = g_noalloc_slot[dev].ptr;
+    return cudaSuccess;
   }
-  *out = g_noalloc_ptr[dev];
+  void* p = nullptr;
+  e = cudaGetSymbolAddress(&p, g_noalloc_scratch);  // also makes the primary context current if none was
+  if (e != cudaSuccess) return e;
+  if (id == 0) id = current_context_id();
+  g_noalloc_slot[dev] = ScratchSlot{id, id != 0 ? p : nullptr};
+  *out = p;
   return cudaSuccess;
 }
 
@@ -74,7 +121,7 @@ extern "C" int scarf_srm_tc_structured_noalloc(const scarf_srm_setup* s, const i
   if (!s || !fs || !n || !d_table || !d_field || nh <= 0)
     return record_error(SCARF_ERR_ARG, "scarf_srm_tc_structured_noalloc: invalid argument");
   TcPlan p{};
-  if (!tc_make_plan(s->ndim, n, nh, &p, 0, true))
+  if (!device_field_plan(s->ndim, n, nh, &p))
     return record_error(SCARF_ERR_ARG, "scarf_srm_tc_structured_noalloc: invalid grid");
   if (p.bytes > kNoAllocScratchBytes)
     return record_error(SCARF_ERR_ARG,
