@@ -71,7 +71,7 @@ int scarf_get_nharm(void);
 /* SCARF_FORM_*. */
 int scarf_set_form(int form);
 /* Install the reference's own uniform source (prng.cpp set_seed / srng,
- * TRNG4 yarn2 + uniform01_dist<float>) so that harmonics are drawn exactly as
+ * TRNG4 yarn2 + uniform01_dist<>) so that harmonics are drawn exactly as
  * the reference draws them. NULL, NULL restores the built-in generator. */
 int scarf_set_uniform_source(void (*set_seed)(int), void (*srng)(float *));
 /* Stream for all device work of the reference-compatible API. */

@@ -43,10 +43,15 @@ static int64_t orc_powmod(int64_t base, int64_t e) {
 }
 
 void orc_rng_seed(orc_rng *g, int seed) {
-  /* seed (unsigned long, prng.cpp:147) reduced modulo the prime; the older
-   * state word starts at 1 so the state is never all-zero. */
-  unsigned long s = (unsigned long)(long)seed;
-  g->r0 = (int64_t)(s % (unsigned long)ORC_MOD);
+  /* prng.cpp:147 converts the int seed to unsigned long and calls
+   * trng::yarn2::seed(unsigned long). The published seeding of TRNG's
+   * multiple recursive generators reduces the seed, read back as a signed
+   * 64-bit integer, into [0, m) (adding m to a negative remainder) and sets
+   * the older state word to 1, so the state is never all-zero. */
+  int64_t t = (int64_t)(unsigned long)(long)seed;
+  t %= ORC_MOD;
+  if (t < 0) t += ORC_MOD;
+  g->r0 = t;
   g->r1 = 1;
 }
 
@@ -58,8 +63,12 @@ uint32_t orc_rng_next(orc_rng *g) {
 }
 
 float orc_u01(uint32_t y) {
-  /* top 23 bits, centred in their bin: exact float in [2^-24, 1-2^-24] */
-  return ((float)(y >> 8) + 0.5f) * (1.0f / 8388608.0f);
+  /* trng::uniform01_dist<> (prng.cpp:159-163) takes its default result type,
+   * double: one generator output y in [0, m-1] scaled into [0,1) by the
+   * generator's range, y * (1/m) in double precision. srng stores each draw
+   * into a float, rounding to nearest (the result can be 0, and can round up
+   * to 1.0f for the largest y). 1/m is 0x1.00000002p-31 in double. */
+  return (float)((double)y * 0x1.00000002p-31);
 }
 
 void orc_srng(orc_rng *g, float r[2]) {

@@ -52,7 +52,7 @@ typedef struct {
 typedef struct { int64_t r0, r1; } orc_rng;
 void orc_rng_seed(orc_rng *g, int seed);
 uint32_t orc_rng_next(orc_rng *g);            /* raw output in [0, 2^31-2]  */
-float orc_u01(uint32_t y);                   /* open-interval float        */
+float orc_u01(uint32_t y);                   /* [0,1] float: double draw rounded to float */
 void orc_srng(orc_rng *g, float r[2]);       /* prng.cpp:152-165 analogue  */
 
 /* --- spectra and quadrature ---------------------------------------------- */

@@ -82,10 +82,13 @@ uint32_t Yarn2::output(uint64_t r) {
 }
 
 void Yarn2::seed(int s) {
-  // trng seed(unsigned long) with the signed seed converted as prng.cpp:147
-  // does; reduced modulo the prime, second word 1 (state never all-zero).
-  const unsigned long us = static_cast<unsigned long>(static_cast<long>(s));
-  r0 = static_cast<uint64_t>(us % static_cast<unsigned long>(kMod));
+  // prng.cpp:147 passes the int seed as unsigned long to yarn2::seed, whose
+  // published rule reduces it, read as a signed 64-bit integer, into [0, m)
+  // and sets the older state word to 1 (the state is never all-zero).
+  int64_t t = static_cast<int64_t>(static_cast<unsigned long>(static_cast<long>(s)));
+  t %= static_cast<int64_t>(kMod);
+  if (t < 0) t += static_cast<int64_t>(kMod);
+  r0 = static_cast<uint64_t>(t);
   r1 = 1;
 }
 

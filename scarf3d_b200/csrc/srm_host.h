@@ -14,8 +14,10 @@ namespace scarf {
 // YARN2-type uniform source: order-2 multiple recursive generator modulo the
 // Mersenne prime 2^31-1 (multipliers 1498809829, 1160990996) whose output is
 // the power g^r mod (2^31-1), g = 123567893 -- the parameters TRNG publishes
-// for trng::yarn2, which prng.cpp:60 instantiates. Draws map to floats in the
-// open interval (0,1) as ((y >> 8) + 0.5) * 2^-23.
+// for trng::yarn2, which prng.cpp:60 instantiates. A draw is
+// trng::uniform01_dist<> with its default (double) result type, stored into
+// a float as srng does (prng.cpp:152-165): y * (1/m) in double, rounded to
+// float, so 0 <= draw <= 1 (0 for y = 0, 1.0f for the largest y).
 class Yarn2 {
  public:
   static constexpr uint64_t kMod = 2147483647ull;
@@ -29,7 +31,8 @@ class Yarn2 {
   // Advance the state by n raw draws in O(log n).
   void jump(uint64_t n);
 
-  static float to_u01(uint32_t y) { return (static_cast<float>(y >> 8) + 0.5f) * (1.0f / 8388608.0f); }
+  static float to_u01(uint32_t y) { return static_cast<float>(static_cast<double>(y) * kInvMod); }
+  static constexpr double kInvMod = 0x1.00000002p-31;  // 1 / (2^31 - 1), rounded to double
   static uint32_t output(uint64_t r);  // g^r mod m (0 for r == 0)
   static uint64_t mulmod(uint64_t a, uint64_t b);
 

@@ -101,8 +101,9 @@ struct Gen {
   }
 };
 
+// The host's Yarn2::to_u01: y * (1/m) in double, rounded to float.
 __device__ __forceinline__ float to_u01(uint32_t y) {
-  return __fmul_rn(__fadd_rn(static_cast<float>(y >> 8), 0.5f), 1.0f / 8388608.0f);
+  return __double2float_rn(__dmul_rn(static_cast<double>(y), 0x1.00000002p-31));
 }
 
 // 0 = certain reject, 1 = certain accept, 2 = uncertain.

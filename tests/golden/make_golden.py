@@ -1,8 +1,9 @@
 """Generate the golden fixtures of the CPU oracle (tests/golden/*.npz).
 
-The reference cannot be built or run in this environment (Fortran + MPI +
-TRNG4) and ships no golden vectors, so these fixtures come from the oracle
-itself. They pin the oracle (setup scalars, harmonic table, FP32 op-order
+The reference cannot be built or run in this environment or on the GPU host
+(Fortran + MPI + TRNG4, all absent) and ships no golden vectors, so these
+fixtures come from the oracle itself, whose uniform stream follows TRNG's
+documented yarn2 seeding and uniform01_dist<> (double draw stored as float). They pin the oracle (setup scalars, harmonic table, FP32 op-order
 field, FP64 field, statistics) against unintended changes; the product is
 checked against them and against the live oracle.
 

@@ -39,12 +39,39 @@ def test_uniform_stream_golden():
     assert np.array_equal(oracle.raw_stream(-7, 64), ref["seed_neg7"])
 
 
-def test_uniform_stream_is_open_interval_and_uniform():
+def test_uniform_stream_is_unit_interval_and_uniform():
     raw = oracle.raw_stream(42, 20000)
     assert raw.max() < 2 ** 31 - 1
     u = np.array([oracle.L.orc_u01(int(y)) for y in raw[:5000]], np.float32)
-    assert u.min() > 0.0 and u.max() < 1.0
+    assert u.min() >= 0.0 and u.max() <= 1.0
     assert abs(u.mean() - 0.5) < 0.02 and abs(u.std() - math.sqrt(1 / 12)) < 0.01
+
+
+def test_uniform_draw_is_a_double_draw_rounded_to_float():
+    """uniform01_dist<> draws a double y/m in [0,1) (default result type) and
+    srng stores it into a float (prng.cpp:152-165): the float is the double
+    y * (1/m) rounded to nearest, so it can be 0 and can round up to 1."""
+    m = 2 ** 31 - 1
+    ys = [0, 1, 2, 255, 256, 1 << 20, m // 2, m - 65, m - 64, m - 2, m - 1]
+    ys += [int(y) for y in oracle.raw_stream(5, 4000)]
+    for y in ys:
+        assert oracle.L.orc_u01(y) == np.float32(np.float64(y) * (1.0 / m))
+    assert oracle.L.orc_u01(0) == 0.0
+    assert oracle.L.orc_u01(m - 1) == 1.0
+
+
+def test_negative_seed_is_reduced_as_a_signed_integer():
+    """prng.cpp:147 turns the int seed into unsigned long; yarn2's seeding
+    reads it back as a signed 64-bit value and reduces it into [0, m): seed -7
+    starts from the state (m - 7, 1)."""
+    m = 2 ** 31 - 1
+    a1, a2, g = 1498809829, 1160990996, 123567893
+    r0, r1 = m - 7, 1
+    want = []
+    for _ in range(8):
+        r0, r1 = (a1 * r0 + a2 * r1) % m, r0
+        want.append(0 if r0 == 0 else pow(g, r0, m))
+    assert list(oracle.raw_stream(-7, 8)) == want
 
 
 # ---------------------------------------------------------------- quadrature --
