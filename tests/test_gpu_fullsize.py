@@ -1,7 +1,8 @@
-"""Full-size workloads on the GPU, checked where the CPU oracle can follow:
-at sampled points (FP32 restatement and FP64 oracle over the identical
-harmonic table) and through size-independent properties (determinism,
-statistics)."""
+"""Full-size workloads on the GPU, checked point by point over the whole field
+against the FP64 sum over the identical harmonic table (oracle/gpu_fp64.py,
+itself pinned to the CPU FP64 oracle below), at sampled points against the
+CPU oracle (FP32 restatement and FP64), and through size-independent
+properties (determinism, statistics)."""
 import ctypes
 
 import numpy as np
@@ -9,7 +10,8 @@ import pytest
 
 import oracle
 import scarf3d_b200 as sb
-from srm_cases import iarr
+from oracle import gpu_fp64
+from srm_cases import iarr, random_points, structured_case
 
 torch = pytest.importorskip("torch")
 pytestmark = pytest.mark.gpu
@@ -54,7 +56,36 @@ def _structured(n, ds, kw, seed, nharm, form, dh=None):
     def ref(idx, f64):
         return oracle.sum_structured(so, fs, list(n), ds, tab, idx=idx, f64=f64)
 
+    def full():
+        return gpu_fp64.compare_structured(out, so, fs, list(n), ds, tab)
+
+    ref.full = full
+    ref.tab = tab
+    ref.setup = so
     return out, ref, npts
+
+
+# --------------------------------------------------- the FP64 full-field checker
+@pytest.mark.parametrize("name", ["vk3d", "vk3d_rot_offset", "vk3d_dh_lt_ds", "gs2d"])
+def test_fp64_checker_matches_cpu_fp64_oracle_structured(name):
+    case = structured_case(name)
+    so = oracle.setup(case["op"])
+    tab, _ = oracle.sample(case["op"], so)
+    ref = oracle.sum_structured(so, case["fs"], case["n"], case["ds"], tab, f64=True)
+    got = gpu_fp64.structured_field(so, case["fs"], case["n"], case["ds"], tab).cpu().numpy()
+    assert np.max(np.abs(got - ref)) <= 1e-11 * ref.std()
+
+
+def test_fp64_checker_matches_cpu_fp64_oracle_points():
+    x, y, z = random_points(5000)
+    p = oracle.params(acf=1, nharm=400, seed=7, sigma=0.1, ds=100.0, cl=[1500.0, 1500.0, 500.0],
+                      nc=[float(a.min()) for a in (x, y, z)], fc=[float(a.max()) for a in (x, y, z)], alpha=25.0)
+    s = oracle.setup(p)
+    tab, _ = oracle.sample(p, s)
+    ref = oracle.sum_points(s, x, y, z, tab, f64=True)
+    dx, dy, dz = (torch.from_numpy(a.copy()).cuda() for a in (x, y, z))
+    got = gpu_fp64.points_field(s, dx, dy, dz, tab).cpu().numpy()
+    assert np.max(np.abs(got - ref)) <= 1e-11 * ref.std()
 
 
 def test_plain_config_128cubed_direct():
@@ -64,6 +95,8 @@ def test_plain_config_128cubed_direct():
     e64, e32, _ = _sampled_errors(out, ref, npts)
     assert e32 <= 1e-6
     assert e64 <= 5e-5
+    full = ref.full()  # every point against the FP64 sum
+    assert full["points"] == npts and full["rel_rms"] <= 5e-5, full
 
 
 def test_precision_config_512cubed_tc_and_determinism():
@@ -73,8 +106,23 @@ def test_precision_config_512cubed_tc_and_determinism():
     first = out.clone()
     e64, e32, emax = _sampled_errors(out, ref, npts, count=192)
     assert e64 <= 1e-5, e64
+    full = ref.full()  # every one of the 1.3e8 points against the FP64 sum
+    assert full["points"] == npts and full["rel_rms"] <= 1e-5, full
+    assert full["max_abs"] <= 1e-4 * full["std_ref"], full
+    # the FP64 checker agrees with the CPU FP64 oracle at 2 000 sampled points
+    idx = np.sort(np.random.default_rng(3).choice(npts, size=2000, replace=False)).astype(np.int64)
+    g64 = gpu_fp64.structured_field(ref.setup, [1, 1, 1], [512, 512, 512], 25.0, ref.tab).cpu().numpy()[idx]
+    assert np.max(np.abs(g64 - ref(idx, True))) <= 1e-10 * full["std_ref"]
     out2, _, _ = _structured((512, 512, 512), 25.0, kw, 1234, 20000, "tc")
     assert torch.equal(first, out2)  # fixed reduction order: bitwise reproducible
+
+
+def test_precision_config_512cubed_direct_full_field():
+    """The plain FP32 direct sum at 512^3 x 20 000, every point against FP64."""
+    kw = dict(acf=0, hurst=0.5, sigma=0.05, cl=[3000.0, 3000.0, 1000.0])
+    out, ref, npts = _structured((512, 512, 512), 25.0, kw, 1234, 20000, "direct")
+    full = ref.full()
+    assert full["points"] == npts and full["rel_rms"] <= 5e-5, full
 
 
 def test_unstructured_config_2M_points_gaussian():
@@ -103,6 +151,9 @@ def test_unstructured_config_2M_points_gaussian():
     e64, e32, _ = _sampled_errors(dev, ref, len(x))
     assert e32 <= 1e-6
     assert abs(stats[2] / float(dev.double().std().item()) - 1) < 1e-5
+    dx, dy, dz = (torch.from_numpy(a.copy()).cuda() for a in (x, y, z))
+    full = gpu_fp64.compare_points(dev, s, dx, dy, dz, tab)  # all 2e6 points against FP64
+    assert full["points"] == len(x) and full["rel_rms"] <= 5e-5, full
 
 
 def test_large_config_2048x2048x512_tc():
@@ -131,6 +182,8 @@ def test_large_config_2048x2048x512_tc():
 
     e64, _, _ = _sampled_errors(dev, ref, int(np.prod(n)), count=96)
     assert e64 <= 1e-5, e64
+    full = gpu_fp64.compare_structured(dev, so, fs, n, 10.0, tab)  # all 2.1e9 points against FP64
+    assert full["points"] == int(np.prod(n)) and full["rel_rms"] <= 1e-5, full
     std = float(dev.double().std().item())
     mean = float(dev.double().mean().item())
     assert abs(stats[2] / std - 1) < 1e-5
