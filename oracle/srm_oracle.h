@@ -112,6 +112,17 @@ int orc_execute_structured(const orc_params *p, const int fs[3], const int fe[3]
                            const float *poi, int npoi, float mute, float taper,
                            float *field, float info[6], int nthreads);
 
+/* FIM restatement (fim_oracle.c): internal grid, spectrum with Hermitian
+ * planes (half grid, interleaved complex), nearest-node mapping. */
+void orc_fim_grid(int ndim, const float nc[3], const float fc[3], float dh, const float cl[3], int pad, int npts[3],
+                  float off_axis[3], float info01[2]);
+void orc_fim_spectrum(const int npts[3], int ndim, float ds, float dh, int acf, const float cl[3], float sigma,
+                      float hurst, int seed, float *spec);
+void orc_fim_map_structured(const int npts[3], const float *delta, float dh, const float off_axis[3], const int fs[3],
+                            const int fe[3], float ds, float *field);
+void orc_fim_map_points(const int npts[3], const float *delta, float dh, const float off_axis[3], const float *x,
+                        const float *y, const float *z, int64_t n, int ndim, float *field);
+
 #ifdef __cplusplus
 }
 #endif
