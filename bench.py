@@ -11,7 +11,18 @@ tables from the harmonic table, then the factorised tcgen05 split-FP16 sum
 (scaled field written to HBM). `value` times K such steps with the harmonic
 table already on the device; `e2e` times K calls of the public C ABI
 (scarf_execute) with a pinned host output buffer: host sampler, H2D of the
-harmonic table, device sum, statistics, D2H of the field.
+harmonic table, device sum, statistics, D2H of the field (`e2e.pageable`: the
+same into a malloc'd field). `accuracy` compares every point of the field
+with the FP64 sum over the same harmonics; `direct_sum` times the FP32 direct
+sum over the whole table on the same grid.
+
+The other configurations are measured on their own (`configs`, single GPU):
+128^3 x 5 000 (plain direct sum, and the tensor-core form beside it),
+2e6 unstructured points x 10 000 (direct sum), 2048 x 2048 x 512 x 50 000
+(tensor-core form), each with kernel time, roofline, end to end through
+scarf_execute, full-field error against FP64 and, for the first two, the CPU
+restatement over the whole workload; `batched` is the 256-field
+configuration.
 
 --impl reference times the CPU restatement of the reference's SRM (the
 reference itself cannot be built here: no Fortran compiler, MPI or TRNG4)
@@ -44,7 +55,7 @@ UNIT = "pt*harm/s"
 WORKLOAD = dict(nx=512, ny=512, nz=512, ds=25.0, acf=0, hurst=0.5, cl=[3000.0, 3000.0, 1000.0], sigma=0.05,
                 nharm=20000, seed=1234)
 FLOP_PER_PTHARM = 12  # 2 real MACs per harmonic and point (complex as real K=2) x 3 split products
-DIRECT_HARM = 2000    # harmonics timed for the direct-sum comparison (throughput is linear in harmonics)
+DIRECT_HARM = 2000    # harmonics of the direct sum's warm-up launch (the timed launch sums the whole table)
 
 
 def workload_name(w) -> str:
@@ -63,16 +74,13 @@ def load_peaks():
 
 
 def pick_peak(clocks: dict):
-    """The burst peak when the timed launches ran at (near) full SM clock (a
-    short run: the power limiter's average has not caught up), else the
-    sustained, power-capped one: the kernel is compared with cuBLAS at the
-    same clock regime. Unsampled clocks count as full clock (the stricter
-    denominator)."""
+    """The burst peak: every kernel here is timed in isolation (back-to-back
+    launches of the kernel alone), which is what the burst cuBLAS figure
+    measures. The sustained, power-capped figure is reported beside it."""
     burst, sustained, src = load_peaks()
     sm, mx = clocks.get("sm_mhz"), clocks.get("sm_max_mhz")
-    if sm is None or not mx or sm >= 0.97 * mx:
-        return burst, f"{src} bf16 dense, burst (the timed launches ran at full SM clock)"
-    return sustained, f"{src} bf16 dense, sustained (the timed launches ran at {sm:.0f} of {mx:.0f} MHz)"
+    note = "" if sm is None or not mx else f" (the timed launches ran at a median {sm:.0f} of {mx:.0f} MHz)"
+    return burst, sustained, f"{src} bf16 dense, burst{note}"
 
 
 def profile_traffic():
@@ -320,6 +328,244 @@ def run_batched(args, nfields=256):
                         "nharm U[2000,20000], ds 50 m, meta-seed 20240"}
 
 
+# ---------------------------------------------------------------------------
+# The other configurations of the path, each measured on its own: kernel time
+# (CUDA events around the summation kernel alone, on its launch stream), the
+# roofline of that kernel, end to end through the public C ABI with host
+# buffers (sampling, H2D, sum, statistics, D2H inside the timed region), the
+# error of every point against the FP64 sum over the identical harmonics, and
+# where it is affordable the CPU restatement over the whole workload.
+CONFIG1 = dict(name="plain_structured_128cubed_ds50m_vk_h0.25_cl2000_nharm5000", n=[128, 128, 128], ds=50.0, acf=0,
+               hurst=0.25, cl=[2000.0, 2000.0, 2000.0], sigma=0.05, nharm=5000, seed=1234)
+CONFIG2 = dict(name="plain_unstructured_2e6pts_20x20x10km_gs_cl1500/1500/500_nharm10000", npts=2_000_000,
+               box=[20000.0, 20000.0, 10000.0], pts_seed=7, dh=100.0, acf=1, hurst=0.0, cl=[1500.0, 1500.0, 500.0],
+               sigma=0.1, nharm=10000, seed=7)
+CONFIG5 = dict(name="large_structured_2048x2048x512_ds10m_vk_h0.3_cl5000/5000/2000_nharm50000", n=[2048, 2048, 512],
+               ds=10.0, acf=0, hurst=0.3, cl=[5000.0, 5000.0, 2000.0], sigma=0.08, nharm=50000, seed=1234)
+DIRECT_WARP_INSTR_PER_PTHARM = 1.19  # ncu: sm__inst_executed per point*harmonic of srm_direct_kernel
+FP32_FLOP_PER_PTHARM = 9             # phase 3 mul + 2 add, accumulate 2 mul + 2 add (plus one sincosf)
+
+
+def _i3(v):
+    return (ctypes.c_int * 3)(*[int(x) for x in v])
+
+
+def _direct_roofline(value, sm_max_mhz):
+    """Issue-bound roofline of the FP32 direct sum: warp instructions per
+    point*harmonic (ncu) against 148 SMs x 4 schedulers x the SM clock."""
+    clk = (sm_max_mhz or 1965.0) * 1e6
+    achieved = value * DIRECT_WARP_INSTR_PER_PTHARM / 1e12
+    peak = 148 * 4 * clk / 1e12
+    fp32 = value * FP32_FLOP_PER_PTHARM / 1e12
+    fp32_peak = 148 * 128 * 2 * clk / 1e12
+    return {"bound": "issue", "achieved": achieved, "peak": peak, "unit": "T warp-instr/s", "frac": achieved / peak,
+            "instr_per_ptharm": DIRECT_WARP_INSTR_PER_PTHARM, "fp32_tflops": fp32, "fp32_peak_tflops": fp32_peak,
+            "fp32_frac": fp32 / fp32_peak, "kernel": "srm_direct_kernel", "traffic": None}
+
+
+def _tc_roofline(value, peaks):
+    burst, sustained, src = peaks
+    achieved = value * FLOP_PER_PTHARM / 1e12
+    return {"bound": "tensor", "achieved": achieved, "peak": burst, "unit": "TFLOP/s", "frac": achieved / burst,
+            "frac_of_sustained": achieved / sustained, "peak_kind": f"{src} bf16 dense, burst",
+            "kernel": "srm_tc_kernel", "traffic": None}
+
+
+def _kernel_times(launch, steps, warm=1):
+    import scarf3d_b200 as sb
+    ms = []
+    for it in range(warm + steps):
+        launch()
+        if it >= warm:
+            ms.append(float(sb.lib.scarf_last_kernel_ms()))
+    return ms
+
+
+def _structured_leg(cfg, forms, steps, e2e_steps, peaks, clocks, cpu_full=False, e2e_form=None):
+    """One structured configuration: kernel timing per form, full-field error
+    against FP64, end to end through scarf_execute with a host field."""
+    import torch
+
+    import oracle
+    import scarf3d_b200 as sb
+    from oracle import gpu_fp64
+
+    n, ds = cfg["n"], cfg["ds"]
+    npts = int(np.prod(n))
+    fs, fe = [1, 1, 1], list(n)
+    ds32 = np.float32(ds)
+    nc = [0.0, 0.0, 0.0]
+    fc = [float(np.float32(n[c] - 1) * ds32) for c in range(3)]
+    kw = dict(acf=cfg["acf"], nharm=cfg["nharm"], seed=cfg["seed"], hurst=cfg["hurst"], sigma=cfg["sigma"], ds=ds,
+              cl=cfg["cl"])
+    p = sb.make_params(nc=nc, fc=fc, **kw)
+    s = sb.compute_setup(p)
+    t0 = time.perf_counter()
+    tab, _ = sb.sample(p, s)
+    t_sample = time.perf_counter() - t0
+    nh = len(tab)
+    d_tab = torch.from_numpy(tab.reshape(-1).copy()).cuda()
+    field = torch.empty(npts, dtype=torch.float32, device="cuda")
+    stream = torch.cuda.current_stream()
+    sptr = ctypes.c_void_p(stream.cuda_stream)
+    so = oracle.setup(oracle.params(nc=nc, fc=fc, **kw))
+    out = {"workload": cfg["name"], "grid": list(n), "nharm": cfg["nharm"], "harmonics_kept": nh,
+           "work_pt_harm": float(npts) * nh, "host_sampling_ms": t_sample * 1e3}
+    for form in forms:
+        if form == "tc":
+            wb = sb.tc_workspace_bytes(3, n, nh)
+            work = torch.empty(wb, dtype=torch.uint8, device="cuda")
+
+            def launch():
+                sb.check(sb.lib.scarf_srm_tc_structured(ctypes.byref(s), _i3(fs), _i3(n), ds,
+                                                        ctypes.c_void_p(d_tab.data_ptr()), nh,
+                                                        ctypes.c_void_p(field.data_ptr()),
+                                                        ctypes.c_void_p(work.data_ptr()), wb, sptr))
+        else:
+            work = None
+
+            def launch():
+                sb.check(sb.lib.scarf_srm_direct_structured(ctypes.byref(s), _i3(fs), _i3(n), ds,
+                                                            ctypes.c_void_p(d_tab.data_ptr()), nh,
+                                                            ctypes.c_void_p(field.data_ptr()), sptr))
+        ms = _kernel_times(launch, steps)
+        torch.cuda.synchronize()
+        value = float(npts) * nh / (np.mean(ms) / 1e3)
+        acc = gpu_fp64.compare_structured(field, so, fs, n, ds, tab)
+        roof = _tc_roofline(value, peaks) if form == "tc" else _direct_roofline(value, clocks.get("sm_max_mhz"))
+        out[form] = {"value": value, "unit": UNIT, "kernel_ms": float(np.mean(ms)), "launches_timed": len(ms),
+                     "roofline": roof,
+                     "accuracy_vs_fp64_full_field": {k: acc[k] for k in ("rel_rms", "max_abs", "std_ref", "points")}}
+        if form == "tc":
+            out[form]["plan"] = sb.tc_plan_info(3, n, nh)
+        del work
+    del field
+    torch.cuda.empty_cache()
+    # End to end: scarf_execute into a page-locked host field.
+    ef = e2e_form or forms[0]
+    host = torch.empty(npts, dtype=torch.float32, pin_memory=True)
+    sb.set_nharm(cfg["nharm"])
+    sb.set_form(sb.FORM_TC if ef == "tc" else sb.FORM_DIRECT)
+    sb.set_stream(stream.cuda_stream)
+    sb.scarf_initialize(fs=fs, fe=fe, ds=ds, acf=cfg["acf"], cl=cfg["cl"], sigma=cfg["sigma"], method=1,
+                        hurst=cfg["hurst"], nc=np.asarray(nc, np.float32), fc=np.asarray(fc, np.float32))
+    stats = np.zeros(8, np.float32)
+    fptr = ctypes.c_void_p(host.data_ptr())
+    sp = stats.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+    try:
+        sb.check(sb.lib.scarf_execute_ex(cfg["seed"], fptr, sp, 0))
+        t0 = time.perf_counter()
+        for _ in range(e2e_steps):
+            sb.check(sb.lib.scarf_execute_ex(cfg["seed"], fptr, sp, 0))
+        t_e2e = (time.perf_counter() - t0) / e2e_steps
+    finally:
+        sb.scarf_finalize()
+        sb.set_form(sb.FORM_AUTO)
+        sb.set_nharm(10000)
+    out["e2e"] = {"value": float(npts) * nh / t_e2e, "unit": UNIT, "form": ef, "ms_per_step": t_e2e * 1e3,
+                  "steps": e2e_steps, "host_memory": "page-locked", "h2d_bytes_per_step": int(nh * 20),
+                  "d2h_bytes_per_step": int(npts * 4 + 8), "stats_std_mean": [float(stats[2]), float(stats[3])]}
+    del host
+    if cpu_full:
+        nth = os.cpu_count() or 1
+        t0 = time.perf_counter()
+        oracle.sum_structured_mt(so, fs, n, ds, tab, nth)
+        dt = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": float(npts) * nh / dt, "unit": UNIT, "cores": nth, "kind": "port",
+                               "sample": f"the whole workload, {dt:.1f} s (FP32 restatement, {nth} threads)"}
+    return out
+
+
+def _points_leg(cfg, steps, e2e_steps, clocks, cpu_full=True):
+    """The unstructured configuration: FP32 direct sum over a point set."""
+    import torch
+
+    import oracle
+    import scarf3d_b200 as sb
+    from oracle import gpu_fp64
+
+    rng = np.random.default_rng(cfg["pts_seed"])
+    pts = (rng.random((3, cfg["npts"])) * np.asarray(cfg["box"])[:, None]).astype(np.float32)
+    x, y, z = (np.ascontiguousarray(a) for a in pts)
+    npts = len(x)
+    nc = [float(a.min()) for a in (x, y, z)]
+    fc = [float(a.max()) for a in (x, y, z)]
+    kw = dict(acf=cfg["acf"], nharm=cfg["nharm"], seed=cfg["seed"], hurst=cfg["hurst"], sigma=cfg["sigma"],
+              ds=cfg["dh"], cl=cfg["cl"])
+    p = sb.make_params(nc=nc, fc=fc, **kw)
+    s = sb.compute_setup(p)
+    tab, _ = sb.sample(p, s)
+    nh = len(tab)
+    d_tab = torch.from_numpy(tab.reshape(-1).copy()).cuda()
+    dx, dy, dz = (torch.from_numpy(a).cuda() for a in (x, y, z))
+    field = torch.empty(npts, dtype=torch.float32, device="cuda")
+    sptr = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+    def launch():
+        sb.check(sb.lib.scarf_srm_direct_points(ctypes.byref(s), ctypes.c_void_p(dx.data_ptr()),
+                                                ctypes.c_void_p(dy.data_ptr()), ctypes.c_void_p(dz.data_ptr()),
+                                                npts, ctypes.c_void_p(d_tab.data_ptr()), nh,
+                                                ctypes.c_void_p(field.data_ptr()), sptr))
+    ms = _kernel_times(launch, steps)
+    torch.cuda.synchronize()
+    value = float(npts) * nh / (np.mean(ms) / 1e3)
+    so = oracle.setup(oracle.params(nc=nc, fc=fc, **kw))
+    acc = gpu_fp64.compare_points(field, so, dx, dy, dz, tab)
+    out = {"workload": cfg["name"], "points": npts, "nharm": cfg["nharm"], "harmonics_kept": nh, "dh": cfg["dh"],
+           "work_pt_harm": float(npts) * nh,
+           "direct": {"value": value, "unit": UNIT, "kernel_ms": float(np.mean(ms)), "launches_timed": len(ms),
+                      "roofline": _direct_roofline(value, clocks.get("sm_max_mhz")),
+                      "accuracy_vs_fp64_full_field": {k: acc[k] for k in ("rel_rms", "max_abs", "std_ref",
+                                                                          "points")}}}
+    # End to end: scarf_nocart_initialize + scarf_execute into a page-locked host field.
+    host = torch.empty(npts, dtype=torch.float32, pin_memory=True)
+    sb.set_nharm(cfg["nharm"])
+    sb.set_stream(torch.cuda.current_stream().cuda_stream)
+    sb.scarf_initialize(x=x, y=y, z=z, dh=cfg["dh"], acf=cfg["acf"], cl=cfg["cl"], sigma=cfg["sigma"], method=1)
+    stats = np.zeros(8, np.float32)
+    fptr = ctypes.c_void_p(host.data_ptr())
+    sp = stats.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+    try:
+        sb.check(sb.lib.scarf_execute_ex(cfg["seed"], fptr, sp, 0))
+        t0 = time.perf_counter()
+        for _ in range(e2e_steps):
+            sb.check(sb.lib.scarf_execute_ex(cfg["seed"], fptr, sp, 0))
+        t_e2e = (time.perf_counter() - t0) / e2e_steps
+    finally:
+        sb.scarf_finalize()
+        sb.set_nharm(10000)
+    out["e2e"] = {"value": float(npts) * nh / t_e2e, "unit": UNIT, "form": "direct", "ms_per_step": t_e2e * 1e3,
+                  "steps": e2e_steps, "host_memory": "page-locked", "h2d_bytes_per_step": int(nh * 20 + 12 * npts),
+                  "d2h_bytes_per_step": int(npts * 4 + 8), "stats_std_mean": [float(stats[2]), float(stats[3])]}
+    if cpu_full:
+        nth = os.cpu_count() or 1
+        t0 = time.perf_counter()
+        oracle.sum_points_mt(so, x, y, z, tab, nth)
+        dt = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": float(npts) * nh / dt, "unit": UNIT, "cores": nth, "kind": "port",
+                               "sample": f"the whole workload, {dt:.1f} s (FP32 restatement, {nth} threads)"}
+    return out
+
+
+def run_configs(args, peaks, clocks):
+    """Configurations 1, 2 and 5 (the batched configuration has its own leg)."""
+    import torch
+    res = {}
+    legs = args.configs.split(",") if args.configs else []
+    if "1" in legs:
+        res["config1"] = _structured_leg(CONFIG1, ["direct", "tc"], steps=min(args.steps, 10), e2e_steps=5,
+                                         peaks=peaks, clocks=clocks, cpu_full=True, e2e_form="direct")
+        torch.cuda.empty_cache()
+    if "2" in legs:
+        res["config2"] = _points_leg(CONFIG2, steps=min(args.steps, 10), e2e_steps=3, clocks=clocks)
+        torch.cuda.empty_cache()
+    if "5" in legs:
+        res["config5"] = _structured_leg(CONFIG5, ["tc"], steps=min(args.steps, 3), e2e_steps=2, peaks=peaks,
+                                         clocks=clocks)
+        torch.cuda.empty_cache()
+    return res
+
+
 def run_b200(args, w):
     import torch
     import torch.distributed as dist
@@ -411,35 +657,73 @@ def run_b200(args, w):
     k_avg_s = float(np.mean(kernel_ms)) / 1e3
     k_avg_s = max_over_ranks(k_avg_s)
 
-    # Accuracy of the tensor-core field: FP64 oracle and FP32 restatement at
-    # sampled points (rank 0), normalised by the field's standard deviation.
+    # Accuracy of the tensor-core field (rank 0): every point against the FP64
+    # sum over the identical harmonics (on the GPU, oracle/gpu_fp64.py), and at
+    # sampled points against the CPU FP64 oracle and FP32 restatement, all
+    # normalised by the field's standard deviation.
     acc = None
     if rank == 0:
         import oracle
+        from oracle import gpu_fp64
         op = oracle.params(nc=nc, fc=fc, **kw)
         so = oracle.setup(op)
+        full = gpu_fp64.compare_structured(field, so, fs, n, ds, tab)
         rng = np.random.default_rng(0)
         idx = np.sort(rng.choice(npts, size=384, replace=False)).astype(np.int64)
-        f_all = field.double()
-        fstd = float(f_all.std().item())
+        fstd = full["std_ref"]
         got = field[torch.from_numpy(idx).cuda()].cpu().numpy().astype(np.float64)
         r64 = oracle.sum_structured(so, fs, n, ds, tab, idx=idx, f64=True)
         r32 = oracle.sum_structured(so, fs, n, ds, tab, idx=idx)
-        acc = {"points": int(len(idx)), "rel_rms_vs_fp64": float(np.sqrt(np.mean((got - r64) ** 2)) / fstd),
-               "max_abs_vs_fp64": float(np.max(np.abs(got - r64))),
-               "rel_rms_fp32_restatement_vs_fp64": float(np.sqrt(np.mean((r32 - r64) ** 2)) / fstd),
-               "field_std": fstd}
+        acc = {"full_field": {k: full[k] for k in ("rel_rms", "max_abs", "std_ref", "points")},
+               "rel_rms_vs_fp64": full["rel_rms"], "max_abs_vs_fp64": full["max_abs"],
+               "sampled_cpu_oracle": {"points": int(len(idx)),
+                                      "rel_rms_vs_fp64": float(np.sqrt(np.mean((got - r64) ** 2)) / fstd),
+                                      "max_abs_vs_fp64": float(np.max(np.abs(got - r64))),
+                                      "rel_rms_fp32_restatement_vs_fp64":
+                                          float(np.sqrt(np.mean((r32 - r64) ** 2)) / fstd)}}
 
-    # FP32 direct sum on the same grid over the first DIRECT_HARM harmonics.
-    dh = min(DIRECT_HARM, nh)
-    d_ms = []
-    for it in range(3):
-        sb.check(sb.lib.scarf_srm_direct_structured(ctypes.byref(s), i3(fs), i3(n), ds,
-                                                    ctypes.c_void_p(d_tab.data_ptr()), dh,
-                                                    ctypes.c_void_p(field.data_ptr()), sptr))
-        if it:
-            d_ms.append(float(sb.lib.scarf_last_kernel_ms()))
-    direct_rate = npts * dh / (np.mean(d_ms) / 1e3)
+    # Operand precision of the tensor-core form: every split (FP16 / BF16
+    # hi-lo parts, 3 or 2 products) timed on the same grid and scored over the
+    # whole field against FP64; the default (FP16, 3 products) is the one that
+    # meets 1e-5.
+    precision = None
+    if rank == 0 and not args.no_precision:
+        precision = []
+        for otype, terms in ((0, 3), (1, 3), (0, 2), (1, 2)):
+            sb.set_tc_precision(otype, terms)
+            try:
+                pb = sb.tc_workspace_bytes(3, n, nh)
+                pwork = torch.empty(pb, dtype=torch.uint8, device="cuda")
+
+                def plaunch():
+                    sb.check(sb.lib.scarf_srm_tc_structured(ctypes.byref(s), i3(fs), i3(n), ds,
+                                                            ctypes.c_void_p(d_tab.data_ptr()), nh,
+                                                            ctypes.c_void_p(field.data_ptr()),
+                                                            ctypes.c_void_p(pwork.data_ptr()), pb, sptr))
+                pms = _kernel_times(plaunch, 3)
+                torch.cuda.synchronize()
+                pf = gpu_fp64.compare_structured(field, so, fs, n, ds, tab)
+                precision.append({"operands": ["fp16", "bf16"][otype], "terms": terms,
+                                  "kernel_ms": float(np.mean(pms)),
+                                  "value": float(npts) * nh / (np.mean(pms) / 1e3),
+                                  "rel_rms_vs_fp64": pf["rel_rms"], "max_abs_vs_fp64": pf["max_abs"],
+                                  "meets_1e-5": bool(pf["rel_rms"] <= 1e-5)})
+                del pwork
+            finally:
+                sb.set_tc_precision(0, 3)
+
+    # FP32 direct sum on the same grid and the same harmonics (one warm-up
+    # launch over the first DIRECT_HARM harmonics, then the whole table).
+    sb.check(sb.lib.scarf_srm_direct_structured(ctypes.byref(s), i3(fs), i3(n), ds, ctypes.c_void_p(d_tab.data_ptr()),
+                                                min(DIRECT_HARM, nh), ctypes.c_void_p(field.data_ptr()), sptr))
+    sb.check(sb.lib.scarf_srm_direct_structured(ctypes.byref(s), i3(fs), i3(n), ds, ctypes.c_void_p(d_tab.data_ptr()),
+                                                nh, ctypes.c_void_p(field.data_ptr()), sptr))
+    d_ms = [float(sb.lib.scarf_last_kernel_ms())]
+    direct_rate = npts * nh / (np.mean(d_ms) / 1e3)
+    direct_acc = None
+    if rank == 0:
+        dfull = gpu_fp64.compare_structured(field, so, fs, n, ds, tab)
+        direct_acc = {k: dfull[k] for k in ("rel_rms", "max_abs", "std_ref", "points")}
 
     # End to end through the public C ABI (scarf_execute), pinned host field.
     del work
@@ -471,14 +755,28 @@ def run_b200(args, w):
         from scarf3d_b200.distributed import merge_stats_across_ranks
         merge_stats_across_ranks(float(stats[2]) ** 2, float(stats[3]), npts)
     e2e_value = work_total / t_e2e
+    # The same calls into a pageable (malloc'd) host field, as the reference's
+    # own C callers allocate it.
+    pageable = np.empty(npts, np.float32)
+    pageable[:] = 0.0  # touch every page before timing, as a caller's array would be
+    pptr = ctypes.c_void_p(pageable.ctypes.data)
+    sb.check(sb.lib.scarf_execute_ex(w["seed"], pptr, sptr_stats, 0))
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        sb.check(sb.lib.scarf_execute_ex(w["seed"], pptr, sptr_stats, 0))
+    t_e2e_pageable = max_over_ranks(time.perf_counter() - t0)
+    pageable_ok = bool(np.array_equal(pageable, host.numpy()))
+    del pageable
     sb.scarf_finalize()
 
     clocks = clk.summary()
-    peak, peak_kind = pick_peak(clocks)
+    peak, peak_sustained, peak_kind = pick_peak(clocks)
     flops_launch = float(npts) * nh * FLOP_PER_PTHARM
     achieved = flops_launch / k_avg_s / 1e12
     traffic = profile_traffic()
     batched = run_batched(args) if (world == 1 and not args.no_batched) else None
+    configs = run_configs(args, load_peaks(), clocks) if world == 1 else None
     if rank == 0:
         cpu = cpu_baseline_sample(w) if world == 1 else None
         line = {
@@ -497,16 +795,25 @@ def run_b200(args, w):
                        "parallelism": f"z-slabs x{world}"},
             "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                          "frac": achieved / peak, "traffic": traffic,
-                         "peak_kind": peak_kind,
+                         "peak_kind": peak_kind, "peak_sustained": peak_sustained,
+                         "frac_of_sustained": achieved / peak_sustained,
                          "kernel": "srm_tc_kernel", "kernel_ms": k_avg_s * 1e3,
                          "flop_per_launch": flops_launch},
-            "direct_sum": {"value": direct_rate, "unit": UNIT, "harmonics_timed": dh,
-                           "kernel_ms": float(np.mean(d_ms)), "tc_over_direct": value / direct_rate},
+            "direct_sum": {"value": direct_rate, "unit": UNIT, "harmonics_timed": nh,
+                           "kernel_ms": float(np.mean(d_ms)), "tc_over_direct": value / direct_rate,
+                           "roofline": _direct_roofline(direct_rate, clocks.get("sm_max_mhz")),
+                           "accuracy_vs_fp64_full_field": direct_acc},
             "accuracy": acc,
+            "precision_plans": precision,
             "batched": batched,
+            "configs": configs,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(nh * 20),
                     "d2h_bytes_per_step": int(npts * 4 + 8), "ms_per_step": t_e2e / args.steps * 1e3,
-                    "host_sampling_ms": float(np.mean(host_s)) * 1e3, "device_ms": float(np.mean(device_s)) * 1e3},
+                    "host_sampling_ms": float(np.mean(host_s)) * 1e3, "device_ms": float(np.mean(device_s)) * 1e3,
+                    "host_memory": "page-locked",
+                    "pageable": {"value": work_total / t_e2e_pageable, "unit": UNIT,
+                                 "ms_per_step": t_e2e_pageable / args.steps * 1e3,
+                                 "host_memory": "pageable (numpy, malloc'd)", "field_equals_pinned": pageable_ok}},
             "gpu_launches": 3 * args.steps,
             "clocks": clocks,
             "cpu_baseline": cpu,
@@ -526,6 +833,9 @@ def main():
     ap.add_argument("--nharm", type=int, default=None)
     ap.add_argument("--no-batched", action="store_true", help="skip the 256-field batched measurement")
     ap.add_argument("--no-autotune", action="store_true", help="default plans instead of autotuned ones")
+    ap.add_argument("--no-precision", action="store_true", help="skip the operand-precision comparison")
+    ap.add_argument("--configs", default="1,2,5",
+                    help="other configurations to measure (comma list of 1, 2, 5; empty to skip)")
     args = ap.parse_args()
     w = dict(WORKLOAD)
     if args.grid:

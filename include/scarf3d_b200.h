@@ -129,6 +129,16 @@ int scarf_set_output_overlap(int items_per_slab);
 #define SCARF_TC_SINGLE 1
 #define SCARF_TC_SINGLE_TMEM_A 2
 int scarf_set_tc_variant(int variant);
+/* Operand precision of the tensor-core form for plans made afterwards (no
+ * counterpart in the reference, which sums in FP32). Each FP32 operand is
+ * split into hi + lo 16-bit parts, operand_type SCARF_TC_FP16 (default) or
+ * SCARF_TC_BF16, and terms = 3 (hi.hi + hi.lo + lo.hi, default) or 2 (hi.hi +
+ * lo.hi) products are accumulated in FP32. The default is the one whose
+ * measured error meets 1e-5 rel-RMS; the others exist to measure the
+ * trade-off. */
+#define SCARF_TC_FP16 0
+#define SCARF_TC_BF16 1
+int scarf_set_tc_precision(int operand_type, int terms);
 
 /* Autotuning of the tensor-core form. No counterpart in the reference (its
  * SRM has one CPU code path). A tuning times every candidate plan -- kernel

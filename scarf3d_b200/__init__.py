@@ -36,7 +36,8 @@ EXPORTED_SYMBOLS = (
     "scarf_set_uniform_source", "scarf_set_stream", "scarf_set_host_threads", "scarf_set_kernel_timing",
     "scarf_last_kernel_ms", "scarf_set_device_memory_cap", "scarf_device_memory_in_use",
     "scarf_release_device_memory",
-    "scarf_selftest_wait_limit", "scarf_set_tc_chunk", "scarf_set_tc_variant", "scarf_set_output_overlap",
+    "scarf_selftest_wait_limit", "scarf_set_tc_chunk", "scarf_set_tc_variant", "scarf_set_tc_precision",
+    "scarf_set_output_overlap",
     "scarf_execute_ex",
     "scarf_srm_compute_setup", "scarf_srm_sample", "scarf_srm_sample_device", "scarf_srm_sample_device_batch",
     "scarf_set_sampler",
@@ -131,6 +132,7 @@ def _load() -> ctypes.CDLL:
         "scarf_selftest_wait_limit": (c_int, [c_int, ctypes.POINTER(c_int), ctypes.POINTER(ctypes.c_double)]),
         "scarf_set_tc_chunk": (c_int, [c_int]),
         "scarf_set_tc_variant": (c_int, [c_int]),
+        "scarf_set_tc_precision": (c_int, [c_int, c_int]),
         "scarf_set_output_overlap": (c_int, [c_int]),
         "scarf_execute_ex": (c_int, [c_int, c_void_p, fp, c_int]),
         "scarf_srm_compute_setup": (c_int, [ctypes.POINTER(SrmParams), ctypes.POINTER(SrmSetup)]),
@@ -410,6 +412,15 @@ def set_tc_variant(variant: int):
     """Tensor-core kernel form for plans made afterwards: TC_SINGLE (default),
     TC_PAIR (CTA pairs with cta_group::2 MMAs) or TC_SINGLE_TMEM_A."""
     check(lib.scarf_set_tc_variant(int(variant)))
+
+
+TC_FP16, TC_BF16 = 0, 1
+
+
+def set_tc_precision(operand_type: int = 0, terms: int = 3):
+    """Operand split of the tensor-core form for plans made afterwards:
+    TC_FP16 (default) or TC_BF16 hi/lo parts, 3 (default) or 2 products."""
+    check(lib.scarf_set_tc_precision(int(operand_type), int(terms)))
 
 
 def set_device_memory_cap(nbytes: int):

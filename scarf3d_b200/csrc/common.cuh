@@ -6,6 +6,8 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include "srm_kernels.h"
+
 #if defined(__CUDA_ARCH__) && (__CUDA_ARCH__ < 1000)
 #error "scarf3d_b200 device code targets sm_100a only"
 #endif
@@ -393,12 +395,62 @@ __device__ __forceinline__ uint64_t umma_smem_desc(uint32_t saddr, uint32_t lbo_
 }
 
 // Instruction descriptor, kind::f16: A=B=F16, D=F32, both K-major.
-__host__ __device__ constexpr uint32_t umma_idesc_f16_f32(uint32_t m, uint32_t n) {
-  return (1u << 4)             // D format: F32
-         | (0u << 7)           // A format: F16
-         | (0u << 10)          // B format: F16
-         | ((n >> 3) << 17)    // N / 8
-         | ((m >> 4) << 24);   // M / 16
+__host__ __device__ constexpr uint32_t umma_idesc_f16_f32(uint32_t m, uint32_t n, bool bf16 = false) {
+  return (1u << 4)                    // D format: F32
+         | ((bf16 ? 1u : 0u) << 7)    // A format: F16 (0) or BF16 (1)
+         | ((bf16 ? 1u : 0u) << 10)   // B format: the same type as A
+         | ((n >> 3) << 17)           // N / 8
+         | ((m >> 4) << 24);          // M / 16
+}
+
+// ------------------------------------------------------------- statistics --
+// (count, mean, M2) of a set of field values in FP64 and the pairwise merge of
+// Chan et al. (the update scarflib_common.f90:823-875 applies across ranks),
+// used by the summation kernels to record per-tile statistics that one small
+// kernel merges in record order (deterministic, independent of scheduling).
+using Moments = StatRecord;  // srm_kernels.h: the records' layout
+
+__host__ __device__ __forceinline__ Moments moments_merge(const Moments& a, const Moments& b) {
+  if (b.n == 0.0) return a;
+  if (a.n == 0.0) return b;
+  const double n = a.n + b.n;
+  const double d = b.mean - a.mean;
+  Moments r;
+  r.n = n;
+  r.mean = a.mean + d * (b.n / n);
+  r.m2 = a.m2 + b.m2 + d * d * (a.n * (b.n / n));
+  return r;
+}
+
+// Moments of values accumulated as sums about a shift (the first value), so
+// that a large common offset does not cancel: s1 = sum(x - shift),
+// s2 = sum((x - shift)^2) over n values.
+__device__ __forceinline__ Moments moments_from_shifted(double n, double shift, double s1, double s2) {
+  Moments m;
+  m.n = n;
+  if (n == 0.0) {
+    m.mean = 0.0;
+    m.m2 = 0.0;
+    return m;
+  }
+  m.mean = shift + s1 / n;
+  m.m2 = fmax(s2 - s1 * (s1 / n), 0.0);
+  return m;
+}
+
+// Merge over the 32 lanes of a warp in a fixed tree order (lane 0 holds the
+// result): at each level lanes [0, o) take in lanes [o, 2o).
+__device__ __forceinline__ Moments warp_moments(Moments m) {
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    Moments b;
+    b.n = __shfl_down_sync(0xffffffffu, m.n, o);
+    b.mean = __shfl_down_sync(0xffffffffu, m.mean, o);
+    b.m2 = __shfl_down_sync(0xffffffffu, m.m2, o);
+    if (lane < o) m = moments_merge(m, b);
+  }
+  return m;
 }
 
 }  // namespace scarf

@@ -124,7 +124,7 @@ struct DeviceBuf {
 
 struct Resources {
   int device = -1;
-  DeviceBuf status, stats, table, field, coords, work, slab_cnt;
+  DeviceBuf status, stats, table, field, coords, work, slab_cnt, statrec, poi;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr, evk0 = nullptr, evk1 = nullptr, evs = nullptr;
   cudaStream_t copy_stream = nullptr;  // non-blocking: runs beside the legacy stream too
   int* slab_flags = nullptr;           // host-mapped, written by the kernel
@@ -148,6 +148,8 @@ struct Resources {
     field.release();
     coords.release();
     work.release();
+    statrec.release();
+    poi.release();
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
     ev0 = ev1 = nullptr;
@@ -280,17 +282,97 @@ scarf_srm_params params_from_object(int seed) {
   return p;
 }
 
+// FIM (method 0) for the global object: scarf3d_structured_fim /
+// scarf3d_unstructured_fim (scarflib_fim.f90:141-1104) on one device
+// (fim.cu). The internal grid covers nc..fc; statistics, rescale and taper
+// act on it, as the reference's do, before the external points take their
+// nearest internal values. Point sets are not tapered unless
+// SCARF_TAPER_UNSTRUCTURED is set: initialize_unstructured drops the POIs
+// (scarflib.f90:273,283), for either method.
+int fim_execute_impl(int seed, float* field, float stats[8], int flags) {
+  cudaStream_t st = g_cfg.stream;
+  FimInputs in{};
+  in.ndim = g_obj.cl[2] > 0.0f ? 3 : 2;  // scarflib_fim.f90:770-774
+  in.acf = g_obj.acf;
+  in.pad = g_obj.pad;
+  in.rescale = g_obj.rescale;
+  in.seed = seed;
+  in.ds = g_obj.ds;
+  in.dh = g_obj.dh;
+  in.sigma = g_obj.sigma;
+  in.hurst = g_obj.hurst;
+  in.mute = g_obj.mute;
+  in.taper = g_obj.taper;
+  for (int c = 0; c < 3; ++c) {
+    in.cl[c] = g_obj.cl[c];
+    in.nc[c] = g_obj.nc[c];
+    in.fc[c] = g_obj.fc[c];
+  }
+  if (in.acf != 0 && in.acf != 1) return fail(SCARF_ERR_ARG, "FIM: acf must be 0 (von Karman) or 1 (Gaussian)");
+  in.structured = g_obj.structured ? 1 : 0;
+  long long npts;
+  if (g_obj.structured) {
+    npts = 1;
+    for (int c = 0; c < 3; ++c) {
+      in.fs[c] = g_obj.fs[c];
+      in.fe[c] = g_obj.fe[c];
+      npts *= g_obj.fe[c] - g_obj.fs[c] + 1;
+    }
+  } else {
+    npts = g_obj.npts;
+  }
+  if (npts <= 0) return fail(SCARF_ERR_ARG, "empty point set");
+  in.npts = npts;
+  const bool taper_ok = g_obj.structured || (flags & SCARF_TAPER_UNSTRUCTURED);
+  if (taper_ok && g_obj.poi && g_obj.npoi > 0) {
+    in.poi = g_obj.poi;
+    in.npoi = g_obj.npoi;
+    in.poi_stride = g_obj.nd;
+  }
+  FimGrid g{};
+  fim_grid(in, &g);
+  for (int c = 0; c < 3; ++c)
+    if (g.npts[c] <= 0) return fail(SCARF_ERR_ARG, "FIM: empty internal grid");
+  const bool on_device = (flags & SCARF_FIELD_ON_DEVICE) || is_device_pointer(field);
+  float* d_field = field;
+  if (!on_device) {
+    SCARF_CUDA(g_res.field.ensure(sizeof(float) * npts));
+    d_field = static_cast<float*>(g_res.field.p);
+  }
+  if (!g_obj.structured) {
+    const size_t stride = (static_cast<size_t>(npts) + 3) / 4 * 4;
+    SCARF_CUDA(g_res.coords.ensure(sizeof(float) * 3 * stride));
+    float* c = static_cast<float*>(g_res.coords.p);
+    SCARF_CUDA(cudaMemcpyAsync(c, g_obj.x, sizeof(float) * npts, cudaMemcpyDefault, st));
+    SCARF_CUDA(cudaMemcpyAsync(c + stride, g_obj.y, sizeof(float) * npts, cudaMemcpyDefault, st));
+    SCARF_CUDA(cudaMemcpyAsync(c + 2 * stride, g_obj.z, sizeof(float) * npts, cudaMemcpyDefault, st));
+    in.d_x = c;
+    in.d_y = c + stride;
+    in.d_z = c + 2 * stride;
+  }
+  SCARF_CUDA(g_res.work.ensure(fim_workspace_bytes(g, in.npoi)));
+  const char* what = "";
+  const cudaError_t e = fim_run(in, g, g_res.work.p, d_field, stats, st, &what);
+  if (e != cudaSuccess) return fail(SCARF_ERR_CUDA, "FIM: %s: %s", what, cudaGetErrorString(e));
+  if (!on_device) {
+    SCARF_CUDA(cudaMemcpyAsync(field, d_field, sizeof(float) * npts, cudaMemcpyDeviceToHost, st));
+    SCARF_CUDA(cudaStreamSynchronize(st));
+  }
+  return SCARF_OK;
+}
+
 // The whole SRM execute (scarflib_srm.f90:505-929 / :105-499) for the global
 // object. field: host or device memory of the local block / point set.
 int execute_impl(int seed, float* field, float stats[8], int flags) {
   if (!g_obj.ready) return fail(SCARF_ERR_STATE, "scarf_execute called before scarf_*_initialize");
-  if (g_obj.method != 1) return fail(SCARF_ERR_UNSUPPORTED, "only the SRM method (method = 1) is implemented");
   if (!field || !stats) return fail(SCARF_ERR_ARG, "field and stats must not be NULL");
   int rc = ensure_resources();
   if (rc) return rc;
   scarf::take_device_alloc_failure();
   cudaStream_t st = g_cfg.stream;
   for (int i = 0; i < 8; ++i) stats[i] = 0.0f;
+  if (g_obj.method == 0) return fim_execute_impl(seed, field, stats, flags);
+  if (g_obj.method != 1) return fail(SCARF_ERR_UNSUPPORTED, "method must be 0 (FIM) or 1 (SRM)");
 
   // Host: setup scalars and harmonic table.
   const double th0 = now_s();
@@ -350,6 +432,17 @@ int execute_impl(int seed, float* field, float stats[8], int flags) {
     }
   } copy_join;
   bool copied_out = false;  // field already on its way to the host (slab copies)
+  // Statistics records written by the summation kernel (its epilogue reads
+  // back what it stored), merged below: no further pass over the field.
+  StatRecord* d_rec = nullptr;
+  long long nrec = 0;
+  auto want_records = [&](long long count) -> int {
+    if (count <= 0) return SCARF_OK;
+    SCARF_CUDA(g_res.statrec.ensure(sizeof(StatRecord) * static_cast<size_t>(count)));
+    d_rec = static_cast<StatRecord*>(g_res.statrec.p);
+    nrec = count;
+    return SCARF_OK;
+  };
   if (g_obj.structured) {
     const bool use_tc = (g_cfg.form != SCARF_FORM_DIRECT);
     TcPlan plan{};
@@ -371,8 +464,10 @@ int execute_impl(int seed, float* field, float stats[8], int flags) {
         sig.d_cnt = static_cast<int*>(g_res.slab_cnt.p);
         sig.flag_dev = g_res.slab_flags_dev;
       }
+      rc = want_records(tc_stat_records(plan));
+      if (rc) return rc;
       SCARF_CUDA(launch_tc_structured(s, g_obj.fs, n, p.ds, d_table, nh, d_field, g_res.work.p, plan, d_status, st,
-                                      kernel_ev0(), kernel_ev1(), overlap ? &sig : nullptr));
+                                      kernel_ev0(), kernel_ev1(), overlap ? &sig : nullptr, d_rec));
       if (overlap) {
         copy_join.active = true;
         rc = copy_slabs_out(plan, sig, d_field, field, st);
@@ -380,8 +475,10 @@ int execute_impl(int seed, float* field, float stats[8], int flags) {
         copied_out = true;
       }
     } else if (nh > 0) {
+      rc = want_records(direct_stat_records(npts));
+      if (rc) return rc;
       if (kernel_ev0()) SCARF_CUDA(cudaEventRecord(kernel_ev0(), st));
-      SCARF_CUDA(launch_direct_structured(s, g_obj.fs, n, p.ds, d_table, nh, d_field, d_status, st));
+      SCARF_CUDA(launch_direct_structured(s, g_obj.fs, n, p.ds, d_table, nh, d_field, d_status, st, d_rec));
       if (kernel_ev1()) SCARF_CUDA(cudaEventRecord(kernel_ev1(), st));
     } else {
       SCARF_CUDA(cudaMemsetAsync(d_field, 0, sizeof(float) * npts, st));
@@ -399,20 +496,27 @@ int execute_impl(int seed, float* field, float stats[8], int flags) {
     dy = c + stride;
     dz = c + 2 * stride;
     if (nh > 0) {
+      rc = want_records(direct_stat_records(npts));
+      if (rc) return rc;
       if (kernel_ev0()) SCARF_CUDA(cudaEventRecord(kernel_ev0(), st));
-      SCARF_CUDA(launch_direct_points(s, dx, dy, dz, npts, d_table, nh, d_field, d_status, st));
+      SCARF_CUDA(launch_direct_points(s, dx, dy, dz, npts, d_table, nh, d_field, d_status, st, d_rec));
       if (kernel_ev1()) SCARF_CUDA(cudaEventRecord(kernel_ev1(), st));
     } else {
       SCARF_CUDA(cudaMemsetAsync(d_field, 0, sizeof(float) * npts, st));
     }
   }
   // Statistics (scarflib_srm.f90:877-895): single set, so the Chan merge
-  // returns (var, mean) unchanged; std = sqrt(var) in FP32. They are
-  // enqueued behind the sum, and the sum's status word comes back with them
-  // in one synchronisation (after a failed sum the statistics are dropped).
+  // returns (var, mean) unchanged; std = sqrt(var) in FP32. The summation
+  // kernel recorded per-tile moments as it stored the field; one small
+  // kernel merges them (a field without harmonics takes the two FP64 passes
+  // instead). The sum's status word comes back with them in one
+  // synchronisation (after a failed sum the statistics are dropped).
   double* d_part = static_cast<double*>(g_res.stats.p);
   float* d_out = reinterpret_cast<float*>(static_cast<char*>(g_res.stats.p) + stats_partials_bytes(0));
-  SCARF_CUDA(launch_field_stats(d_field, npts, d_part, d_out, st));
+  if (d_rec)
+    SCARF_CUDA(launch_stats_records(d_rec, nrec, d_out, st));
+  else
+    SCARF_CUDA(launch_field_stats(d_field, npts, d_part, d_out, st));
   float mv[2];
   int dev_status = 0;
   SCARF_CUDA(cudaMemcpyAsync(&dev_status, d_status, sizeof(int), cudaMemcpyDeviceToHost, st));
@@ -426,21 +530,41 @@ int execute_impl(int seed, float* field, float stats[8], int flags) {
   stats[2] = sqrtf(mv[1]);
   stats[3] = mv[0];
 
-  // Rescale (:897-912) and taper (:920-925).
-  if (p.rescale == 1) {
-    SCARF_CUDA(launch_rescale(d_field, npts, p.sigma, stats[2], stats[3], st));
-    stats[2] = p.sigma;
-    stats[3] = 0.0f;
-  }
-  if (tapering) {
-    for (int q = 0; q < g_obj.npoi; ++q) {
-      float pt[3] = {0.0f, 0.0f, 0.0f};
-      for (int c = 0; c < s.ndim; ++c) pt[c] = g_obj.poi[g_obj.nd * q + c];
-      if (g_obj.structured)
-        SCARF_CUDA(launch_taper_structured(d_field, g_obj.fs, n, p.ds, pt, g_obj.mute, g_obj.taper, st));
-      else
-        SCARF_CUDA(launch_taper_points(d_field, dx, dy, dz, npts, pt, g_obj.mute, g_obj.taper, st));
+  // Rescale (:897-912) and taper (:920-925), in one pass over the field.
+  std::vector<float> poi3;
+  if (p.rescale == 1 || tapering) {
+    FinalizeArgs fa{};
+    if (p.rescale == 1) {
+      fa.rescale = 1;
+      fa.scaling = p.sigma / stats[2];  // scarflib_srm.f90:899, FP32 on the host
+      fa.mean = stats[3];
+      stats[2] = p.sigma;
+      stats[3] = 0.0f;
     }
+    if (tapering) {
+      poi3.assign(3 * static_cast<size_t>(g_obj.npoi), 0.0f);
+      for (int q = 0; q < g_obj.npoi; ++q)
+        for (int c = 0; c < s.ndim; ++c) poi3[3 * q + c] = g_obj.poi[g_obj.nd * q + c];
+      SCARF_CUDA(g_res.poi.ensure(sizeof(float) * poi3.size()));
+      SCARF_CUDA(cudaMemcpyAsync(g_res.poi.p, poi3.data(), sizeof(float) * poi3.size(), cudaMemcpyHostToDevice, st));
+      fa.d_poi = static_cast<const float*>(g_res.poi.p);
+      fa.npoi = g_obj.npoi;
+      fa.mute = g_obj.mute;
+      fa.taper = g_obj.taper;
+      if (g_obj.structured) {
+        fa.n0 = n[0];
+        fa.n1 = n[1];
+        fa.o0 = g_obj.fs[0] - 1;
+        fa.o1 = g_obj.fs[1] - 1;
+        fa.o2 = g_obj.fs[2] - 1;
+        fa.dh = p.ds;
+      } else {
+        fa.d_x = dx;
+        fa.d_y = dy;
+        fa.d_z = dz;
+      }
+    }
+    SCARF_CUDA(launch_finalize_field(d_field, npts, fa, st));
   }
   if (copied_out) {
     // Device time ends with the last slab copy.
@@ -1124,6 +1248,14 @@ int scarf_set_tc_variant(int variant) {
     return fail(SCARF_ERR_ARG, "unknown tensor-core variant %d", variant);
   std::lock_guard<std::mutex> lk(g_mu);
   tc_set_variant(variant);
+  return SCARF_OK;
+}
+
+int scarf_set_tc_precision(int operand_type, int terms) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (!tc_set_precision(operand_type, terms))
+    return fail(SCARF_ERR_ARG, "tensor-core precision: operand type %d (0 FP16, 1 BF16), terms %d (2 or 3)",
+                operand_type, terms);
   return SCARF_OK;
 }
 

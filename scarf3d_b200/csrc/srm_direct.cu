@@ -37,6 +37,8 @@ struct DirectArgs {
   const float* x;
   const float* y;
   const float* z;
+  // optional: one statistics record per block (count, mean, M2 of its stored values)
+  Moments* stats;
 };
 
 __device__ __forceinline__ void rotate(const DirectArgs& A, float x, float y, float z, float& p1, float& p2,
@@ -156,13 +158,42 @@ __global__ void __launch_bounds__(kThreads) srm_direct_kernel(const DirectArgs A
     for (int q = 0; q < kPts; ++q)
       if (p0 + q < A.npts) dst[q] = out[q];
   }
+  if (A.stats) {
+    // Statistics of the stored values (FP64): thread, warp (fixed tree), then
+    // the block's warps in order; one record per block.
+    __shared__ Moments s_warp[kThreads / 32];
+    double s1 = 0.0, s2 = 0.0, cnt = 0.0;
+    const double shift = p0 < A.npts ? static_cast<double>(out[0]) : 0.0;
+#pragma unroll
+    for (int q = 0; q < kPts; ++q) {
+      if (p0 + q < A.npts) {
+        const double d = static_cast<double>(out[q]) - shift;
+        s1 += d;
+        s2 = fma(d, d, s2);
+        cnt += 1.0;
+      }
+    }
+    Moments m = warp_moments(moments_from_shifted(cnt, shift, s1, s2));
+    if ((tid & 31) == 0) s_warp[tid >> 5] = m;
+    __syncthreads();
+    if (tid == 0) {
+      Moments b = s_warp[0];
+      for (int w = 1; w < kThreads / 32; ++w) b = moments_merge(b, s_warp[w]);
+      A.stats[blockIdx.x] = b;
+    }
+  }
 }
 
 }  // namespace
 
+long long direct_stat_records(long long npts) {
+  const long long per_block = static_cast<long long>(kThreads) * kPts;
+  return (npts + per_block - 1) / per_block;
+}
+
 cudaError_t launch_direct_structured(const scarf_srm_setup& s, const int fs[3], const int n[3], float ds,
                                      const float* d_table, int nh, float* d_field, int* d_status,
-                                     cudaStream_t stream) {
+                                     cudaStream_t stream, StatRecord* d_stats) {
   DirectArgs A{};
   for (int i = 0; i < 9; ++i) A.m[i] = s.m[i];
   for (int i = 0; i < 3; ++i) A.bar[i] = s.bar[i];
@@ -178,6 +209,7 @@ cudaError_t launch_direct_structured(const scarf_srm_setup& s, const int fs[3], 
   A.off0 = fs[0] - 2;
   A.off1 = fs[1] - 2;
   A.off2 = fs[2] - 2;
+  A.stats = d_stats;
   const long long per_block = static_cast<long long>(kThreads) * kPts;
   const long long blocks = (A.npts + per_block - 1) / per_block;
   if (blocks <= 0) return cudaSuccess;
@@ -187,7 +219,7 @@ cudaError_t launch_direct_structured(const scarf_srm_setup& s, const int fs[3], 
 
 cudaError_t launch_direct_points(const scarf_srm_setup& s, const float* d_x, const float* d_y, const float* d_z,
                                  long long npts, const float* d_table, int nh, float* d_field, int* d_status,
-                                 cudaStream_t stream) {
+                                 cudaStream_t stream, StatRecord* d_stats) {
   DirectArgs A{};
   for (int i = 0; i < 9; ++i) A.m[i] = s.m[i];
   for (int i = 0; i < 3; ++i) A.bar[i] = s.bar[i];
@@ -200,6 +232,7 @@ cudaError_t launch_direct_points(const scarf_srm_setup& s, const float* d_x, con
   A.x = d_x;
   A.y = d_y;
   A.z = d_z;
+  A.stats = d_stats;
   const long long per_block = static_cast<long long>(kThreads) * kPts;
   const long long blocks = (npts + per_block - 1) / per_block;
   if (blocks <= 0) return cudaSuccess;

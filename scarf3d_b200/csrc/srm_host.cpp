@@ -57,6 +57,8 @@ const PowTables& pow_tables() {
   static const PowTables t;
   return t;
 }
+}  // namespace
+
 // The device's split of the same transform: g^k, g^(k 2^11), g^(k 2^22).
 std::vector<uint32_t> device_pow_tables() {
   std::vector<uint32_t> w;
@@ -73,7 +75,6 @@ std::vector<uint32_t> device_pow_tables() {
   }
   return w;
 }
-}  // namespace
 
 uint32_t Yarn2::output(uint64_t r) {
   if (r == 0) return 0u;

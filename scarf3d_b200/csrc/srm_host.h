@@ -39,6 +39,10 @@ class Yarn2 {
   uint64_t r0 = 0, r1 = 1;  // r0 = newest state word
 };
 
+// Output-transform tables of the device generator (yarn2.cuh): g^k,
+// g^(k 2^11), g^(k 2^22) mod m for k < 2048, 2048, 512.
+std::vector<uint32_t> device_pow_tables();
+
 // Spectral integrand of the SRM (scarflib_srm.f90:975-995 with
 // psdf.f90:50-90): x * psd(float(x)) [* x in 3D], FP32 spectrum, FP64 rest.
 double srm_fn(double x, int ndim, int acf, float nu);

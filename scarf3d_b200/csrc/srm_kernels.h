@@ -10,13 +10,23 @@
 
 namespace scarf {
 
+// Statistics records written by the summation kernels when asked for: one
+// (count, mean, M2) triple (FP64) per epilogue warp and work item of the
+// tensor-core form, or per block of the direct form, merged in record order by
+// launch_stats_records (srm_stats.cu). Layout of struct Moments (common.cuh).
+struct StatRecord {
+  double n, mean, m2;
+};
+
 // ---- direct sum (srm_direct.cu) ----
+// d_stats (optional): direct_stat_records(npts) records.
+long long direct_stat_records(long long npts);
 cudaError_t launch_direct_structured(const scarf_srm_setup& s, const int fs[3], const int n[3], float ds,
                                      const float* d_table, int nh, float* d_field, int* d_status,
-                                     cudaStream_t stream);
+                                     cudaStream_t stream, StatRecord* d_stats = nullptr);
 cudaError_t launch_direct_points(const scarf_srm_setup& s, const float* d_x, const float* d_y, const float* d_z,
                                  long long npts, const float* d_table, int nh, float* d_field, int* d_status,
-                                 cudaStream_t stream);
+                                 cudaStream_t stream, StatRecord* d_stats = nullptr);
 
 // ---- factorised tensor-core form (srm_tc.cu) ----
 // Geometry of one structured field in the factorised form:
@@ -37,6 +47,8 @@ struct TcPlan {
   int tmem_a;            // 1: A operand generated into tensor memory (ntile_n <= 192)
   int pair;              // 1: CTA-pair form (M = 256 over two SMs, each holding half of B)
   int pair_i;            // pairs split along i (when bj == 1) instead of j
+  int bf16;              // operands split into BF16 (else FP16)
+  int terms;             // split products per K step: 3, or 2 (the A-hi x B-lo product dropped)
   int bix, bjx;          // item grid (bi x bj, halved along the pair axis, rounded up)
   int ax_r, ax_s, ax_c;  // physical axis (0 x, 1 y, 2 z) of i (row-fast), j (row-slow), k (column)
   long long sr, ss, sc;  // field strides of i, j, k in elements
@@ -48,6 +60,9 @@ constexpr int kTcVariantPair = 0;         // cta_group::2 pairs, A in shared mem
 constexpr int kTcVariantSingle = 1;       // one CTA per tile, A in shared memory (default)
 constexpr int kTcVariantSingleTmemA = 2;  // one CTA per tile, A in tensor memory
 void tc_set_variant(int v);
+// Operand precision of plans made from now on: FP16 (bf16 = 0) or BF16 split
+// operands, 3 or 2 split products. False for other values.
+bool tc_set_precision(int bf16, int terms);
 int tc_get_variant();
 
 // tj_force > 0 fixes the row tile to (128 / tj_force) x tj_force.
@@ -94,10 +109,13 @@ void tc_slab_layout(const TcPlan& p, int target_items, TcSlabSignal* sig);
 TcSlab tc_slab_extent(const TcPlan& p, const TcSlabSignal& sig, int q);
 
 // Status word at d_status[0]; d_status[1] is used as the work-queue counter.
+// d_stats (optional): tc_stat_records(plan) records of the stored field.
+long long tc_stat_records(const TcPlan& plan);
 cudaError_t launch_tc_structured(const scarf_srm_setup& s, const int fs[3], const int n[3], float ds,
                                  const float* d_table, int nh, float* d_field, void* d_work, const TcPlan& plan,
                                  int* d_status, cudaStream_t stream, cudaEvent_t ev_main0 = nullptr,
-                                 cudaEvent_t ev_main1 = nullptr, const TcSlabSignal* slabs = nullptr);
+                                 cudaEvent_t ev_main1 = nullptr, const TcSlabSignal* slabs = nullptr,
+                                 StatRecord* d_stats = nullptr);
 
 // Batched form: many fields in one persistent launch fed by a device work
 // queue. All fields of a batch share one row-tile shape.
@@ -178,13 +196,52 @@ size_t stats_partials_bytes(long long n);
 // results as the reference returns them) to d_out[0..1] (float).
 cudaError_t launch_field_stats(const float* d_field, long long n, double* d_partials, float* d_out,
                                cudaStream_t stream);
-// field = field * (sigma / std) - mean (scarflib_srm.f90:897-912).
-cudaError_t launch_rescale(float* d_field, long long n, float sigma, float std_, float mean, cudaStream_t stream);
-// Structured / point taper for one point of interest
-// (scarflib_common.f90:881-994).
-cudaError_t launch_taper_structured(float* d_field, const int fs[3], const int n[3], float dh, const float poi[3],
-                                    float mute, float taper, cudaStream_t stream);
-cudaError_t launch_taper_points(float* d_field, const float* d_x, const float* d_y, const float* d_z, long long n,
-                                const float poi[3], float mute, float taper, cudaStream_t stream);
+// Merge `count` statistics records in record order (one block, fixed tree)
+// into the FP32 mean and unbiased variance at d_out[0..1], as
+// launch_field_stats reports them.
+cudaError_t launch_stats_records(const StatRecord* d_rec, long long count, float* d_out, cudaStream_t stream);
+// Rescale (when rescale != 0, scarflib_srm.f90:897-912) and the taper of
+// every point of interest (scarflib_common.f90:881-994), in the reference's
+// order, in one pass over the field. d_poi: npoi x 3 floats.
+// Structured fields (d_x null) take coordinates (i + fs - 2) dh from the
+// index; point sets read d_x, d_y, d_z.
+struct FinalizeArgs {
+  int rescale;
+  float scaling, mean;  // field * scaling - mean
+  const float* d_poi;
+  int npoi;
+  float mute, taper;
+  int n0, n1, o0, o1, o2;  // structured: extents and fs - 1
+  float dh;
+  const float *d_x, *d_y, *d_z;
+};
+cudaError_t launch_finalize_field(float* d_field, long long n, const FinalizeArgs& a, cudaStream_t stream);
+
+// ---- FIM, the Fourier integral method (fim.cu) ----
+struct FimInputs {
+  int ndim, acf, pad, rescale, seed;
+  float ds, dh, sigma, hurst, mute, taper;
+  float cl[3], nc[3], fc[3];  // nc/fc: extent of the external points (the internal grid covers it)
+  int structured;             // 1: external grid fs..fe at step ds; 0: the points d_x, d_y, d_z
+  int fs[3], fe[3];
+  const float *d_x, *d_y, *d_z;
+  long long npts;
+  const float* poi;  // host, npoi points of poi_stride floats
+  int npoi, poi_stride;
+};
+// Internal (FFT) grid: points per axis, offset of its first node, and the
+// reference's info(1:2) flags (scarflib_fim.f90:787-818).
+struct FimGrid {
+  int npts[3];
+  float off_axis[3];
+  float info0, info1;
+};
+void fim_grid(const FimInputs& in, FimGrid* g);
+size_t fim_workspace_bytes(const FimGrid& g, int npoi);
+// The whole FIM into the device field of the external points; stats as the
+// reference's info(1:8). d_work: fim_workspace_bytes, 256-byte aligned. On
+// failure *what names the failing step. Synchronises `st`.
+cudaError_t fim_run(const FimInputs& in, const FimGrid& g, void* d_work, float* d_field, float stats[8],
+                    cudaStream_t st, const char** what);
 
 }  // namespace scarf

@@ -4,13 +4,17 @@
 //   mean     = running mean of the FP32 field, returned as FP32   (:780-817)
 //   variance = (s2 - s1^2/n)/(n-1) with x - mu, mu the FP32 mean,
 //              returned as FP32                                   (:694-737)
-// Here both passes are FP64 sums over the field in a fixed, deterministic
-// tree order (per-block partials, then one block); results are rounded to
-// FP32 exactly where the reference rounds them.
+// scarf_execute takes them from per-tile (count, mean, M2) records that the
+// summation kernels write as they store the field, merged here in record
+// order (Chan's pairwise formula, FP64); scarf_field_stats and fields
+// without harmonics take two FP64 passes over the field in a fixed tree
+// order (per-block partials, then one block). Results are rounded to FP32
+// exactly where the reference rounds them. Rescale and taper run as one pass.
 #include <cuda_runtime.h>
 
 #include <cstdint>
 
+#include "common.cuh"
 #include "srm_kernels.h"
 
 namespace scarf {
@@ -97,10 +101,34 @@ __global__ void __launch_bounds__(1024) stats_finish(const double* part, int npa
   }
 }
 
-__global__ void rescale_kernel(float* f, long long n, float scaling, float mean) {
-  const long long stride = static_cast<long long>(gridDim.x) * blockDim.x;
-  for (long long i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride)
-    f[i] = __fsub_rn(__fmul_rn(f[i], scaling), mean);
+// One block merges the statistics records written by a summation kernel:
+// thread t takes a contiguous run of records in order, then the threads'
+// results are merged by a fixed tree in shared memory. FP64 throughout;
+// mean and variance rounded to FP32 once, where the reference rounds them.
+// The record merge gives the variance as M2 / (n - 1), which is the
+// reference's compensated two-pass sum (s2 - s1^2 / n) / (n - 1) about the
+// FP32 mean in exact arithmetic.
+constexpr int kMergeThreads = 1024;
+
+__global__ void __launch_bounds__(kMergeThreads) stats_records_merge(const Moments* __restrict__ rec, long long count,
+                                                                      float* out) {
+  __shared__ Moments red[kMergeThreads];
+  const long long per = (count + kMergeThreads - 1) / kMergeThreads;
+  const long long r0 = static_cast<long long>(threadIdx.x) * per;
+  const long long r1 = r0 + per < count ? r0 + per : count;
+  Moments m{0.0, 0.0, 0.0};
+  for (long long r = r0; r < r1; ++r) m = moments_merge(m, rec[r]);
+  red[threadIdx.x] = m;
+  __syncthreads();
+  for (int o = kMergeThreads / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o) red[threadIdx.x] = moments_merge(red[threadIdx.x], red[threadIdx.x + o]);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    const Moments t = red[0];
+    out[0] = static_cast<float>(t.mean);
+    out[1] = static_cast<float>(t.m2 / (t.n - 1.0));
+  }
 }
 
 __device__ __forceinline__ float taper_value(float f, float d, float mute, float taper, float dsum) {
@@ -113,36 +141,48 @@ __device__ __forceinline__ float taper_value(float f, float d, float mute, float
   return f;
 }
 
-__global__ void taper_structured_kernel(float* f, int n0, int n1, long long npts, int o0, int o1, int o2, float dh,
-                                        float p0, float p1, float p2, float mute, float taper) {
-  const float dsum = __fadd_rn(mute, taper);
+// Rescale, then the taper of every point of interest in order, per point:
+// the same operations, in the same order, as a rescale pass followed by one
+// taper pass per point of interest.
+__global__ void finalize_kernel(float* f, long long n, const FinalizeArgs a) {
+  const float dsum = __fadd_rn(a.mute, a.taper);
   const long long stride = static_cast<long long>(gridDim.x) * blockDim.x;
-  const long long plane = static_cast<long long>(n0) * n1;
-  for (long long p = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x; p < npts; p += stride) {
-    const int k = static_cast<int>(p / plane);
-    const long long rem = p - k * plane;
-    const int j = static_cast<int>(rem / n0);
-    const int i = static_cast<int>(rem - static_cast<long long>(j) * n0);
-    // ((i - 1) * dh - poi)^2 with the global 1-based index i.
-    float dx = __fsub_rn(__fmul_rn(static_cast<float>(i + o0), dh), p0);
-    float dy = __fsub_rn(__fmul_rn(static_cast<float>(j + o1), dh), p1);
-    float dz = __fsub_rn(__fmul_rn(static_cast<float>(k + o2), dh), p2);
-    dx = __fmul_rn(dx, dx);
-    dy = __fmul_rn(dy, dy);
-    dz = __fmul_rn(dz, dz);
-    const float d = __fsqrt_rn(__fadd_rn(__fadd_rn(dx, dy), dz));
-    f[p] = taper_value(f[p], d, mute, taper, dsum);
-  }
-}
-
-__global__ void taper_points_kernel(float* f, const float* x, const float* y, const float* z, long long n, float p0,
-                                    float p1, float p2, float mute, float taper) {
-  const float dsum = __fadd_rn(mute, taper);
-  const long long stride = static_cast<long long>(gridDim.x) * blockDim.x;
-  for (long long i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride) {
-    const float ex = __fsub_rn(x[i], p0), ey = __fsub_rn(y[i], p1), ez = __fsub_rn(z[i], p2);
-    const float d = __fsqrt_rn(__fadd_rn(__fadd_rn(__fmul_rn(ex, ex), __fmul_rn(ey, ey)), __fmul_rn(ez, ez)));
-    f[i] = taper_value(f[i], d, mute, taper, dsum);
+  const long long plane = static_cast<long long>(a.n0) * a.n1;
+  for (long long p = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x; p < n; p += stride) {
+    float v = f[p];
+    if (a.rescale) v = __fsub_rn(__fmul_rn(v, a.scaling), a.mean);
+    if (a.npoi > 0) {
+      float x, y, z;
+      if (a.d_x) {
+        x = a.d_x[p];
+        y = a.d_y[p];
+        z = a.d_z[p];
+      } else {
+        const int k = static_cast<int>(p / plane);
+        const long long rem = p - k * plane;
+        const int j = static_cast<int>(rem / a.n0);
+        const int i = static_cast<int>(rem - static_cast<long long>(j) * a.n0);
+        x = __fmul_rn(static_cast<float>(i + a.o0), a.dh);
+        y = __fmul_rn(static_cast<float>(j + a.o1), a.dh);
+        z = __fmul_rn(static_cast<float>(k + a.o2), a.dh);
+      }
+      for (int q = 0; q < a.npoi; ++q) {
+        const float* pt = a.d_poi + 3 * q;
+        float d;
+        if (a.d_x) {
+          const float ex = __fsub_rn(x, pt[0]), ey = __fsub_rn(y, pt[1]), ez = __fsub_rn(z, pt[2]);
+          d = __fsqrt_rn(__fadd_rn(__fadd_rn(__fmul_rn(ex, ex), __fmul_rn(ey, ey)), __fmul_rn(ez, ez)));
+        } else {
+          float dx = __fsub_rn(x, pt[0]), dy = __fsub_rn(y, pt[1]), dz = __fsub_rn(z, pt[2]);
+          dx = __fmul_rn(dx, dx);
+          dy = __fmul_rn(dy, dy);
+          dz = __fmul_rn(dz, dz);
+          d = __fsqrt_rn(__fadd_rn(__fadd_rn(dx, dy), dz));
+        }
+        v = taper_value(v, d, a.mute, a.taper, dsum);
+      }
+    }
+    f[p] = v;
   }
 }
 
@@ -166,24 +206,13 @@ cudaError_t launch_field_stats(const float* d_field, long long n, double* d_part
   return cudaGetLastError();
 }
 
-cudaError_t launch_rescale(float* d_field, long long n, float sigma, float std_, float mean, cudaStream_t stream) {
-  const float scaling = sigma / std_;  // scarflib_srm.f90:899, FP32 on the host
-  rescale_kernel<<<elementwise_blocks(n), 256, 0, stream>>>(d_field, n, scaling, mean);
+cudaError_t launch_stats_records(const StatRecord* d_rec, long long count, float* d_out, cudaStream_t stream) {
+  stats_records_merge<<<1, kMergeThreads, 0, stream>>>(d_rec, count, d_out);
   return cudaGetLastError();
 }
 
-cudaError_t launch_taper_structured(float* d_field, const int fs[3], const int n[3], float dh, const float poi[3],
-                                    float mute, float taper, cudaStream_t stream) {
-  const long long npts = static_cast<long long>(n[0]) * n[1] * n[2];
-  taper_structured_kernel<<<elementwise_blocks(npts), 256, 0, stream>>>(
-      d_field, n[0], n[1], npts, fs[0] - 1, fs[1] - 1, fs[2] - 1, dh, poi[0], poi[1], poi[2], mute, taper);
-  return cudaGetLastError();
-}
-
-cudaError_t launch_taper_points(float* d_field, const float* d_x, const float* d_y, const float* d_z, long long n,
-                                const float poi[3], float mute, float taper, cudaStream_t stream) {
-  taper_points_kernel<<<elementwise_blocks(n), 256, 0, stream>>>(d_field, d_x, d_y, d_z, n, poi[0], poi[1], poi[2],
-                                                                  mute, taper);
+cudaError_t launch_finalize_field(float* d_field, long long n, const FinalizeArgs& a, cudaStream_t stream) {
+  finalize_kernel<<<elementwise_blocks(n), 256, 0, stream>>>(d_field, n, a);
   return cudaGetLastError();
 }
 

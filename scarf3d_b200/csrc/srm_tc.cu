@@ -20,6 +20,7 @@
 // atomic counter over an item list sorted longest first); the producer warp
 // fetches each item and broadcasts it to the other warp roles through a small
 // shared-memory ring.
+#include <cuda_bf16.h>
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
@@ -56,6 +57,25 @@ __host__ __device__ constexpr uint32_t swz64(uint32_t row, uint32_t chunk) {
   return (row >> 3) * 512u + (row & 7u) * 64u + ((chunk ^ ((row & 7u) >> 1)) << 4);
 }
 
+// Split of two FP32 values into hi and lo 16-bit operands (hi = round(v),
+// lo = round(v - hi)), packed as two 2-byte elements: FP16 (the default) or
+// BF16 (the operand-precision setting; same layouts, same MMA kind).
+__device__ __forceinline__ void split_pair(float a, float b, bool bf16, uint32_t& hi, uint32_t& lo) {
+  if (bf16) {
+    const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
+    const float2 f = __bfloat1622float2(h);
+    const __nv_bfloat162 l = __floats2bfloat162_rn(a - f.x, b - f.y);
+    hi = *reinterpret_cast<const uint32_t*>(&h);
+    lo = *reinterpret_cast<const uint32_t*>(&l);
+  } else {
+    const __half2 h = __floats2half2_rn(a, b);
+    const float2 f = __half22float2(h);
+    const __half2 l = __floats2half2_rn(a - f.x, b - f.y);
+    hi = *reinterpret_cast<const uint32_t*>(&h);
+    lo = *reinterpret_cast<const uint32_t*>(&l);
+  }
+}
+
 // Geometry and table images of one field in the factorised form.
 struct TcField {
   int n1, n2, n3;
@@ -63,6 +83,9 @@ struct TcField {
   int bix, bjx;         // item grid: bi x bj, or CTA pairs along j (bi x ceil(bj/2)) or i (ceil(bi/2) x bj)
   long long sr, ss, sc; // field strides (elements) of the i, j and k axes
   int pair_i;           // CTA pairs split along i (2D fields: one row block along j)
+  int band;             // item order: row blocks along i per band (>= bix: natural order)
+  int terms;            // split products per K step: 3 (hi.hi, hi.lo, lo.hi) or 2 (hi.hi, lo.hi)
+  int bf16;             // operands split into BF16 instead of FP16
   uint32_t idesc;
   float scaling;
   const float2* rimg;   // [bi][stages][16][ti]
@@ -75,10 +98,14 @@ struct TcField {
   int* done_cnt;
   volatile int* done_flag;
   int done_expect;
+  // Statistics records of the stored field (null when unused): one per
+  // epilogue warp and item, at (local item * CTAs per item + CTA) * 4 + warp.
+  Moments* stats;
 };
 
 struct TcKernelArgs {
   TcField f0;             // the field when `fields` is null
+  int bf16;               // generators split A into BF16 (uniform over a launch)
   const TcField* fields;  // per-field descriptors of a batch
   const int2* items;      // {field, local item}, longest first; null: field 0 in natural order
   int num_items;
@@ -108,6 +135,7 @@ struct TableJob {
   int ax_r, ax_s, ax_c;  // physical axis of the row-fast, row-slow and column factors
   int n1, n2, n3, ti, tj, bi, bj, ntile_n, bn;  // bj: S-image blocks (even for CTA pairs)
   int parts;             // column image split: 1, or 2 halves (one per CTA of a pair)
+  int bf16;              // C image split into BF16 instead of FP16
   float2* rimg;
   float2* simg;
   uint8_t* cimg;
@@ -180,7 +208,7 @@ __global__ void tc_build_c(const TableJob j0, const TableJob* jobs) {
     const int col = nb * T.ntile_n + row;
     const int part_rows = T.ntile_n / T.parts;
     const int part = row / part_rows, prow = row - part * part_rows;
-    __half2 hi[4], lo[4];
+    uint32_t hi[4], lo[4];
 #pragma unroll
     for (int u = 0; u < 4; ++u) {
       const int h = k * kStageHarm + chunk * 4 + u;
@@ -194,9 +222,7 @@ __global__ void tc_build_c(const TableJob j0, const TableJob* jobs) {
         cs32 = static_cast<float>(cs);
         sn32 = static_cast<float>(sn);
       }
-      hi[u] = __floats2half2_rn(cs32, sn32);
-      const float2 hf = __half22float2(hi[u]);
-      lo[u] = __floats2half2_rn(cs32 - hf.x, sn32 - hf.y);
+      split_pair(cs32, sn32, T.bf16 != 0, hi[u], lo[u]);
     }
     uint8_t* base = T.cimg + ((static_cast<size_t>(nb) * T.stages + k) * T.parts + part) *
                                  (2u * part_rows * kRowBytes);
@@ -314,7 +340,7 @@ __global__ void tc_build_c_factored(const TableJob j0, const TableJob* jobs) {
     for (int col = threadIdx.x; col < ncol; col += blockDim.x) {
       const int nb = col / T.ntile_n, row = col - nb * T.ntile_n;
       const int part = row / part_rows, prow = row - part * part_rows;
-      __half2 hi[4], lo[4];
+      uint32_t hi[4], lo[4];
 #pragma unroll
       for (int u = 0; u < 4; ++u) {
         float cs32 = 0.0f, sn32 = 0.0f;
@@ -323,9 +349,7 @@ __global__ void tc_build_c_factored(const TableJob j0, const TableJob* jobs) {
           cs32 = static_cast<float>(z.x);
           sn32 = static_cast<float>(z.y);
         }
-        hi[u] = __floats2half2_rn(cs32, sn32);
-        const float2 hf = __half22float2(hi[u]);
-        lo[u] = __floats2half2_rn(cs32 - hf.x, sn32 - hf.y);
+        split_pair(cs32, sn32, T.bf16 != 0, hi[u], lo[u]);
       }
       uint8_t* base = T.cimg + ((static_cast<size_t>(nb) * T.stages + k) * T.parts + part) *
                                    (2u * part_rows * kRowBytes);
@@ -430,7 +454,7 @@ __global__ void __launch_bounds__(32 * kBuilderWarps) tc_build_c_warps(const Tab
     for (int col = lane; col < ncol; col += 32) {
       const int nb = col / T.ntile_n, row = col - nb * T.ntile_n;
       const int part = row / part_rows, prow = row - part * part_rows;
-      __half2 hi[4], lo[4];
+      uint32_t hi[4], lo[4];
 #pragma unroll
       for (int u = 0; u < 4; ++u) {
         float cs32 = 0.0f, sn32 = 0.0f;
@@ -439,9 +463,7 @@ __global__ void __launch_bounds__(32 * kBuilderWarps) tc_build_c_warps(const Tab
           cs32 = static_cast<float>(z.x);
           sn32 = static_cast<float>(z.y);
         }
-        hi[u] = __floats2half2_rn(cs32, sn32);
-        const float2 hf = __half22float2(hi[u]);
-        lo[u] = __floats2half2_rn(cs32 - hf.x, sn32 - hf.y);
+        split_pair(cs32, sn32, T.bf16 != 0, hi[u], lo[u]);
       }
       uint8_t* base = T.cimg + ((static_cast<size_t>(nb) * T.stages + k) * T.parts + part) *
                                    (2u * part_rows * kRowBytes);
@@ -506,6 +528,7 @@ void launch_table_builders(const TableJob& T, const TableJob* jobs, int nfields,
 struct Item {
   TcField f;
   int ib, jb, nt;
+  int local;  // item index within its field
 };
 
 __device__ __forceinline__ Item decode_item(const TcKernelArgs& A, int idx) {
@@ -517,11 +540,19 @@ __device__ __forceinline__ Item decode_item(const TcKernelArgs& A, int idx) {
     local = e.y;
   }
   it.f = A.fields ? A.fields[fid] : A.f0;
+  it.local = local;
   const int tiles_m = it.f.bix * it.f.bjx;
   it.nt = local / tiles_m;
   const int mt = local - it.nt * tiles_m;
-  it.ib = mt % it.f.bix;
-  it.jb = mt / it.f.bix;
+  // Within a column tile, bands of `band` row blocks along i, each walked
+  // over every j (the next band in the opposite j direction).
+  const int g = min(it.f.band, it.f.bix);
+  const int b = mt / (g * it.f.bjx);
+  const int gb = min(g, it.f.bix - b * g);
+  const int o = mt - b * g * it.f.bjx;
+  const int jo = o / gb;
+  it.ib = b * g + (o - jo * gb);
+  it.jb = (b & 1) ? it.f.bjx - 1 - jo : jo;
   return it;
 }
 
@@ -587,6 +618,28 @@ __device__ __forceinline__ void signal_slab(const TcKernelArgs& A, const TcField
   }
 }
 
+// Statistics of the values one warp stored for its 32 rows of an item (one
+// row per lane, columns k0 .. min(k0 + ntile_n, n3) - 1), read back after the
+// accumulator is released (the warp just stored them: L2 hits), accumulated
+// in FP64 about the row's first value, merged over the warp in a fixed order
+// and written by lane 0 into the item's record.
+__device__ __forceinline__ void record_stats(Moments* rec, const float* dst, long long plane, int k0, int ntile_n,
+                                             int n3, bool row_ok, int lane) {
+  double s1 = 0.0, s2 = 0.0, cnt = 0.0, shift = 0.0;
+  if (row_ok) {
+    const int kend = min(k0 + ntile_n, n3);
+    if (k0 < kend) shift = static_cast<double>(__ldcg(dst + plane * k0));
+    for (int k = k0; k < kend; ++k) {
+      const double d = static_cast<double>(__ldcg(dst + plane * k)) - shift;
+      s1 += d;
+      s2 = fma(d, d, s2);
+      cnt += 1.0;
+    }
+  }
+  const Moments m = warp_moments(moments_from_shifted(cnt, shift, s1, s2));
+  if (lane == 0) *rec = m;
+}
+
 // The field's last item is stored: the last epilogue warp to arrive raises
 // the field's host flag. System-scope fences order the field stores before
 // the count and the count before the flag, as for slabs.
@@ -607,16 +660,14 @@ __device__ __forceinline__ void generate_a_smem(const TcKernelArgs& A, uint8_t* 
   // rs: the stage's R tile [16][ti] followed by its S tile [16][tj] (float2)
   const float2* rt = reinterpret_cast<const float2*>(rs) + h0 * A.ti + ii;
   const float2* stt = reinterpret_cast<const float2*>(rs) + kStageHarm * A.ti + h0 * A.tj + jj;
-  __half2 hv[kGenHarm], lv[kGenHarm];
+  uint32_t hv[kGenHarm], lv[kGenHarm];
 #pragma unroll
   for (int u = 0; u < kGenHarm; ++u) {
     const float2 x = rt[u * A.ti];
     const float2 y = stt[u * A.tj];
     const float re = x.x * y.x - x.y * y.y;
     const float nim = -(x.x * y.y + x.y * y.x);
-    hv[u] = __floats2half2_rn(re, nim);
-    const float2 hf = __half22float2(hv[u]);
-    lv[u] = __floats2half2_rn(re - hf.x, nim - hf.y);
+    split_pair(re, nim, A.bf16 != 0, hv[u], lv[u]);
   }
   uint8_t* a_hi = st + A.off_a;
   uint8_t* a_lo = a_hi + kATileBytes;
@@ -818,14 +869,14 @@ __global__ void __launch_bounds__(kThreads, 1) srm_tc_kernel(const TcKernelArgs 
               if constexpr (kTmemA) {
                 const uint32_t ta = tmem_base + kTmemACol0 + s * kTmemAStageCols + 8 * kk;
                 umma_f16_ts(tmem_base, ta, dbh, w.f.idesc, acc);
-                umma_f16_ts(tmem_base, ta, dbl, w.f.idesc, 1u);
+                if (w.f.terms == 3) umma_f16_ts(tmem_base, ta, dbl, w.f.idesc, 1u);
                 umma_f16_ts(tmem_base, ta + 16, dbh, w.f.idesc, 1u);
               } else {
                 const uint32_t a_hi = st + A.off_a, a_lo = a_hi + kATileBytes;
                 const uint64_t dah = umma_smem_desc(a_hi + 32 * kk, 16, 512, kSwizzle64);
                 const uint64_t dal = umma_smem_desc(a_lo + 32 * kk, 16, 512, kSwizzle64);
                 umma_f16(tmem_base, dah, dbh, w.f.idesc, acc);
-                umma_f16(tmem_base, dah, dbl, w.f.idesc, 1u);
+                if (w.f.terms == 3) umma_f16(tmem_base, dah, dbl, w.f.idesc, 1u);
                 umma_f16(tmem_base, dal, dbh, w.f.idesc, 1u);
               }
               if (kk == 0 && k + 1 < c1) next_ok = stage_inputs_ready(s_next, ph_next);
@@ -886,6 +937,8 @@ __global__ void __launch_bounds__(kThreads, 1) srm_tc_kernel(const TcKernelArgs 
         if (lane == 0) mbar_arrive(acce);
         if (last && A.slab_cnt) signal_slab(A, w.f, w.ib, w.jb, w.nt, lane);
         if (last && w.f.done_flag) signal_field(w.f, lane);
+        if (last && w.f.stats)
+          record_stats(w.f.stats + w.local * 4 + q, dst, plane, k0, w.f.ntile_n, w.f.n3, row_ok, lane);
       }
     }
   } else if (warp >= kGenWarp0) {
@@ -916,16 +969,14 @@ __global__ void __launch_bounds__(kThreads, 1) srm_tc_kernel(const TcKernelArgs 
         uint8_t* st = smem + s * A.stage_bytes;
         const float2* rt = reinterpret_cast<const float2*>(st + A.off_r) + h0 * A.ti + ii;
         const float2* stt = reinterpret_cast<const float2*>(st + A.off_s) + h0 * A.tj + jj;
-        __half2 hv[kGenHarm], lv[kGenHarm];
+        uint32_t hv[kGenHarm], lv[kGenHarm];
 #pragma unroll
         for (int u = 0; u < kGenHarm; ++u) {
           const float2 x = rt[u * A.ti];
           const float2 y = stt[u * A.tj];
           const float re = x.x * y.x - x.y * y.y;
           const float nim = -(x.x * y.y + x.y * y.x);
-          hv[u] = __floats2half2_rn(re, nim);
-          const float2 hf = __half22float2(hv[u]);
-          lv[u] = __floats2half2_rn(re - hf.x, nim - hf.y);
+          split_pair(re, nim, A.bf16 != 0, hv[u], lv[u]);
         }
         if constexpr (kTmemA) {
           // Harmonic h = column h of the stage's hi half (16 + h: lo half).
@@ -1223,7 +1274,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1) srm_tc_
               const uint64_t dbh = umma_smem_desc(b_hi + 32 * kk, 16, 512, kSwizzle64);
               const uint64_t dbl = umma_smem_desc(b_lo + 32 * kk, 16, 512, kSwizzle64);
               umma_f16_pair(tmem_base, dah, dbh, w.f.idesc, (k > c0 || kk > 0) ? 1u : 0u);
-              umma_f16_pair(tmem_base, dah, dbl, w.f.idesc, 1u);
+              if (w.f.terms == 3) umma_f16_pair(tmem_base, dah, dbl, w.f.idesc, 1u);
               umma_f16_pair(tmem_base, dal, dbh, w.f.idesc, 1u);
               if (kk == 0 && k + 1 < c1) next_ok = stage_inputs_ready(s_next, ph_next);
             }
@@ -1317,6 +1368,9 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1) srm_tc_
         if (lane == 0) mbar_arrive_cluster(acce0);
         if (last && A.slab_cnt) signal_slab(A, w.f, ib, jb, w.nt, lane);
         if (last && w.f.done_flag) signal_field(w.f, lane);
+        if (last && w.f.stats)
+          record_stats(w.f.stats + (w.local * 2 + static_cast<int>(rank)) * 4 + q, dst, plane, k0, w.f.ntile_n,
+                       w.f.n3, row_ok, lane);
       }
     }
   } else if (warp >= kGenWarp0) {
@@ -1383,6 +1437,7 @@ int ilog2(int v) {
 constexpr int kDefaultChunkStages = 32;
 int g_chunk_stages = kDefaultChunkStages;
 int g_variant = kTcVariantSingle;
+int g_prec_bf16 = 0, g_prec_terms = 3;  // operand precision of plans made from now on
 
 TableJob make_job(const scarf_srm_setup& s, const int fs[3], float ds, const float* d_table, int nh,
                   const TcPlan& p, void* d_work) {
@@ -1408,6 +1463,7 @@ TableJob make_job(const scarf_srm_setup& s, const int fs[3], float ds, const flo
   T.ntile_n = p.ntile_n;
   T.bn = p.bn;
   T.parts = p.pair ? 2 : 1;
+  T.bf16 = p.bf16;
   T.rimg = reinterpret_cast<float2*>(work + p.off_r);
   T.simg = reinterpret_cast<float2*>(work + p.off_s);
   T.cimg = work + p.off_c;
@@ -1427,10 +1483,13 @@ TcField make_field(const scarf_srm_setup& s, const TcPlan& p, const TableJob& T,
   f.bix = p.bix;
   f.bjx = p.bjx;
   f.pair_i = p.pair_i;
+  f.band = p.bix;
   f.ntile_n = p.ntile_n;
   f.stages = p.stages;
   f.chunk_stages = std::max(1, p.chunk_stages);
-  f.idesc = umma_idesc_f16_f32(p.pair ? 2 * kRows : kRows, static_cast<uint32_t>(p.ntile_n));
+  f.idesc = umma_idesc_f16_f32(p.pair ? 2 * kRows : kRows, static_cast<uint32_t>(p.ntile_n), p.bf16 != 0);
+  f.terms = p.terms;
+  f.bf16 = p.bf16;
   f.scaling = s.scaling;
   f.rimg = T.rimg;
   f.simg = T.simg;
@@ -1524,6 +1583,13 @@ int tc_get_variant() { return g_variant; }
 
 void tc_set_variant(int v) { g_variant = v; }
 
+bool tc_set_precision(int bf16, int terms) {
+  if ((bf16 != 0 && bf16 != 1) || (terms != 2 && terms != 3)) return false;
+  g_prec_bf16 = bf16;
+  g_prec_terms = terms;
+  return true;
+}
+
 void tc_set_chunk_harmonics(int harmonics) {
   g_chunk_stages = harmonics > 0 ? (harmonics + kStageHarm - 1) / kStageHarm : kDefaultChunkStages;
 }
@@ -1574,6 +1640,8 @@ bool tc_make_plan(int ndim, const int n[3], int nh, TcPlan* P, int tj_force, boo
   const int n3_16 = (p.n3 + 15) / 16 * 16;
   p.bn = (n3_16 + max_n - 1) / max_n;
   p.ntile_n = ((p.n3 + p.bn - 1) / p.bn + 15) / 16 * 16;
+  p.bf16 = g_prec_bf16;
+  p.terms = g_prec_terms;
   p.nh = nh;
   p.nh_pad = (nh + kStageHarm - 1) / kStageHarm * kStageHarm;
   p.stages = p.nh_pad / kStageHarm;
@@ -1610,10 +1678,52 @@ TcSlab tc_slab_extent(const TcPlan& p, const TcSlabSignal& sig, int q) {
   return e;
 }
 
+// Item order of a single-field launch. The items in flight at once (one per
+// SM, or per CTA pair) each stream their R, S and C factor tiles through all
+// harmonics; in natural order they cover every row block along i, and the
+// tiles of one wave of items overflow L2 before the next wave reads them
+// again. In bands of g row blocks along i, consecutive waves share the band's
+// R tiles and the column tile's C tiles, which then stay in L2. The widest g
+// whose per-wave footprint fits in 3/4 of L2 is taken (natural order when
+// even one row block's does not); SCARF3D_B200_ITEM_BAND overrides it.
+int tc_item_band(const TcPlan& p, int nsm) {
+  if (const char* e = std::getenv("SCARF3D_B200_ITEM_BAND")) {
+    const int g = std::atoi(e);
+    if (g > 0) return g;
+  }
+  static int l2 = -1;
+  if (l2 < 0) {
+    int dev = 0, v = 0;
+    l2 = (cudaGetDevice(&dev) == cudaSuccess && cudaDeviceGetAttribute(&v, cudaDevAttrL2CacheSize, dev) == cudaSuccess)
+             ? v
+             : 0;
+  }
+  if (l2 <= 0) return p.bix;
+  const int conc = std::max(1, p.pair ? nsm / 2 : nsm);
+  const double rb = 16.0 * p.ti * sizeof(float2) * ((p.pair && p.pair_i) ? 2 : 1);
+  const double sb = 16.0 * p.tj * sizeof(float2) * ((p.pair && !p.pair_i) ? 2 : 1);
+  const double cb = 2.0 * p.ntile_n * kRowBytes;
+  auto footprint = [&](int g) {
+    const int jbs = std::min(p.bjx, (conc + g - 1) / g);
+    return static_cast<double>(p.stages) * (g * rb + jbs * sb + cb);
+  };
+  const double limit = 0.75 * static_cast<double>(l2);
+  if (footprint(p.bix) <= limit) return p.bix;
+  int g = 1;
+  while (2 * g < p.bix) g *= 2;
+  for (; g >= 1; g /= 2)
+    if (footprint(g) <= limit) return g;
+  return p.bix;
+}
+
+long long tc_stat_records(const TcPlan& p) {
+  return static_cast<long long>(p.bix) * p.bjx * p.bn * (p.pair ? 8 : 4);
+}
+
 cudaError_t launch_tc_structured(const scarf_srm_setup& s, const int fs[3], const int n[3], float ds,
                                  const float* d_table, int nh, float* d_field, void* d_work, const TcPlan& p,
                                  int* d_status, cudaStream_t stream, cudaEvent_t ev_main0, cudaEvent_t ev_main1,
-                                 const TcSlabSignal* slabs) {
+                                 const TcSlabSignal* slabs, StatRecord* d_stats) {
   const TableJob T = make_job(s, fs, ds, d_table, nh, p, d_work);
   const int nsm = device_sms();
   launch_table_builders(T, nullptr, 1, p.stages, factor_smem_rs(p), factor_smem_c(p), nsm, stream);
@@ -1622,6 +1732,9 @@ cudaError_t launch_tc_structured(const scarf_srm_setup& s, const int fs[3], cons
 
   TcKernelArgs A{};
   A.f0 = make_field(s, p, T, d_field);
+  A.bf16 = p.bf16;
+  A.f0.stats = d_stats;
+  A.f0.band = tc_item_band(p, nsm);
   A.fields = nullptr;
   A.items = nullptr;
   A.num_items = p.bix * p.bjx * p.bn;
@@ -1742,6 +1855,7 @@ cudaError_t tc_batch_launch(const TcBatchPlan& bp, void* d_work, cudaStream_t st
   if (e != cudaSuccess) return e;
   TcKernelArgs A{};
   A.fields = reinterpret_cast<const TcField*>(work + bp.off_fields);
+  A.bf16 = bp.nfields > 0 ? bp.plans[0].bf16 : 0;
   A.items = reinterpret_cast<const int2*>(work + bp.off_items);
   A.num_items = bp.num_items;
   A.status = status;

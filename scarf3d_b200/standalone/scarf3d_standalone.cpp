@@ -23,8 +23,7 @@
 // Defaults and checks follow main.f90:111-127 and 270-345, including their
 // messages; as in the reference, the Hurst-range check can never fire
 // (main.f90:333: hurst < 0 .and. hurst > 1). The reference's default method
-// is FIM (0), which this library does not implement: such inputs end with an
-// error naming '# method 1'. One process computes the whole grid
+// is FIM (0); both methods run here. One process computes the whole grid
 // (fs = 1, fe = npts), where the reference splits it over MPI ranks.
 #include <chrono>
 #include <cmath>
@@ -268,10 +267,7 @@ int main(int argc, char** argv) {
   const int rc = scarf_execute_ex(in.seed, field.data(), stats, 0);
   const double t_exec = seconds_since(t0);
   if (rc != SCARF_OK) {
-    if (rc == SCARF_ERR_UNSUPPORTED && in.method != 1)
-      std::printf(" Error: method %d (FIM) is not available in this library; set '# method' to 1 (SRM)\n", in.method);
-    else
-      std::printf(" Error: %s\n", scarf_last_error());
+    std::printf(" Error: %s\n", scarf_last_error());
     scarf_finalize();
     return 1;
   }

@@ -12,6 +12,8 @@ from pathlib import Path
 import numpy as np
 import pytest
 
+from conftest import HAS_GPU
+
 import scarf3d_b200 as sb
 
 ROOT = Path(__file__).resolve().parent.parent
@@ -103,10 +105,13 @@ def test_error_paths_without_a_gpu():
     fp = stats.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
     assert sb.lib.scarf_execute_ex(1, ctypes.c_void_p(field.ctypes.data), fp, 0) == sb.SCARF_ERR_STATE
     assert "before" in sb.last_error()
-    # FIM (method 0) is not implemented: the drop-in serves the SRM path only.
-    sb.scarf_initialize(fs=[1, 1, 1], fe=[2, 2, 2], ds=50.0, acf=0, cl=[2000.0] * 3, sigma=0.05, method=0)
-    assert sb.lib.scarf_execute_ex(1, ctypes.c_void_p(field.ctypes.data), fp, 0) == sb.SCARF_ERR_UNSUPPORTED
-    sb.scarf_finalize()
+    # Both methods reach the device: without one, execute reports a CUDA error.
+    for method in (0, 1):
+        sb.scarf_initialize(fs=[1, 1, 1], fe=[2, 2, 2], ds=50.0, acf=0, cl=[2000.0] * 3, sigma=0.05, method=method)
+        if not HAS_GPU:
+            assert sb.lib.scarf_execute_ex(1, ctypes.c_void_p(field.ctypes.data), fp, 0) == sb.SCARF_ERR_CUDA
+            assert sb.last_error()
+        sb.scarf_finalize()
     assert sb.lib.scarf_set_nharm(0) == sb.SCARF_ERR_ARG
     assert sb.lib.scarf_set_form(7) == sb.SCARF_ERR_ARG
     assert sb.lib.scarf_set_uniform_source(ctypes.c_void_p(1), None) == sb.SCARF_ERR_ARG

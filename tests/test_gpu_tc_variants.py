@@ -147,3 +147,27 @@ def test_degenerate_blocks_and_tiny_harmonic_counts(fs, n, nharm):
     ref64 = oracle.sum_structured(oracle.setup(op), fs, n, 50.0, tab, f64=True)
     # absolute bound: 1e-4 of sigma (the bench's 512^3 field sees ~1e-5)
     assert float(np.max(np.abs(fields[0].astype(np.float64) - ref64))) <= 1e-4 * 0.05
+
+
+@pytest.mark.parametrize("variant", VARIANTS)
+def test_operand_precision_settings_against_fp64(variant):
+    """FP16 hi/lo with 3 products (the default) meets 1e-5 against FP64; BF16
+    parts keep fewer bits and dropping the hi.lo product loses the B
+    correction, so both come out worse (measured, not assumed)."""
+    case = structured_case("vk3d_rot_offset", nharm=1500)
+    s = sb.compute_setup(case["pp"])
+    tab, _ = sb.sample(case["pp"], s)
+    ref64 = oracle.sum_structured(oracle.setup(case["op"]), case["fs"], case["n"], case["ds"], tab, f64=True)
+    err = {}
+    try:
+        for otype, terms in ((sb.TC_FP16, 3), (sb.TC_BF16, 3), (sb.TC_FP16, 2), (sb.TC_BF16, 2)):
+            sb.set_tc_precision(otype, terms)
+            f = _run(variant, s, case["fs"], case["n"], case["ds"], tab)
+            assert np.all(np.isfinite(f))
+            err[(otype, terms)] = rel_rms(f, ref64)
+    finally:
+        sb.set_tc_precision(sb.TC_FP16, 3)
+    assert err[(sb.TC_FP16, 3)] <= 1e-5
+    assert err[(sb.TC_BF16, 3)] > err[(sb.TC_FP16, 3)]
+    assert err[(sb.TC_FP16, 2)] > 1e-5
+    assert err[(sb.TC_BF16, 2)] > err[(sb.TC_FP16, 2)]

@@ -133,7 +133,17 @@ def test_run_writes_the_library_field(exe, tmp_path):
 
 
 @pytest.mark.gpu
-def test_fim_method_is_reported(exe, tmp_path):
-    r = run(exe, write_input(tmp_path / "in.txt", dict(BASE, method="0")), cwd=tmp_path)
-    assert r.returncode == 1
-    assert "set '# method' to 1 (SRM)" in r.stdout
+def test_fim_run_writes_the_library_field(exe, tmp_path):
+    """# method 0 (the reference's default, FIM) runs too; with # pad 1."""
+    import scarf3d_b200 as sb
+    r = run(exe, write_input(tmp_path / "in.txt", dict(BASE, method="0", pad="1")), cwd=tmp_path)
+    assert r.returncode == 0, r.stdout + r.stderr
+    got = np.fromfile(tmp_path / "random_field.bin", dtype=np.float32)
+    n = [24, 20, 16]
+    sb.scarf_initialize(fs=[1, 1, 1], fe=n, ds=25.0, acf=0, cl=[2000.0, 2000.0, 1000.0], sigma=0.05, method=0,
+                        hurst=0.5, pad=1)
+    try:
+        ref, _ = sb.scarf_execute(1234)
+    finally:
+        sb.scarf_finalize()
+    assert np.array_equal(got.view(np.uint32), np.asarray(ref, np.float32).view(np.uint32))
