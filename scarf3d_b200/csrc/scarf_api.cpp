@@ -130,7 +130,18 @@ struct Resources {
   int* slab_flags = nullptr;           // host-mapped, written by the kernel
   int* slab_flags_dev = nullptr;
   int slab_cap = 0;
+  // Page-locked bounce ring for pageable host fields (kBounceSlots slots).
+  char* bounce = nullptr;
+  size_t bounce_slot = 0;
+  cudaEvent_t bounce_ev[4] = {};
   void release() {
+    if (bounce) cudaFreeHost(bounce);
+    bounce = nullptr;
+    bounce_slot = 0;
+    for (auto& e : bounce_ev) {
+      if (e) cudaEventDestroy(e);
+      e = nullptr;
+    }
     if (slab_flags) cudaFreeHost(slab_flags);
     slab_flags = slab_flags_dev = nullptr;
     slab_cap = 0;
@@ -207,8 +218,121 @@ inline void cpu_relax() {
 // slab order, each as soon as the kernel has flagged it, on the copy stream.
 // Once the launch stream is idle every remaining slab is copied without
 // waiting (the status check that follows reports a failed launch).
+// ------------------------------------------------ pageable host output --
+// A device-to-host copy into pageable memory goes through the driver's own
+// staging at a fraction of the link's rate. For pageable fields the copies go
+// instead into a ring of page-locked slots at full rate, and the host's
+// worker threads move each slot into the caller's array (in parallel pieces)
+// while the next slots are in flight.
+constexpr int kBounceSlots = 4;
+constexpr size_t kBounceSlotCap = size_t(16) << 20;
+
+bool is_pageable(const void* p) {
+  cudaPointerAttributes a{};
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return true;
+  }
+  return a.type == cudaMemoryTypeUnregistered;
+}
+
+int ensure_bounce(size_t slot_bytes) {
+  slot_bytes = (slot_bytes + 4095) / 4096 * 4096;
+  if (g_res.bounce && g_res.bounce_slot >= slot_bytes) return SCARF_OK;
+  if (g_res.bounce) cudaFreeHost(g_res.bounce);
+  g_res.bounce = nullptr;
+  g_res.bounce_slot = 0;
+  void* h = nullptr;
+  SCARF_CUDA(cudaHostAlloc(&h, slot_bytes * kBounceSlots, cudaHostAllocDefault));
+  g_res.bounce = static_cast<char*>(h);
+  g_res.bounce_slot = slot_bytes;
+  for (auto& e : g_res.bounce_ev)
+    if (!e) SCARF_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  return SCARF_OK;
+}
+
+// A 2-D region (rows of `width` bytes, `height` rows) copied device -> a
+// pageable host array through the ring. Regions are issued in order; each
+// issue first completes the copy that last used its slot.
+class BounceCopier {
+ public:
+  explicit BounceCopier(cudaStream_t cs) : cs_(cs) {}
+  ~BounceCopier() { finish(); }
+  int issue(char* dst, size_t dpitch, const char* src, size_t spitch, size_t width, size_t height) {
+    const size_t cap = g_res.bounce_slot;
+    const size_t rows_per = std::max<size_t>(1, cap / std::max<size_t>(width, 1));
+    if (width > cap) {  // one row longer than a slot: split the row
+      for (size_t r = 0; r < height; ++r)
+        for (size_t o = 0; o < width; o += cap) {
+          const int rc = issue_piece(dst + r * dpitch + o, dpitch, src + r * spitch + o, spitch,
+                                     std::min(cap, width - o), 1);
+          if (rc) return rc;
+        }
+      return SCARF_OK;
+    }
+    for (size_t r = 0; r < height; r += rows_per) {
+      const int rc = issue_piece(dst + r * dpitch, dpitch, src + r * spitch, spitch, width,
+                                 std::min(rows_per, height - r));
+      if (rc) return rc;
+    }
+    return SCARF_OK;
+  }
+  int finish() {
+    int rc = SCARF_OK;
+    for (int k = 0; k < kBounceSlots; ++k) {
+      const int c = complete((next_ + k) % kBounceSlots);
+      if (c && !rc) rc = c;
+    }
+    return rc;
+  }
+
+ private:
+  struct Pending {
+    bool busy = false;
+    char* dst = nullptr;
+    size_t dpitch = 0, width = 0, height = 0;
+  };
+  int issue_piece(char* dst, size_t dpitch, const char* src, size_t spitch, size_t width, size_t height) {
+    const int slot = next_;
+    next_ = (next_ + 1) % kBounceSlots;
+    int rc = complete(slot);
+    if (rc) return rc;
+    char* buf = g_res.bounce + static_cast<size_t>(slot) * g_res.bounce_slot;
+    SCARF_CUDA(cudaMemcpy2DAsync(buf, width, src, spitch, width, height, cudaMemcpyDeviceToHost, cs_));
+    SCARF_CUDA(cudaEventRecord(g_res.bounce_ev[slot], cs_));
+    pend_[slot] = Pending{true, dst, dpitch, width, height};
+    return SCARF_OK;
+  }
+  int complete(int slot) {
+    Pending& q = pend_[slot];
+    if (!q.busy) return SCARF_OK;
+    q.busy = false;
+    SCARF_CUDA(cudaEventSynchronize(g_res.bounce_ev[slot]));
+    const char* buf = g_res.bounce + static_cast<size_t>(slot) * g_res.bounce_slot;
+    constexpr size_t kPiece = size_t(1) << 20;
+    const size_t per_row = (q.width + kPiece - 1) / kPiece;
+    const Pending w = q;
+    parallel_tasks(static_cast<int>(per_row * w.height), host_threads(), [&](int t) {
+      const size_t r = static_cast<size_t>(t) / per_row, o = (static_cast<size_t>(t) % per_row) * kPiece;
+      std::memcpy(w.dst + r * w.dpitch + o, buf + r * w.width + o, std::min(kPiece, w.width - o));
+    });
+    return SCARF_OK;
+  }
+  cudaStream_t cs_;
+  int next_ = 0;
+  Pending pend_[kBounceSlots];
+};
+
 int copy_slabs_out(const TcPlan& plan, const TcSlabSignal& sig, const float* d_field, float* field,
                    cudaStream_t st) {
+  const bool bounce = is_pageable(field);
+  if (bounce) {
+    const TcSlab e0 = tc_slab_extent(plan, sig, 0);
+    const size_t slab_bytes = static_cast<size_t>(e0.y1 - e0.y0) * plan.n1 * (e0.z1 - e0.z0) * sizeof(float);
+    const int rc = ensure_bounce(std::min(kBounceSlotCap, std::max<size_t>(slab_bytes, 1 << 20)));
+    if (rc) return rc;
+  }
+  BounceCopier bc(g_res.copy_stream);
   volatile int* flags = g_res.slab_flags;
   const size_t plane = static_cast<size_t>(plan.n1) * plan.n2;
   bool idle = false;
@@ -223,11 +347,38 @@ int copy_slabs_out(const TcPlan& plan, const TcSlabSignal& sig, const float* d_f
     const TcSlab e = tc_slab_extent(plan, sig, q);
     if (e.z1 <= e.z0 || e.y1 <= e.y0) continue;
     const size_t off = static_cast<size_t>(e.z0) * plane + static_cast<size_t>(e.y0) * plan.n1;
-    SCARF_CUDA(cudaMemcpy2DAsync(field + off, plane * sizeof(float), d_field + off, plane * sizeof(float),
-                                 static_cast<size_t>(e.y1 - e.y0) * plan.n1 * sizeof(float), e.z1 - e.z0,
-                                 cudaMemcpyDeviceToHost, g_res.copy_stream));
+    const size_t width = static_cast<size_t>(e.y1 - e.y0) * plan.n1 * sizeof(float);
+    if (bounce) {
+      const int rc = bc.issue(reinterpret_cast<char*>(field + off), plane * sizeof(float),
+                              reinterpret_cast<const char*>(d_field + off), plane * sizeof(float), width, e.z1 - e.z0);
+      if (rc) return rc;
+      continue;
+    }
+    SCARF_CUDA(cudaMemcpy2DAsync(field + off, plane * sizeof(float), d_field + off, plane * sizeof(float), width,
+                                 e.z1 - e.z0, cudaMemcpyDeviceToHost, g_res.copy_stream));
   }
-  return SCARF_OK;
+  return bc.finish();
+}
+
+// Whole field device -> host on `st` (after the kernels queued there): direct
+// for page-locked or mapped memory, through the bounce ring for pageable.
+int copy_field_out(float* field, const float* d_field, long long npts, cudaStream_t st) {
+  const size_t bytes = sizeof(float) * static_cast<size_t>(npts);
+  if (!is_pageable(field)) {
+    SCARF_CUDA(cudaMemcpyAsync(field, d_field, bytes, cudaMemcpyDeviceToHost, st));
+    return SCARF_OK;
+  }
+  int rc = ensure_bounce(std::min(kBounceSlotCap, std::max<size_t>(bytes / kBounceSlots, 1 << 20)));
+  if (rc) return rc;
+  BounceCopier bc(st);
+  const size_t row = g_res.bounce_slot;
+  const size_t rows = bytes / row, rest = bytes - rows * row;
+  char* dst = reinterpret_cast<char*>(field);
+  const char* src = reinterpret_cast<const char*>(d_field);
+  if (rows) rc = bc.issue(dst, row, src, row, row, rows);
+  if (!rc && rest) rc = bc.issue(dst + rows * row, rest, src + rows * row, rest, rest, 1);
+  const int fr = bc.finish();
+  return rc ? rc : fr;
 }
 
 // Events bracketing the dominant kernel of the next launch, when enabled.
@@ -355,7 +506,8 @@ int fim_execute_impl(int seed, float* field, float stats[8], int flags) {
   const cudaError_t e = fim_run(in, g, g_res.work.p, d_field, stats, st, &what);
   if (e != cudaSuccess) return fail(SCARF_ERR_CUDA, "FIM: %s: %s", what, cudaGetErrorString(e));
   if (!on_device) {
-    SCARF_CUDA(cudaMemcpyAsync(field, d_field, sizeof(float) * npts, cudaMemcpyDeviceToHost, st));
+    const int rc = copy_field_out(field, d_field, npts, st);
+    if (rc) return rc;
     SCARF_CUDA(cudaStreamSynchronize(st));
   }
   return SCARF_OK;
@@ -574,8 +726,10 @@ int execute_impl(int seed, float* field, float stats[8], int flags) {
     SCARF_CUDA(cudaStreamSynchronize(g_res.copy_stream));
   } else {
     SCARF_CUDA(cudaEventRecord(g_res.ev1, st));
-    if (!on_device)
-      SCARF_CUDA(cudaMemcpyAsync(field, d_field, sizeof(float) * npts, cudaMemcpyDeviceToHost, st));
+    if (!on_device) {
+      rc = copy_field_out(field, d_field, npts, st);
+      if (rc) return rc;
+    }
   }
   SCARF_CUDA(cudaStreamSynchronize(st));
   float ms = 0.0f;

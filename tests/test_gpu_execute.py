@@ -171,3 +171,30 @@ def test_execute_overlap_falls_back_when_rescaling():
         sb.set_output_overlap(1)
     assert np.array_equal(a, b) and np.array_equal(sa[:4], sbb[:4])
     assert sbb[2] == np.float32(0.05)
+
+
+@pytest.mark.parametrize("form,rescale,method", [(sb.FORM_TC, 0, 1), (sb.FORM_TC, 1, 1), (sb.FORM_DIRECT, 0, 1),
+                                                 (sb.FORM_AUTO, 0, 0)])
+def test_execute_pageable_and_page_locked_outputs_agree(form, rescale, method):
+    """Pageable host fields go through the page-locked bounce ring (in slabs
+    while the tensor-core kernel runs, or in whole after it); page-locked
+    fields are copied directly; both equal the device output bit for bit."""
+    fs, fe = [1, 1, 1], [130, 96, 290]
+    sb.set_form(form)
+    sb.scarf_initialize(fs=fs, fe=fe, acf=0, hurst=0.25, sigma=0.05, ds=50.0, cl=[2000.0] * 3, method=method,
+                        rescale=rescale)
+    npts = int(np.prod([e - s + 1 for s, e in zip(fs, fe)]))
+    sb.set_output_overlap(2)
+    try:
+        dev = torch.empty(npts, dtype=torch.float32, device="cuda")
+        _, sd = sb.scarf_execute(77, dev)
+        pageable = np.full(npts, np.nan, np.float32)
+        _, sp = sb.scarf_execute(77, pageable)
+        pinned = torch.full((npts,), float("nan"), dtype=torch.float32, pin_memory=True)
+        _, sl = sb.scarf_execute(77, pinned.numpy())
+    finally:
+        sb.set_output_overlap(1)
+    ref = dev.cpu().numpy()
+    assert np.array_equal(pageable.view(np.uint32), ref.view(np.uint32))
+    assert np.array_equal(pinned.numpy().view(np.uint32), ref.view(np.uint32))
+    assert np.array_equal(sd[:4], sp[:4]) and np.array_equal(sd[:4], sl[:4])
