@@ -547,6 +547,60 @@ def _points_leg(cfg, steps, e2e_steps, clocks, cpu_full=True):
     return out
 
 
+def run_fim(args, clocks):
+    """The reference's other method (FIM, method 0) on the precision
+    configuration's grid: 512^3 at 25 m, von Karman H=0.5, cl 3000/3000/1000 m,
+    no padding (internal grid 514^3). Timed through scarf_execute into a
+    device field (stats[4..7]: spectrum, symmetry, transform with statistics,
+    mapping) and into a page-locked host field; every point checked against
+    the CPU restatement at sampled points of the internal grid is left to the
+    tests (the full oracle needs the whole spectrum on the host)."""
+    import torch
+
+    import scarf3d_b200 as sb
+
+    n = [512, 512, 512]
+    npts = int(np.prod(n))
+    sb.set_stream(torch.cuda.current_stream().cuda_stream)
+    sb.scarf_initialize(fs=[1, 1, 1], fe=n, ds=25.0, acf=0, cl=[3000.0, 3000.0, 1000.0], sigma=0.05, method=0,
+                        hurst=0.5)
+    try:
+        dev = torch.empty(npts, dtype=torch.float32, device="cuda")
+        for _ in range(2):
+            sb.scarf_execute(1234, dev)
+        parts, t_dev = [], []
+        for _ in range(max(3, min(args.steps, 10))):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            _, st = sb.scarf_execute(1234, dev)
+            t_dev.append(time.perf_counter() - t0)
+            parts.append([float(v) for v in st[4:8]])
+        host = torch.empty(npts, dtype=torch.float32, pin_memory=True)
+        sb.scarf_execute(1234, host.numpy())
+        t_host = []
+        for _ in range(3):
+            t0 = time.perf_counter()
+            sb.scarf_execute(1234, host.numpy())
+            t_host.append(time.perf_counter() - t0)
+        same = bool(torch.equal(host, dev.cpu()))
+    finally:
+        sb.scarf_finalize()
+    ph = np.mean(np.asarray(parts), axis=0)
+    # internal grid 514^3: spectrum writes n3 n2 (n1/2+1) complex (8 B), the
+    # transform reads/writes them and writes the real grid (4 B per point)
+    internal = 514 ** 3
+    spec_bytes = 514 * 514 * 258 * 8
+    return {"workload": "fim_structured_512x512x512_ds25m_vk_h0.5_cl3000/3000/1000_nopad", "points": npts,
+            "internal_grid": [514, 514, 514], "unit": "points/s",
+            "device": {"value": npts / float(np.median(t_dev)), "s_per_call": float(np.median(t_dev)),
+                       "spectrum_s": ph[0], "symmetry_s": ph[1], "transform_stats_s": ph[2], "mapping_s": ph[3],
+                       "spectrum_gbs": spec_bytes / ph[0] / 1e9 if ph[0] > 0 else None,
+                       "internal_points": internal},
+            "e2e": {"value": npts / float(np.median(t_host)), "s_per_call": float(np.median(t_host)),
+                    "host_memory": "page-locked", "d2h_bytes_per_step": npts * 4,
+                    "field_equals_device_output": same}}
+
+
 def run_configs(args, peaks, clocks):
     """Configurations 1, 2 and 5 (the batched configuration has its own leg)."""
     import torch
@@ -777,6 +831,7 @@ def run_b200(args, w):
     traffic = profile_traffic()
     batched = run_batched(args) if (world == 1 and not args.no_batched) else None
     configs = run_configs(args, load_peaks(), clocks) if world == 1 else None
+    fim_leg = run_fim(args, clocks) if (world == 1 and not args.no_fim) else None
     if rank == 0:
         cpu = cpu_baseline_sample(w) if world == 1 else None
         line = {
@@ -807,6 +862,7 @@ def run_b200(args, w):
             "precision_plans": precision,
             "batched": batched,
             "configs": configs,
+            "fim": fim_leg,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(nh * 20),
                     "d2h_bytes_per_step": int(npts * 4 + 8), "ms_per_step": t_e2e / args.steps * 1e3,
                     "host_sampling_ms": float(np.mean(host_s)) * 1e3, "device_ms": float(np.mean(device_s)) * 1e3,
@@ -834,6 +890,7 @@ def main():
     ap.add_argument("--no-batched", action="store_true", help="skip the 256-field batched measurement")
     ap.add_argument("--no-autotune", action="store_true", help="default plans instead of autotuned ones")
     ap.add_argument("--no-precision", action="store_true", help="skip the operand-precision comparison")
+    ap.add_argument("--no-fim", action="store_true", help="skip the FIM (method 0) measurement")
     ap.add_argument("--configs", default="1,2,5",
                     help="other configurations to measure (comma list of 1, 2, 5; empty to skip)")
     args = ap.parse_args()

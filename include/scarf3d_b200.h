@@ -160,6 +160,7 @@ typedef struct scarf_tc_tuning {
   int tile_j;  /* row tile (128 / tile_j) x tile_j                */
   int permute; /* 1: longest axis as column axis (device fields)  */
   float ms;    /* kernel time of the chosen plan on the probe      */
+  int split;   /* harmonic segments per tile (1: none; device fields) */
 } scarf_tc_tuning;
 /* 0 = default plans (the initial state), 1 = follow recorded tunings. */
 int scarf_set_tc_autotune(int mode);

@@ -96,7 +96,7 @@ class TcField(ctypes.Structure):
 class TcTuning(ctypes.Structure):
     """scarf_tc_tuning: a tuned plan choice of the tensor-core form."""
     _fields_ = [("variant", ctypes.c_int), ("tile_j", ctypes.c_int), ("permute", ctypes.c_int),
-                ("ms", ctypes.c_float)]
+                ("ms", ctypes.c_float), ("split", ctypes.c_int)]
 
 
 def _load() -> ctypes.CDLL:
@@ -466,14 +466,14 @@ def tc_autotune(s: "SrmSetup", fs, n, ds: float, d_table: int, nh: int, fixed_co
     check(lib.scarf_srm_tc_autotune(ctypes.byref(s), _iptr(fs), _iptr(n), float(ds), ctypes.c_void_p(int(d_table)),
                                     int(nh), int(bool(fixed_columns)), ctypes.c_void_p(stream_handle or 0),
                                     ctypes.byref(t)))
-    return {"variant": t.variant, "tile_j": t.tile_j, "permute": t.permute, "ms": t.ms}
+    return {"variant": t.variant, "tile_j": t.tile_j, "permute": t.permute, "ms": t.ms, "split": t.split}
 
 
 def tc_plan_info(ndim: int, n, nh: int) -> dict:
     """The plan the device-field tensor-core entry points would use now."""
     t = TcTuning()
     check(lib.scarf_srm_tc_plan_info(int(ndim), _iptr(n), int(nh), ctypes.byref(t)))
-    return {"variant": t.variant, "tile_j": t.tile_j, "permute": t.permute}
+    return {"variant": t.variant, "tile_j": t.tile_j, "permute": t.permute, "split": t.split}
 
 
 def set_output_overlap(items_per_slab: int = 1):

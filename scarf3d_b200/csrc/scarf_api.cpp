@@ -10,6 +10,7 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <fstream>
 #include <map>
@@ -1129,8 +1130,12 @@ namespace scarf {
 bool device_field_plan(int ndim, const int n[3], int nh, TcPlan* p) {
   TcChoice c{};
   if (n[0] > 0 && n[1] > 0 && n[2] > 0 && tc_tuned_choice(ndim, n, false, &c))
-    return tc_make_plan(ndim, n, nh, p, c.tile_j, c.permute != 0, c.variant);
-  return tc_make_plan(ndim, n, nh, p, 0, true);
+    return tc_make_plan(ndim, n, nh, p, c.tile_j, c.permute != 0, c.variant, std::max(1, c.split));
+  // SCARF3D_B200_TC_SPLIT=<n> splits the harmonics of untuned device-field
+  // plans over n items per tile (tests compare split and unsplit sums).
+  const char* e = std::getenv("SCARF3D_B200_TC_SPLIT");
+  const int split = e ? std::max(1, std::atoi(e)) : 1;
+  return tc_make_plan(ndim, n, nh, p, 0, true, -1, split);
 }
 }  // namespace scarf
 extern "C" {
@@ -1147,6 +1152,7 @@ int scarf_srm_tc_plan_info(int ndim, const int n[3], int nh, scarf_tc_tuning* ou
   out->tile_j = p.tj;
   out->permute = p.ax_c != (ndim == 3 ? 2 : 1) ? 1 : 0;
   out->ms = 0.0f;
+  out->split = p.split;
   return SCARF_OK;
 }
 
@@ -1438,7 +1444,7 @@ int scarf_field_stats(const float* d_field, long long n, void* d_work, size_t wo
 // row tile (128 / tile_j) x tile_j and column axis, per shape bucket (grid
 // extents rounded up to a multiple of 16; the key also names the GPU and the
 // driver). Entries live in memory and, when a cache file is set, one line
-// each in that file ("key variant tile_j permute ms").
+// each in that file ("key variant tile_j permute ms split").
 namespace {
 struct TuneState {
   std::mutex mu;
@@ -1489,7 +1495,10 @@ void load_cache_locked(const std::string& path) {
     std::istringstream is(line);
     std::string key;
     scarf::TcChoice c{};
-    if (is >> key >> c.variant >> c.tile_j >> c.permute >> c.ms) g_tune.entries[key] = c;
+    if (is >> key >> c.variant >> c.tile_j >> c.permute >> c.ms) {
+      if (!(is >> c.split) || c.split < 1) c.split = 1;  // lines written before the split existed
+      g_tune.entries[key] = c;
+    }
   }
 }
 
@@ -1497,7 +1506,8 @@ void store_locked(const std::string& key, const scarf::TcChoice& c) {
   g_tune.entries[key] = c;
   if (g_tune.path.empty()) return;
   std::ofstream f(g_tune.path, std::ios::app);
-  f << key << ' ' << c.variant << ' ' << c.tile_j << ' ' << c.permute << ' ' << c.ms << '\n';
+  f << key << ' ' << c.variant << ' ' << c.tile_j << ' ' << c.permute << ' ' << c.ms << ' ' << std::max(1, c.split)
+    << '\n';
 }
 
 // Time of one plan on the caller's data, table builds and kernel (the
@@ -1566,6 +1576,12 @@ int scarf_srm_tc_autotune(const scarf_srm_setup* s, const int fs[3], const int n
   const int tiles[5] = {1, 2, 4, 8, 16};
   std::vector<TcPlan> plans;
   std::vector<scarf::TcChoice> choices;
+  int nsm = 148;
+  {
+    int dev = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    cudaGetLastError();
+  }
   for (int v : forms)
     for (int tj : tiles)
       for (int perm = 0; perm < (fixed_columns ? 1 : 2); ++perm) {
@@ -1576,7 +1592,18 @@ int scarf_srm_tc_autotune(const scarf_srm_setup* s, const int fs[3], const int n
           if (q.ax_c == p.ax_c && q.tj == p.tj && q.pair == p.pair && q.tmem_a == p.tmem_a) continue;
         }
         plans.push_back(p);
-        choices.push_back(scarf::TcChoice{v, tj, perm, 0.0f});
+        choices.push_back(scarf::TcChoice{v, tj, perm, 0.0f, 1});
+        // Fewer tiles than SMs: splitting the harmonics over 2-8 items per
+        // tile fills the GPU (device fields only: scarf_execute needs the
+        // final values in the kernel for its statistics and slab copies).
+        const long long tiles_m = static_cast<long long>(p.bix) * p.bjx * p.bn;
+        if (fixed_columns || p.pair || tiles_m >= nsm) continue;
+        for (int split = 2; split <= 8 && tiles_m * split <= 2LL * nsm; split *= 2) {
+          TcPlan q{};
+          if (!tc_make_plan(s->ndim, n, nh_probe, &q, tj, perm != 0, v, split) || q.split != split) continue;
+          plans.push_back(q);
+          choices.push_back(scarf::TcChoice{v, tj, perm, 0.0f, split});
+        }
       }
   size_t work = 0;
   for (const TcPlan& p : plans) work = std::max(work, p.bytes);
@@ -1610,8 +1637,8 @@ int scarf_srm_tc_autotune(const scarf_srm_setup* s, const int fs[3], const int n
   if (tc_make_plan(s->ndim, n, nh_probe, &dp, 0, fixed_columns == 0, SCARF_TC_SINGLE)) {
     for (size_t c = 0; c < plans.size(); ++c) {
       const TcPlan& q = plans[c];
-      if (q.ax_c == dp.ax_c && q.tj == dp.tj && q.pair == dp.pair && q.tmem_a == dp.tmem_a && choices[c].ms > 0.0f &&
-          choices[best].ms > 0.97f * choices[c].ms)
+      if (q.ax_c == dp.ax_c && q.tj == dp.tj && q.pair == dp.pair && q.tmem_a == dp.tmem_a && q.split == 1 &&
+          choices[c].ms > 0.0f && choices[best].ms > 0.97f * choices[c].ms)
         best = static_cast<int>(c);
     }
   }
@@ -1624,6 +1651,7 @@ int scarf_srm_tc_autotune(const scarf_srm_setup* s, const int fs[3], const int n
   out->tile_j = b.tile_j;
   out->permute = b.permute;
   out->ms = b.ms;
+  out->split = std::max(1, b.split);
   return SCARF_OK;
 }
 
@@ -1640,7 +1668,7 @@ int scarf_srm_tc_batch_autotune(const scarf_tc_field* fields, int nfields, void*
     if (e0) cudaEventDestroy(e0);
     return fail(SCARF_ERR_CUDA, "autotune: event creation failed");
   }
-  scarf::TcChoice best{-1, 0, 1, 0.0f}, deflt{-1, 0, 1, 0.0f};
+  scarf::TcChoice best{-1, 0, 1, 0.0f, 1}, deflt{-1, 0, 1, 0.0f, 1};
   int auto_tj = 8;  // the row tile the batch would get with tile_j = 0
   {
     auto in0 = batch_inputs(fields, nfields);
@@ -1678,8 +1706,8 @@ int scarf_srm_tc_batch_autotune(const scarf_tc_field* fields, int nfields, void*
       }
       cudaGetLastError();
       scarf::device_free(d_work, bp.bytes);
-      if (ms > 0.0f && (best.variant < 0 || ms < best.ms)) best = scarf::TcChoice{v, tj, 1, ms};
-      if (ms > 0.0f && v == SCARF_TC_SINGLE && tj == auto_tj) deflt = scarf::TcChoice{v, tj, 1, ms};
+      if (ms > 0.0f && (best.variant < 0 || ms < best.ms)) best = scarf::TcChoice{v, tj, 1, ms, 1};
+      if (ms > 0.0f && v == SCARF_TC_SINGLE && tj == auto_tj) deflt = scarf::TcChoice{v, tj, 1, ms, 1};
     }
   }
   // As for single grids: the default (one-CTA form, automatic row tile)
@@ -1693,6 +1721,7 @@ int scarf_srm_tc_batch_autotune(const scarf_tc_field* fields, int nfields, void*
   out->tile_j = best.tile_j;
   out->permute = 1;
   out->ms = best.ms;
+  out->split = 1;
   return SCARF_OK;
 }
 

@@ -49,10 +49,11 @@ struct TcPlan {
   int pair_i;            // pairs split along i (when bj == 1) instead of j
   int bf16;              // operands split into BF16 (else FP16)
   int terms;             // split products per K step: 3, or 2 (the A-hi x B-lo product dropped)
+  int split;             // harmonic segments per tile (1: none)
   int bix, bjx;          // item grid (bi x bj, halved along the pair axis, rounded up)
   int ax_r, ax_s, ax_c;  // physical axis (0 x, 1 y, 2 z) of i (row-fast), j (row-slow), k (column)
   long long sr, ss, sc;  // field strides of i, j, k in elements
-  size_t off_r, off_s, off_c, off_status, bytes;  // workspace layout
+  size_t off_r, off_s, off_c, off_partial, off_status, bytes;  // workspace layout
 };
 
 // Kernel form for plans made from now on (SCARF_TC_* of scarf3d_b200.h).
@@ -69,8 +70,10 @@ int tc_get_variant();
 // permute: let the longest axis be the column axis (device-field entry
 // points; the default layout keeps k = z, which the slab copy-out relies on).
 // variant >= 0 selects the kernel form (kTcVariant*) instead of the global one.
+// split > 1 divides the harmonics over that many work items per tile
+// (single-CTA forms), their partial sums reduced in order after the kernel.
 bool tc_make_plan(int ndim, const int n[3], int nh, TcPlan* plan, int tj_force = 0, bool permute = false,
-                  int variant = -1);
+                  int variant = -1, int split = 1);
 
 // ---- autotuning (tc_tune.cpp) ----
 // A tuned plan choice for one shape bucket (grid extents rounded up to a
@@ -79,6 +82,7 @@ bool tc_make_plan(int ndim, const int n[3], int nh, TcPlan* plan, int tj_force =
 struct TcChoice {
   int variant, tile_j, permute;
   float ms;
+  int split;  // harmonic segments per tile (device-field plans only)
 };
 // The tuned choice for a grid when tuned plans are enabled and its bucket has
 // an entry (fixed_columns: the caller keeps k = z, as scarf_execute does).

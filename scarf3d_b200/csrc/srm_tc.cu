@@ -81,6 +81,7 @@ struct TcField {
   int n1, n2, n3;
   int bi, bj, ntile_n, stages, chunk_stages;
   int bix, bjx;         // item grid: bi x bj, or CTA pairs along j (bi x ceil(bj/2)) or i (ceil(bi/2) x bj)
+  int bn;               // column tiles
   long long sr, ss, sc; // field strides (elements) of the i, j and k axes
   int pair_i;           // CTA pairs split along i (2D fields: one row block along j)
   int band;             // item order: row blocks along i per band (>= bix: natural order)
@@ -101,6 +102,13 @@ struct TcField {
   // Statistics records of the stored field (null when unused): one per
   // epilogue warp and item, at (local item * CTAs per item + CTA) * 4 + warp.
   Moments* stats;
+  // Split of the harmonics (K) over `split` segments, each its own work item
+  // (1: none). Segment s sums stages [s stages / split, (s + 1) stages /
+  // split) and stores its unscaled partial sums at partial + s * seg_stride
+  // (the field's layout); an ordered reduction then scales their sum.
+  int split;
+  float* partial;
+  long long seg_stride;
 };
 
 struct TcKernelArgs {
@@ -194,6 +202,7 @@ __global__ void tc_build_rs(const TableJob j0, const TableJob* jobs) {
 
 // Column image: per (column block, stage) a 64-B-swizzled K-major tile of
 // ntile_n rows x 32 fp16 ([cos, sin] of 16 harmonics), hi then lo.
+template <bool kBf16>
 __global__ void tc_build_c(const TableJob j0, const TableJob* jobs) {
   const TableJob& T = jobs ? jobs[blockIdx.y] : j0;
   const long long nchunks = static_cast<long long>(T.bn) * T.stages * T.ntile_n * 4;
@@ -222,7 +231,7 @@ __global__ void tc_build_c(const TableJob j0, const TableJob* jobs) {
         cs32 = static_cast<float>(cs);
         sn32 = static_cast<float>(sn);
       }
-      split_pair(cs32, sn32, T.bf16 != 0, hi[u], lo[u]);
+      split_pair(cs32, sn32, kBf16, hi[u], lo[u]);
     }
     uint8_t* base = T.cimg + ((static_cast<size_t>(nb) * T.stages + k) * T.parts + part) *
                                  (2u * part_rows * kRowBytes);
@@ -309,6 +318,7 @@ __global__ void tc_build_rs_factored(const TableJob j0, const TableJob* jobs) {
 
 // Column image: one block per 4-harmonic chunk of a stage at a time
 // (grid-strided), blockIdx.y the field of a batch.
+template <bool kBf16>
 __global__ void tc_build_c_factored(const TableJob j0, const TableJob* jobs) {
   extern __shared__ double2 fsh[];
   const TableJob& T = jobs ? jobs[blockIdx.y] : j0;
@@ -349,7 +359,7 @@ __global__ void tc_build_c_factored(const TableJob j0, const TableJob* jobs) {
           cs32 = static_cast<float>(z.x);
           sn32 = static_cast<float>(z.y);
         }
-        split_pair(cs32, sn32, T.bf16 != 0, hi[u], lo[u]);
+        split_pair(cs32, sn32, kBf16, hi[u], lo[u]);
       }
       uint8_t* base = T.cimg + ((static_cast<size_t>(nb) * T.stages + k) * T.parts + part) *
                                    (2u * part_rows * kRowBytes);
@@ -422,6 +432,7 @@ __global__ void __launch_bounds__(32 * kBuilderWarps) tc_build_rs_warps(const Ta
   }
 }
 
+template <bool kBf16>
 __global__ void __launch_bounds__(32 * kBuilderWarps) tc_build_c_warps(const TableJob j0, const TableJob* jobs) {
   extern __shared__ double2 fsh[];
   const TableJob& T = jobs ? jobs[blockIdx.y] : j0;
@@ -463,7 +474,7 @@ __global__ void __launch_bounds__(32 * kBuilderWarps) tc_build_c_warps(const Tab
           cs32 = static_cast<float>(z.x);
           sn32 = static_cast<float>(z.y);
         }
-        split_pair(cs32, sn32, T.bf16 != 0, hi[u], lo[u]);
+        split_pair(cs32, sn32, kBf16, hi[u], lo[u]);
       }
       uint8_t* base = T.cimg + ((static_cast<size_t>(nb) * T.stages + k) * T.parts + part) *
                                    (2u * part_rows * kRowBytes);
@@ -492,7 +503,7 @@ size_t factor_smem_c(const TcPlan& p) {
 // step latency-bound (a sincos and two barriers), so they get many small
 // blocks: ~64 per SM over all fields.
 void launch_table_builders(const TableJob& T, const TableJob* jobs, int nfields, int max_stages, size_t smem_rs,
-                           size_t smem_c, int nsm, cudaStream_t stream) {
+                           size_t smem_c, int nsm, cudaStream_t stream, bool bf16) {
   const int per_field = std::max(1, nsm * 64 / std::max(1, nfields));
   const int grid_old = std::max(1, std::min(64, nsm * 8 / std::max(1, nfields)));
   // Builder form: warps while each warp's factor tables fit (default), else
@@ -515,20 +526,35 @@ void launch_table_builders(const TableJob& T, const TableJob* jobs, int nfields,
         T, jobs);
   else
     tc_build_rs<<<dim3(jobs ? grid_old : nsm * 8, nfields), 256, 0, stream>>>(T, jobs);
-  if (forced == 0 && smem_c <= warps_limit)
-    tc_build_c_warps<<<dim3(std::min((max_stages * 4 + kBuilderWarps - 1) / kBuilderWarps, per_field), nfields),
-                       32 * kBuilderWarps, kBuilderWarps * smem_c, stream>>>(T, jobs);
-  else if (forced <= 1 && smem_c <= static_cast<size_t>(kFactorSmem))
-    tc_build_c_factored<<<dim3(std::min(max_stages * 4, per_field), nfields), 128, smem_c, stream>>>(T, jobs);
-  else
-    tc_build_c<<<dim3(jobs ? grid_old : nsm * 8, nfields), 256, 0, stream>>>(T, jobs);
+  // The C image's operand type (FP16 or BF16 hi/lo) is uniform over a launch.
+  const dim3 g_warps(std::min((max_stages * 4 + kBuilderWarps - 1) / kBuilderWarps, per_field), nfields);
+  const dim3 g_fact(std::min(max_stages * 4, per_field), nfields);
+  const dim3 g_old(jobs ? grid_old : nsm * 8, nfields);
+  if (forced == 0 && smem_c <= warps_limit) {
+    if (bf16)
+      tc_build_c_warps<true><<<g_warps, 32 * kBuilderWarps, kBuilderWarps * smem_c, stream>>>(T, jobs);
+    else
+      tc_build_c_warps<false><<<g_warps, 32 * kBuilderWarps, kBuilderWarps * smem_c, stream>>>(T, jobs);
+  } else if (forced <= 1 && smem_c <= static_cast<size_t>(kFactorSmem)) {
+    if (bf16)
+      tc_build_c_factored<true><<<g_fact, 128, smem_c, stream>>>(T, jobs);
+    else
+      tc_build_c_factored<false><<<g_fact, 128, smem_c, stream>>>(T, jobs);
+  } else {
+    if (bf16)
+      tc_build_c<true><<<g_old, 256, 0, stream>>>(T, jobs);
+    else
+      tc_build_c<false><<<g_old, 256, 0, stream>>>(T, jobs);
+  }
 }
 
 // One work item: field descriptor and the tile's block coordinates.
 struct Item {
   TcField f;
   int ib, jb, nt;
-  int local;  // item index within its field
+  int local;   // item index within its field
+  int seg;     // harmonic segment (0 without a split)
+  int k0, k1;  // stages [k0, k1) of the segment
 };
 
 __device__ __forceinline__ Item decode_item(const TcKernelArgs& A, int idx) {
@@ -542,8 +568,13 @@ __device__ __forceinline__ Item decode_item(const TcKernelArgs& A, int idx) {
   it.f = A.fields ? A.fields[fid] : A.f0;
   it.local = local;
   const int tiles_m = it.f.bix * it.f.bjx;
-  it.nt = local / tiles_m;
-  const int mt = local - it.nt * tiles_m;
+  const int per_seg = tiles_m * it.f.bn;
+  it.seg = local / per_seg;
+  it.k0 = static_cast<int>(static_cast<long long>(it.seg) * it.f.stages / it.f.split);
+  it.k1 = static_cast<int>(static_cast<long long>(it.seg + 1) * it.f.stages / it.f.split);
+  const int lt = local - it.seg * per_seg;
+  it.nt = lt / tiles_m;
+  const int mt = lt - it.nt * tiles_m;
   // Within a column tile, bands of `band` row blocks along i, each walked
   // over every j (the next band in the opposite j direction).
   const int g = min(it.f.band, it.f.bix);
@@ -554,6 +585,23 @@ __device__ __forceinline__ Item decode_item(const TcKernelArgs& A, int idx) {
   it.ib = b * g + (o - jo * gb);
   it.jb = (b & 1) ? it.f.bjx - 1 - jo : jo;
   return it;
+}
+
+// Number of stages of work item idx (its harmonic segment), read without
+// copying the field descriptor (the generator warps only count stages).
+__device__ __forceinline__ int item_stages(const TcKernelArgs& A, int idx) {
+  int fid = 0, local = idx;
+  if (A.items) {
+    const int2 e = A.items[idx];
+    fid = e.x;
+    local = e.y;
+  }
+  const TcField& f = A.fields ? A.fields[fid] : A.f0;
+  const int split = f.split;
+  if (split <= 1) return f.stages;
+  const int seg = local / (f.bix * f.bjx * f.bn);
+  return static_cast<int>(static_cast<long long>(seg + 1) * f.stages / split -
+                          static_cast<long long>(seg) * f.stages / split);
 }
 
 // W (16 or 32) columns of a chunk drain: all TMEM loads issued before one
@@ -776,7 +824,7 @@ __global__ void __launch_bounds__(kThreads, 1) srm_tc_kernel(const TcKernelArgs 
         const uint8_t* csrc = w.f.cimg + static_cast<size_t>(w.nt) * w.f.stages * bbytes;
         const float2* rsrc = w.f.rimg + static_cast<size_t>(w.ib) * w.f.stages * kStageHarm * A.ti;
         const float2* ssrc = w.f.simg + static_cast<size_t>(w.jb) * w.f.stages * kStageHarm * A.tj;
-        for (int k = 0; k < w.f.stages; ++k) {
+        for (int k = w.k0; k < w.k1; ++k) {
           if (!mbar_wait_bounded(&empty[s], ph ^ 1, A.status)) {
             ok = false;
             break;
@@ -838,8 +886,8 @@ __global__ void __launch_bounds__(kThreads, 1) srm_tc_kernel(const TcKernelArgs 
         if (idx < 0) break;
         const Item w = decode_item(A, idx);
         const uint32_t b_lo_off = A.off_b + w.f.ntile_n * kRowBytes;
-        for (int c0 = 0; c0 < w.f.stages && ok; c0 += w.f.chunk_stages, ++chunk) {
-          const int c1 = min(w.f.stages, c0 + w.f.chunk_stages);
+        for (int c0 = w.k0; c0 < w.k1 && ok; c0 += w.f.chunk_stages, ++chunk) {
+          const int c1 = min(w.k1, c0 + w.f.chunk_stages);
           // The previous chunk must be drained before the buffer restarts.
           if (chunk > 0 && !mbar_wait_bounded(acce, (chunk - 1) & 1, A.status)) {
             ok = false;
@@ -923,22 +971,25 @@ __global__ void __launch_bounds__(kThreads, 1) srm_tc_kernel(const TcKernelArgs 
       const long long plane = w.f.sc;
       float* dst = w.f.field + i * w.f.sr + j * w.f.ss;
       const int k0 = w.nt * w.f.ntile_n;
-      for (int s0 = 0; s0 < w.f.stages; s0 += w.f.chunk_stages, ++chunk) {
-        const bool first = (s0 == 0);
-        const bool last = (s0 + w.f.chunk_stages >= w.f.stages);
+      // A split item stores its segment's unscaled partial sums.
+      float* out = w.f.split > 1 ? w.f.partial + w.seg * w.f.seg_stride + (dst - w.f.field) : dst;
+      const float out_scale = w.f.split > 1 ? 1.0f : w.f.scaling;
+      for (int s0 = w.k0; s0 < w.k1; s0 += w.f.chunk_stages, ++chunk) {
+        const bool first = (s0 == w.k0);
+        const bool last = (s0 + w.f.chunk_stages >= w.k1);
         if (!warp_wait_bounded(accf, chunk & 1, A.status, false)) {
           ok = false;
           break;
         }
         tc_fence_after();
-        drain_chunk(lane_base, kMasterCol, w.f.ntile_n, first, last, row_ok, dst, plane, k0, w.f.n3, w.f.scaling);
+        drain_chunk(lane_base, kMasterCol, w.f.ntile_n, first, last, row_ok, out, plane, k0, w.f.n3, out_scale);
         tc_fence_before();
         __syncwarp();
         if (lane == 0) mbar_arrive(acce);
         if (last && A.slab_cnt) signal_slab(A, w.f, w.ib, w.jb, w.nt, lane);
         if (last && w.f.done_flag) signal_field(w.f, lane);
-        if (last && w.f.stats)
-          record_stats(w.f.stats + w.local * 4 + q, dst, plane, k0, w.f.ntile_n, w.f.n3, row_ok, lane);
+        if (last && w.f.stats)  // (never with a split: out is the field then)
+          record_stats(w.f.stats + w.local * 4 + q, out, plane, k0, w.f.ntile_n, w.f.n3, row_ok, lane);
       }
     }
   } else if (warp >= kGenWarp0) {
@@ -958,7 +1009,7 @@ __global__ void __launch_bounds__(kThreads, 1) srm_tc_kernel(const TcKernelArgs 
         break;
       }
       if (idx < 0) break;
-      const int stages = (A.fields ? A.fields[A.items ? A.items[idx].x : 0] : A.f0).stages;
+      const int stages = item_stages(A, idx);
       for (int k = 0; k < stages; ++k, ++cnt) {
         const int s = cnt % S;
         const uint32_t ph = (cnt / S) & 1;
@@ -1159,7 +1210,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1) srm_tc_
         const uint32_t sbytes = kStageHarm * A.tj * 8u;
         const float2* rsrc = w.f.rimg + static_cast<size_t>(ib) * w.f.stages * kStageHarm * A.ti;
         const float2* ssrc = w.f.simg + static_cast<size_t>(jb) * w.f.stages * kStageHarm * A.tj;
-        for (int k = 0; k < w.f.stages; ++k) {
+        for (int k = w.k0; k < w.k1; ++k) {
           if (!mbar_wait_bounded(&rs_empty[r], rph ^ 1, A.status)) {
             ok = false;
             break;
@@ -1200,7 +1251,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1) srm_tc_
         const Item w = decode_item(A, idx);
         const uint32_t bbytes = w.f.ntile_n * kRowBytes;  // this CTA's half: N / 2 rows, hi and lo
         const uint8_t* csrc = w.f.cimg + (static_cast<size_t>(w.nt) * w.f.stages * 2 + rank) * bbytes;
-        for (int k = 0; k < w.f.stages; ++k) {
+        for (int k = w.k0; k < w.k1; ++k) {
           if (!mbar_wait_bounded_cluster(&empty[s], ph ^ 1, A.status)) {
             ok = false;
             break;
@@ -1247,8 +1298,8 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1) srm_tc_
         if (idx < 0) break;
         const Item w = decode_item(A, idx);
         const uint32_t b_lo_off = A.off_b + (w.f.ntile_n / 2) * kRowBytes;
-        for (int c0 = 0; c0 < w.f.stages && ok; c0 += w.f.chunk_stages, ++chunk) {
-          const int c1 = min(w.f.stages, c0 + w.f.chunk_stages);
+        for (int c0 = w.k0; c0 < w.k1 && ok; c0 += w.f.chunk_stages, ++chunk) {
+          const int c1 = min(w.k1, c0 + w.f.chunk_stages);
           if (chunk > 0 && !mbar_wait_bounded_cluster(acce, (chunk - 1) & 1, A.status)) {
             ok = false;
             break;
@@ -1312,7 +1363,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1) srm_tc_
         }
         release_item(it);
         if (idx < 0) break;
-        const int stages = (A.fields ? A.fields[A.items ? A.items[idx].x : 0] : A.f0).stages;
+        const int stages = item_stages(A, idx);
         for (int k = 0; k < stages; ++k) {
           if (!mbar_wait_bounded(&agen[s], ph, A.status) || !mbar_wait_bounded(&b_full[s], ph, A.status)) {
             ok = false;
@@ -1354,22 +1405,25 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1) srm_tc_
       const long long plane = w.f.sc;
       float* dst = w.f.field + i * w.f.sr + j * w.f.ss;
       const int k0 = w.nt * w.f.ntile_n;
-      for (int s0 = 0; s0 < w.f.stages; s0 += w.f.chunk_stages, ++chunk) {
-        const bool first = (s0 == 0);
-        const bool last = (s0 + w.f.chunk_stages >= w.f.stages);
+      // A split item stores its segment's unscaled partial sums.
+      float* out = w.f.split > 1 ? w.f.partial + w.seg * w.f.seg_stride + (dst - w.f.field) : dst;
+      const float out_scale = w.f.split > 1 ? 1.0f : w.f.scaling;
+      for (int s0 = w.k0; s0 < w.k1; s0 += w.f.chunk_stages, ++chunk) {
+        const bool first = (s0 == w.k0);
+        const bool last = (s0 + w.f.chunk_stages >= w.k1);
         if (!warp_wait_bounded(accf, chunk & 1, A.status, true)) {
           ok = false;
           break;
         }
         tc_fence_after();
-        drain_chunk(lane_base, kMasterCol, w.f.ntile_n, first, last, row_ok, dst, plane, k0, w.f.n3, w.f.scaling);
+        drain_chunk(lane_base, kMasterCol, w.f.ntile_n, first, last, row_ok, out, plane, k0, w.f.n3, out_scale);
         tc_fence_before();
         __syncwarp();
         if (lane == 0) mbar_arrive_cluster(acce0);
         if (last && A.slab_cnt) signal_slab(A, w.f, ib, jb, w.nt, lane);
         if (last && w.f.done_flag) signal_field(w.f, lane);
-        if (last && w.f.stats)
-          record_stats(w.f.stats + (w.local * 2 + static_cast<int>(rank)) * 4 + q, dst, plane, k0, w.f.ntile_n,
+        if (last && w.f.stats)  // (never with a split: out is the field then)
+          record_stats(w.f.stats + (w.local * 2 + static_cast<int>(rank)) * 4 + q, out, plane, k0, w.f.ntile_n,
                        w.f.n3, row_ok, lane);
       }
     }
@@ -1389,7 +1443,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1) srm_tc_
         break;
       }
       if (idx < 0) break;
-      const int stages = (A.fields ? A.fields[A.items ? A.items[idx].x : 0] : A.f0).stages;
+      const int stages = item_stages(A, idx);
       for (int k = 0; k < stages; ++k) {
         // factor tiles in place, and the A slot's previous MMAs complete
         if (!warp_wait_bounded(&rs_full[rr], rph, A.status, false) ||
@@ -1423,6 +1477,18 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1) srm_tc_
   if (warp == 2) {
     tc_fence_after();
     tmem_dealloc_pair(tmem_base, 512);
+  }
+}
+
+// Ordered sum of the split segments' partial sums, then the scaling of
+// scarflib_srm.f90:847 (segments added in index order: deterministic).
+__global__ void tc_split_reduce(const float* __restrict__ partial, int split, long long n, float* field,
+                                float scaling) {
+  const long long stride = static_cast<long long>(gridDim.x) * blockDim.x;
+  for (long long p = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x; p < n; p += stride) {
+    float v = partial[p];
+    for (int sgm = 1; sgm < split; ++sgm) v = __fadd_rn(v, partial[sgm * n + p]);
+    field[p] = __fmul_rn(v, scaling);
   }
 }
 
@@ -1483,6 +1549,8 @@ TcField make_field(const scarf_srm_setup& s, const TcPlan& p, const TableJob& T,
   f.bix = p.bix;
   f.bjx = p.bjx;
   f.pair_i = p.pair_i;
+  f.bn = p.bn;
+  f.split = 1;
   f.band = p.bix;
   f.ntile_n = p.ntile_n;
   f.stages = p.stages;
@@ -1594,7 +1662,7 @@ void tc_set_chunk_harmonics(int harmonics) {
   g_chunk_stages = harmonics > 0 ? (harmonics + kStageHarm - 1) / kStageHarm : kDefaultChunkStages;
 }
 
-bool tc_make_plan(int ndim, const int n[3], int nh, TcPlan* P, int tj_force, bool permute, int variant) {
+bool tc_make_plan(int ndim, const int n[3], int nh, TcPlan* P, int tj_force, bool permute, int variant, int split) {
   if (nh <= 0 || n[0] <= 0 || n[1] <= 0 || n[2] <= 0) return false;
   TcPlan p{};
   // Rows (i, j) over two axes, columns k over the third. By default k = z
@@ -1655,6 +1723,12 @@ bool tc_make_plan(int ndim, const int n[3], int nh, TcPlan* P, int tj_force, boo
                         sizeof(float2));
   p.off_c = off;
   off = align(off + static_cast<size_t>(p.bn) * p.stages * 2 * p.ntile_n * kRowBytes);
+  // Harmonic split (single-CTA forms; at most one segment per stage).
+  p.split = std::max(1, std::min(split, p.stages));
+  if (p.pair) p.split = 1;
+  p.off_partial = off;
+  if (p.split > 1)
+    off = align(off + sizeof(float) * static_cast<size_t>(p.split) * n[0] * n[1] * n[2]);
   p.off_status = off;  // status word, then the work-queue counter
   off = align(off + 256);
   p.bytes = off;
@@ -1726,18 +1800,26 @@ cudaError_t launch_tc_structured(const scarf_srm_setup& s, const int fs[3], cons
                                  const TcSlabSignal* slabs, StatRecord* d_stats) {
   const TableJob T = make_job(s, fs, ds, d_table, nh, p, d_work);
   const int nsm = device_sms();
-  launch_table_builders(T, nullptr, 1, p.stages, factor_smem_rs(p), factor_smem_c(p), nsm, stream);
+  launch_table_builders(T, nullptr, 1, p.stages, factor_smem_rs(p), factor_smem_c(p), nsm, stream, p.bf16 != 0);
   cudaError_t le = cudaGetLastError();
   if (le != cudaSuccess) return le;
 
   TcKernelArgs A{};
   A.f0 = make_field(s, p, T, d_field);
   A.bf16 = p.bf16;
-  A.f0.stats = d_stats;
   A.f0.band = tc_item_band(p, nsm);
+  const long long npts = static_cast<long long>(n[0]) * n[1] * n[2];
+  if (p.split > 1) {
+    // Statistics and slab signals need the final values in the kernel.
+    if (d_stats || (slabs && slabs->nslabs > 0)) return cudaErrorInvalidValue;
+    A.f0.split = p.split;
+    A.f0.partial = reinterpret_cast<float*>(static_cast<uint8_t*>(d_work) + p.off_partial);
+    A.f0.seg_stride = npts;
+  }
+  A.f0.stats = d_stats;
   A.fields = nullptr;
   A.items = nullptr;
-  A.num_items = p.bix * p.bjx * p.bn;
+  A.num_items = p.bix * p.bjx * p.bn * p.split;
   A.status = d_status;
   A.queue = d_status + 1;
   const size_t smem = compute_layout(A, p.ti, p.tj, p.ntile_n, p.tmem_a != 0, p.pair != 0);
@@ -1756,6 +1838,11 @@ cudaError_t launch_tc_structured(const scarf_srm_setup& s, const int fs[3], cons
   }
   if (ev_main0) cudaEventRecord(ev_main0, stream);
   launch_tc_kernel(A, p.tmem_a != 0, p.pair != 0, nsm, smem, stream);
+  if (p.split > 1) {
+    const long long blocks = std::min<long long>((npts + 255) / 256, static_cast<long long>(nsm) * 16);
+    tc_split_reduce<<<static_cast<unsigned>(std::max(1LL, blocks)), 256, 0, stream>>>(A.f0.partial, p.split, npts,
+                                                                                       d_field, s.scaling);
+  }
   if (ev_main1) cudaEventRecord(ev_main1, stream);
   return cudaGetLastError();
 }
@@ -1850,7 +1937,8 @@ cudaError_t tc_batch_launch(const TcBatchPlan& bp, void* d_work, cudaStream_t st
   if (e != cudaSuccess) return e;
   e = cudaMemsetAsync(work + bp.off_done, 0, sizeof(int) * bp.nfields, stream);  // field completion counts
   if (e != cudaSuccess) return e;
-  launch_table_builders(none, jobs, bp.nfields, bp.max_stages, bp.smem_rs, bp.smem_c, nsm, stream);
+  launch_table_builders(none, jobs, bp.nfields, bp.max_stages, bp.smem_rs, bp.smem_c, nsm, stream,
+                        bp.nfields > 0 && bp.plans[0].bf16 != 0);
   e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   TcKernelArgs A{};

@@ -61,6 +61,7 @@ int main(void) {
   printf("scarf_srm_setup.size %zu\n", sizeof(scarf_srm_setup));
   P(scarf_srm_setup, m); P(scarf_srm_setup, ier_full);
   P(scarf_tc_tuning, variant); P(scarf_tc_tuning, tile_j); P(scarf_tc_tuning, permute); P(scarf_tc_tuning, ms);
+  P(scarf_tc_tuning, split);
   printf("scarf_tc_tuning.size %zu\n", sizeof(scarf_tc_tuning));
   return 0;
 }
@@ -193,7 +194,8 @@ def test_tensor_core_plan_and_workspace_without_a_gpu():
     # and C images are 32 x 16 rows, 64 x 8 rows and 2 x 256 columns (hi and lo
     # halves of 64-byte rows) per stage, 8 bytes per R/S entry: 81.92 MB each,
     # plus 256 bytes of status and queue words.
-    assert sb.tc_plan_info(3, [512, 512, 512], 20000) == {"variant": sb.TC_SINGLE, "tile_j": 8, "permute": 0}
+    assert sb.tc_plan_info(3, [512, 512, 512], 20000) == {"variant": sb.TC_SINGLE, "tile_j": 8, "permute": 0,
+                                                          "split": 1}
     stages = 20000 // 16
     image = stages * 16 * 512 * 8
     assert sb.tc_workspace_bytes(3, [512, 512, 512], 20000) == 3 * image + 256

@@ -171,3 +171,46 @@ def test_operand_precision_settings_against_fp64(variant):
     assert err[(sb.TC_BF16, 3)] > err[(sb.TC_FP16, 3)]
     assert err[(sb.TC_FP16, 2)] > 1e-5
     assert err[(sb.TC_BF16, 2)] > err[(sb.TC_FP16, 2)]
+
+
+@pytest.mark.parametrize("variant", [sb.TC_SINGLE, sb.TC_SINGLE_TMEM_A])
+@pytest.mark.parametrize("split", [2, 3, 8])
+def test_harmonic_split_matches_unsplit_and_fp64(variant, split, monkeypatch):
+    """Splitting the harmonics over several work items per tile (partial sums
+    reduced in segment order after the kernel) gives the unsplit sum up to
+    FP32 rounding, the FP64 oracle within the tensor-core tolerance, and the
+    same bits on every run."""
+    case = structured_case("gs3d_aniso", nharm=900)
+    s = sb.compute_setup(case["pp"])
+    tab, _ = sb.sample(case["pp"], s)
+    base = _run(variant, s, case["fs"], case["n"], case["ds"], tab)
+    monkeypatch.setenv("SCARF3D_B200_TC_SPLIT", str(split))
+    assert sb.tc_plan_info(3, case["n"], len(tab))["split"] == split
+    a = _run(variant, s, case["fs"], case["n"], case["ds"], tab)
+    b = _run(variant, s, case["fs"], case["n"], case["ds"], tab)
+    assert np.all(np.isfinite(a))
+    assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
+    assert rel_rms(a, base) <= 2e-6
+    ref64 = oracle.sum_structured(oracle.setup(case["op"]), case["fs"], case["n"], case["ds"], tab, f64=True)
+    assert rel_rms(a, ref64) <= 1e-5
+
+
+def test_autotuner_offers_splits_for_small_grids():
+    """A grid with fewer tiles than SMs gets split candidates; whatever the
+    tuner records is followed by the device-field entry point and agrees with
+    the FP64 oracle."""
+    case = structured_case("gs3d_aniso", nharm=2000)
+    s = sb.compute_setup(case["pp"])
+    tab, _ = sb.sample(case["pp"], s)
+    d_tab = torch.from_numpy(np.ascontiguousarray(tab.reshape(-1))).cuda()
+    try:
+        t = sb.tc_autotune(s, case["fs"], case["n"], case["ds"], d_tab.data_ptr(), len(tab))
+        sb.set_tc_autotune(1)
+        info = sb.tc_plan_info(3, case["n"], len(tab))
+        assert info["split"] == t["split"] >= 1
+        sb.set_tc_variant(t["variant"])
+        f = _run(t["variant"], s, case["fs"], case["n"], case["ds"], tab)
+    finally:
+        sb.set_tc_autotune(0)
+    ref64 = oracle.sum_structured(oracle.setup(case["op"]), case["fs"], case["n"], case["ds"], tab, f64=True)
+    assert rel_rms(f, ref64) <= 1e-5
