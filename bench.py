@@ -879,6 +879,62 @@ def run_b200(args, w):
         dist.destroy_process_group()
 
 
+def run_profile_leg(args, w):
+    """One leg alone, for ncu captures of its kernels (prints no bench line):
+    tc = table builders + tensor-core sum (warm-up, then one launch) on the
+    grid and harmonic count given; direct = the FP32 direct sum over 2 000
+    harmonics of it; batched = the 256-field batch (device-assisted sampling,
+    builders, persistent launch); fim = scarf_execute with method 0 on the
+    grid; execute = scarf_execute (tensor-core form, statistics records) into
+    a device field."""
+    import torch
+
+    import scarf3d_b200 as sb
+
+    torch.cuda.set_device(0)
+    if args.profile_leg == "batched":
+        run_batched(args)
+        return
+    n = [w["nx"], w["ny"], w["nz"]]
+    ds = w["ds"]
+    fs = [1, 1, 1]
+    ds32 = np.float32(ds)
+    nc = [0.0, 0.0, 0.0]
+    fc = [float(np.float32(n[c] - 1) * ds32) for c in range(3)]
+    kw = dict(acf=w["acf"], nharm=w["nharm"], seed=w["seed"], hurst=w["hurst"], sigma=w["sigma"], ds=ds, cl=w["cl"])
+    if args.profile_leg in ("fim", "execute"):
+        sb.set_nharm(w["nharm"])
+        sb.set_form(sb.FORM_TC)
+        sb.scarf_initialize(fs=fs, fe=n, ds=ds, acf=w["acf"], cl=w["cl"], sigma=w["sigma"],
+                            method=0 if args.profile_leg == "fim" else 1, hurst=w["hurst"],
+                            nc=np.asarray(nc, np.float32), fc=np.asarray(fc, np.float32))
+        dev = torch.empty(int(np.prod(n)), dtype=torch.float32, device="cuda")
+        for _ in range(args.warmup + args.steps):
+            sb.scarf_execute(w["seed"], dev)
+        sb.scarf_finalize()
+        return
+    p = sb.make_params(nc=nc, fc=fc, **kw)
+    s = sb.compute_setup(p)
+    tab, _ = sb.sample(p, s)
+    nh = len(tab) if args.profile_leg == "tc" else min(DIRECT_HARM, len(tab))
+    d_tab = torch.from_numpy(tab.reshape(-1).copy()).cuda()
+    field = torch.empty(int(np.prod(n)), dtype=torch.float32, device="cuda")
+    sptr = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    wb = sb.tc_workspace_bytes(3, n, nh)
+    work = torch.empty(max(wb, 1), dtype=torch.uint8, device="cuda")
+    for _ in range(args.warmup + args.steps):
+        if args.profile_leg == "tc":
+            sb.check(sb.lib.scarf_srm_tc_structured(ctypes.byref(s), _i3(fs), _i3(n), ds,
+                                                    ctypes.c_void_p(d_tab.data_ptr()), nh,
+                                                    ctypes.c_void_p(field.data_ptr()),
+                                                    ctypes.c_void_p(work.data_ptr()), wb, sptr))
+        else:
+            sb.check(sb.lib.scarf_srm_direct_structured(ctypes.byref(s), _i3(fs), _i3(n), ds,
+                                                        ctypes.c_void_p(d_tab.data_ptr()), nh,
+                                                        ctypes.c_void_p(field.data_ptr()), sptr))
+    torch.cuda.synchronize()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -891,6 +947,8 @@ def main():
     ap.add_argument("--no-autotune", action="store_true", help="default plans instead of autotuned ones")
     ap.add_argument("--no-precision", action="store_true", help="skip the operand-precision comparison")
     ap.add_argument("--no-fim", action="store_true", help="skip the FIM (method 0) measurement")
+    ap.add_argument("--profile-leg", choices=["tc", "direct", "batched", "fim", "execute"], default=None,
+                    help="run one leg alone for a profiler capture (no bench line)")
     ap.add_argument("--configs", default="1,2,5",
                     help="other configurations to measure (comma list of 1, 2, 5; empty to skip)")
     args = ap.parse_args()
@@ -899,6 +957,9 @@ def main():
         w["nx"], w["ny"], w["nz"] = args.grid
     if args.nharm:
         w["nharm"] = args.nharm
+    if args.profile_leg:
+        run_profile_leg(args, w)
+        return
     if args.impl == "reference":
         if int(os.environ.get("RANK", "0")) != 0:
             return

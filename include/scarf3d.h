@@ -1,12 +1,12 @@
 /*
- * scarf3d.h -- reference-compatible C/C++ interface of the B200 SRM library.
+ * scarf3d.h -- reference-compatible C/C++ interface of the B200 SCARF3D library.
  *
  * Same names, argument meaning and struct layout as SCARF3D's own header
  * (src/scarf3d.h:52-85 and the C++ wrapper :91-159), so that C and C++ callers
  * of the reference link against libscarf3d_b200.so unchanged. Single precision
- * only (the reference's default build; `real` = float). Only the SRM method
- * (scarf_opt.method == 1) is implemented; a call with method 0 (FIM) records
- * SCARF_ERR_UNSUPPORTED, readable with scarf_last_error().
+ * only (the reference's default build; `real` = float). scarf_opt.method == 1
+ * selects the SRM, 0 (the default) the FIM (scarflib_fim.f90:141-1104, on
+ * cuFFT, with the reference's default build options: no rotated axes).
  *
  * Entry points and the reference interface each one replaces:
  *   scarf_opt_init           <- src/c_binding.c:62-80
@@ -16,6 +16,7 @@
  *                               -> scarflib.f90:195-296
  *   scarf_execute            <- src/c_binding.c:138-143 -> f_binding.f90:181-217
  *                               -> scarflib.f90:302-426 -> scarflib_srm.f90:105-929
+ *                               or scarflib_fim.f90:141-1104
  *   scarf_finalize           <- src/c_binding.c:145-150 -> scarflib.f90:432-455
  *   scarf_io_one             <- src/c_binding.c:154-158 -> scarflib_common.f90:245-418
  *   scarf_io_slice           <- src/c_binding.c:160-164 -> scarflib_common.f90:527-646
