@@ -217,6 +217,15 @@ int scarf_set_sampler_pass_pairs(long long pairs);
  * d_table: nh rows of 5 floats on the device. */
 int scarf_srm_direct_structured(const scarf_srm_setup *s, const int fs[3], const int n[3], float ds,
                                 const float *d_table, int nh, float *d_field, void *stream);
+/* sin/cos of the FP32 direct sum (no counterpart in the reference, which
+ * calls the Fortran intrinsics): SCARF_SINCOS_FAST (default) reduces each
+ * phase to [-pi, pi] by Cody-Waite's method (2 pi in three floats, FMA) and
+ * takes the SFU's sin and cos (~6e-7 absolute per term; fields within ~4e-7
+ * rel-RMS of the reference's FP32 arithmetic); SCARF_SINCOS_ACCURATE uses
+ * CUDA's sincosf (~1 ulp; ~2e-7 rel-RMS) at about half the speed. */
+#define SCARF_SINCOS_ACCURATE 0
+#define SCARF_SINCOS_FAST 1
+int scarf_set_direct_sincos(int mode);
 /* FP32 direct sum over npts points (x, y, z device arrays). */
 int scarf_srm_direct_points(const scarf_srm_setup *s, const float *d_x, const float *d_y, const float *d_z,
                             long long npts, const float *d_table, int nh, float *d_field, void *stream);

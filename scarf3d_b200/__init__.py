@@ -37,6 +37,7 @@ EXPORTED_SYMBOLS = (
     "scarf_last_kernel_ms", "scarf_set_device_memory_cap", "scarf_device_memory_in_use",
     "scarf_release_device_memory",
     "scarf_selftest_wait_limit", "scarf_set_tc_chunk", "scarf_set_tc_variant", "scarf_set_tc_precision",
+    "scarf_set_direct_sincos",
     "scarf_set_output_overlap",
     "scarf_execute_ex",
     "scarf_srm_compute_setup", "scarf_srm_sample", "scarf_srm_sample_device", "scarf_srm_sample_device_batch",
@@ -133,6 +134,7 @@ def _load() -> ctypes.CDLL:
         "scarf_set_tc_chunk": (c_int, [c_int]),
         "scarf_set_tc_variant": (c_int, [c_int]),
         "scarf_set_tc_precision": (c_int, [c_int, c_int]),
+        "scarf_set_direct_sincos": (c_int, [c_int]),
         "scarf_set_output_overlap": (c_int, [c_int]),
         "scarf_execute_ex": (c_int, [c_int, c_void_p, fp, c_int]),
         "scarf_srm_compute_setup": (c_int, [ctypes.POINTER(SrmParams), ctypes.POINTER(SrmSetup)]),
@@ -415,6 +417,13 @@ def set_tc_variant(variant: int):
 
 
 TC_FP16, TC_BF16 = 0, 1
+SINCOS_ACCURATE, SINCOS_FAST = 0, 1
+
+
+def set_direct_sincos(mode: int):
+    """sin/cos of the FP32 direct sum: SINCOS_FAST (default: Cody-Waite
+    reduction + SFU) or SINCOS_ACCURATE (CUDA's sincosf)."""
+    check(lib.scarf_set_direct_sincos(int(mode)))
 
 
 def set_tc_precision(operand_type: int = 0, terms: int = 3):

@@ -1411,6 +1411,14 @@ int scarf_set_tc_variant(int variant) {
   return SCARF_OK;
 }
 
+int scarf_set_direct_sincos(int mode) {
+  if (mode != SCARF_SINCOS_FAST && mode != SCARF_SINCOS_ACCURATE)
+    return fail(SCARF_ERR_ARG, "direct-sum sincos mode %d (0 accurate, 1 fast)", mode);
+  std::lock_guard<std::mutex> lk(g_mu);
+  direct_set_sincos(mode == SCARF_SINCOS_FAST ? 1 : 0);
+  return SCARF_OK;
+}
+
 int scarf_set_tc_precision(int operand_type, int terms) {
   std::lock_guard<std::mutex> lk(g_mu);
   if (!tc_set_precision(operand_type, terms))

@@ -49,7 +49,36 @@ __device__ __forceinline__ void rotate(const DirectArgs& A, float x, float y, fl
   p3 = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(A.m[6], x), __fmul_rn(A.m[7], y)), __fmul_rn(A.m[8], z)), A.bar[2]);
 }
 
-template <bool kStructured>
+// sin and cos of an FP32 phase, two ways.
+// Accurate (kFast = false): CUDA's sincosf, correctly rounded to ~1 ulp with
+// full range reduction. Fast (default): the phase reduced to [-pi, pi] by
+// Cody-Waite's method (Cody & Waite, "Software Manual for the Elementary
+// Functions", 1980) with 2 pi split into three floats (C1 + C2 + C3; the
+// residual is 4e-23), each product applied by one FMA, then the SFU's
+// __sinf/__cosf, whose absolute error on [-pi, pi] is about 2^-21.4. For the
+// phases here (|arg| < 1e4 rad) the reduced argument is within ~2.5e-7 of
+// exact, so each term is within ~6e-7 absolute, and fields agree with the
+// FP32 restatement (glibc sinf/cosf) to ~4e-7 of their standard deviation.
+constexpr float kInv2Pi = 0x1.45f306p-3f;
+constexpr float kTwoPi1 = 0x1.921fb6p+2f;
+constexpr float kTwoPi2 = -0x1.777a5cp-23f;
+constexpr float kTwoPi3 = -0x1.ee59dap-48f;
+
+template <bool kFast>
+__device__ __forceinline__ void phase_sincos(float arg, float* sn, float* cs) {
+  if constexpr (kFast) {
+    const float j = rintf(__fmul_rn(arg, kInv2Pi));
+    float r = fmaf(-j, kTwoPi1, arg);
+    r = fmaf(-j, kTwoPi2, r);
+    r = fmaf(-j, kTwoPi3, r);
+    *sn = __sinf(r);
+    *cs = __cosf(r);
+  } else {
+    sincosf(arg, sn, cs);
+  }
+}
+
+template <bool kStructured, bool kFast>
 __global__ void __launch_bounds__(kThreads) srm_direct_kernel(const DirectArgs A) {
   __shared__ __align__(128) float s_tab[2][kTile * kRow];
   __shared__ __align__(8) uint64_t s_full[2];
@@ -126,7 +155,7 @@ __global__ void __launch_bounds__(kThreads) srm_direct_kernel(const DirectArgs A
       for (int q = 0; q < kPts; ++q) {
         const float arg = __fadd_rn(__fadd_rn(__fmul_rn(v1, P1[q]), __fmul_rn(v2, P2[q])), __fmul_rn(v3, P3[q]));
         float sn, cs;
-        sincosf(arg, &sn, &cs);
+        phase_sincos<kFast>(arg, &sn, &cs);
         acc[q] = __fadd_rn(__fadd_rn(acc[q], __fmul_rn(a, sn)), __fmul_rn(b, cs));
       }
     }
@@ -186,6 +215,11 @@ __global__ void __launch_bounds__(kThreads) srm_direct_kernel(const DirectArgs A
 
 }  // namespace
 
+int g_direct_fast = 1;
+
+void direct_set_sincos(int fast) { g_direct_fast = fast ? 1 : 0; }
+int direct_get_sincos() { return g_direct_fast; }
+
 long long direct_stat_records(long long npts) {
   const long long per_block = static_cast<long long>(kThreads) * kPts;
   return (npts + per_block - 1) / per_block;
@@ -213,7 +247,10 @@ cudaError_t launch_direct_structured(const scarf_srm_setup& s, const int fs[3], 
   const long long per_block = static_cast<long long>(kThreads) * kPts;
   const long long blocks = (A.npts + per_block - 1) / per_block;
   if (blocks <= 0) return cudaSuccess;
-  srm_direct_kernel<true><<<static_cast<unsigned>(blocks), kThreads, 0, stream>>>(A);
+  if (g_direct_fast)
+    srm_direct_kernel<true, true><<<static_cast<unsigned>(blocks), kThreads, 0, stream>>>(A);
+  else
+    srm_direct_kernel<true, false><<<static_cast<unsigned>(blocks), kThreads, 0, stream>>>(A);
   return cudaGetLastError();
 }
 
@@ -236,7 +273,10 @@ cudaError_t launch_direct_points(const scarf_srm_setup& s, const float* d_x, con
   const long long per_block = static_cast<long long>(kThreads) * kPts;
   const long long blocks = (npts + per_block - 1) / per_block;
   if (blocks <= 0) return cudaSuccess;
-  srm_direct_kernel<false><<<static_cast<unsigned>(blocks), kThreads, 0, stream>>>(A);
+  if (g_direct_fast)
+    srm_direct_kernel<false, true><<<static_cast<unsigned>(blocks), kThreads, 0, stream>>>(A);
+  else
+    srm_direct_kernel<false, false><<<static_cast<unsigned>(blocks), kThreads, 0, stream>>>(A);
   return cudaGetLastError();
 }
 

@@ -19,6 +19,10 @@ struct StatRecord {
 };
 
 // ---- direct sum (srm_direct.cu) ----
+// sin/cos of the direct sum: 1 = Cody-Waite reduction + SFU (default),
+// 0 = CUDA's sincosf.
+void direct_set_sincos(int fast);
+int direct_get_sincos();
 // d_stats (optional): direct_stat_records(npts) records.
 long long direct_stat_records(long long npts);
 cudaError_t launch_direct_structured(const scarf_srm_setup& s, const int fs[3], const int n[3], float ds,

@@ -112,3 +112,33 @@ def test_tc_agrees_with_direct(lib, orc):
     tc = _tc_structured(lib, case, tab)
     direct = _direct_structured(lib, case, tab)
     assert rel_rms(tc, direct) <= 1e-4
+
+
+@pytest.mark.parametrize("mode,tol", [(1, 1e-6), (0, 3e-7)])
+def test_direct_sincos_modes_on_large_phases(lib, orc, mode, tol):
+    """Points over 20 x 20 x 10 km with 1500/500 m correlation lengths put
+    the phases at thousands of radians: the fast mode (Cody-Waite reduction
+    to [-pi, pi] + SFU sin/cos) stays within 1e-6 of the FP32 restatement,
+    CUDA's sincosf within 3e-7."""
+    x, y, z = random_points(20000, seed=11)
+    kw = dict(acf=1, nharm=3000, seed=7, hurst=0.0, sigma=0.1, ds=100.0, cl=[1500.0, 1500.0, 500.0])
+    nc = [float(a.min()) for a in (x, y, z)]
+    fc = [float(a.max()) for a in (x, y, z)]
+    pp = lib.make_params(nc=nc, fc=fc, **kw)
+    s = lib.compute_setup(pp)
+    tab, _ = lib.sample(pp, s)
+    so = orc.setup(orc.params(nc=nc, fc=fc, **kw))
+    dx, dy, dz, dt = (_dev(a) for a in (x, y, z, tab.reshape(-1)))
+    out = torch.empty(len(x), dtype=torch.float32, device="cuda")
+    try:
+        lib.set_direct_sincos(mode)
+        lib.check(lib.lib.scarf_srm_direct_points(ctypes.byref(s), ctypes.c_void_p(dx.data_ptr()),
+                                                  ctypes.c_void_p(dy.data_ptr()), ctypes.c_void_p(dz.data_ptr()),
+                                                  len(x), ctypes.c_void_p(dt.data_ptr()), len(tab),
+                                                  ctypes.c_void_p(out.data_ptr()), None))
+    finally:
+        lib.set_direct_sincos(1)
+    got = out.cpu().numpy()
+    ref32 = orc.sum_points(so, x, y, z, tab)
+    assert rel_rms(got, ref32) <= tol
+    assert np.max(np.abs(got - ref32)) <= 1e-5 * ref32.std()
