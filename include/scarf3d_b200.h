@@ -175,6 +175,17 @@ int scarf_srm_tc_plan_info(int ndim, const int n[3], int nh, scarf_tc_tuning *ou
 int scarf_srm_tc_autotune(const scarf_srm_setup *s, const int fs[3], const int n[3], float ds, const float *d_table,
                           int nh, int fixed_columns, void *stream, scarf_tc_tuning *out);
 
+/* The FIM's internal (FFT) grid for a domain nc..fc (no counterpart in the
+ * reference; it lets a caller size the device memory of method 0): points
+ * per axis, offset of the first node, and the reference's info(1:2) flags
+ * (scarflib_fim.f90:787-818). ndim 2 or 3; pad as scarf_opt.pad. */
+int scarf_fim_internal_grid(int ndim, const float nc[3], const float fc[3], float dh, const float cl[3], int pad,
+                            int npts[3], float off_axis[3], float flags[2]);
+/* Device bytes the FIM workspace of that grid takes (spectrum, transform
+ * output, statistics records, points of interest; cuFFT's own work area
+ * comes on top). */
+size_t scarf_fim_workspace_bytes(const int npts[3], int npoi);
+
 /* Status-returning scarf_execute (c_binding.c:138-143); stats[8] as the
  * reference fills it (stats[4] host seconds, stats[5] device seconds). */
 int scarf_execute_ex(int seed, float *field, float stats[8], int flags);

@@ -37,7 +37,7 @@ EXPORTED_SYMBOLS = (
     "scarf_last_kernel_ms", "scarf_set_device_memory_cap", "scarf_device_memory_in_use",
     "scarf_release_device_memory",
     "scarf_selftest_wait_limit", "scarf_set_tc_chunk", "scarf_set_tc_variant", "scarf_set_tc_precision",
-    "scarf_set_direct_sincos",
+    "scarf_set_direct_sincos", "scarf_fim_internal_grid", "scarf_fim_workspace_bytes",
     "scarf_set_output_overlap",
     "scarf_execute_ex",
     "scarf_srm_compute_setup", "scarf_srm_sample", "scarf_srm_sample_device", "scarf_srm_sample_device_batch",
@@ -135,6 +135,9 @@ def _load() -> ctypes.CDLL:
         "scarf_set_tc_variant": (c_int, [c_int]),
         "scarf_set_tc_precision": (c_int, [c_int, c_int]),
         "scarf_set_direct_sincos": (c_int, [c_int]),
+        "scarf_fim_internal_grid": (c_int, [c_int, c_void_p, c_void_p, ctypes.c_float, c_void_p, c_int, c_void_p,
+                                            c_void_p, c_void_p]),
+        "scarf_fim_workspace_bytes": (ctypes.c_size_t, [c_void_p, c_int]),
         "scarf_set_output_overlap": (c_int, [c_int]),
         "scarf_execute_ex": (c_int, [c_int, c_void_p, fp, c_int]),
         "scarf_srm_compute_setup": (c_int, [ctypes.POINTER(SrmParams), ctypes.POINTER(SrmSetup)]),
@@ -430,6 +433,20 @@ def set_tc_precision(operand_type: int = 0, terms: int = 3):
     """Operand split of the tensor-core form for plans made afterwards:
     TC_FP16 (default) or TC_BF16 hi/lo parts, 3 (default) or 2 products."""
     check(lib.scarf_set_tc_precision(int(operand_type), int(terms)))
+
+
+def fim_internal_grid(ndim: int, nc, fc, dh: float, cl, pad: int = 0):
+    """(npts[3], off_axis[3], flags[2]) of the FIM's internal grid."""
+    ncv = np.zeros(3, np.float32)
+    fcv = np.zeros(3, np.float32)
+    clv = np.zeros(3, np.float32)
+    ncv[:len(nc)], fcv[:len(fc)], clv[:len(cl)] = nc, fc, cl
+    npts = np.zeros(3, np.int32)
+    off = np.zeros(3, np.float32)
+    flags = np.zeros(2, np.float32)
+    check(lib.scarf_fim_internal_grid(int(ndim), ncv.ctypes.data, fcv.ctypes.data, float(dh), clv.ctypes.data,
+                                      int(pad), npts.ctypes.data, off.ctypes.data, flags.ctypes.data))
+    return [int(v) for v in npts], off, flags
 
 
 def set_device_memory_cap(nbytes: int):

@@ -1411,6 +1411,37 @@ int scarf_set_tc_variant(int variant) {
   return SCARF_OK;
 }
 
+int scarf_fim_internal_grid(int ndim, const float nc[3], const float fc[3], float dh, const float cl[3], int pad,
+                            int npts[3], float off_axis[3], float flags[2]) {
+  if ((ndim != 2 && ndim != 3) || !nc || !fc || !cl || !npts || !off_axis || !flags || !(dh > 0.0f))
+    return fail(SCARF_ERR_ARG, "invalid FIM grid arguments");
+  FimInputs in{};
+  in.ndim = ndim;
+  in.dh = dh;
+  in.pad = pad;
+  for (int c = 0; c < 3; ++c) {
+    in.nc[c] = nc[c];
+    in.fc[c] = fc[c];
+    in.cl[c] = (c < ndim) ? cl[c] : 0.0f;
+  }
+  FimGrid g{};
+  fim_grid(in, &g);
+  for (int c = 0; c < 3; ++c) {
+    npts[c] = g.npts[c];
+    off_axis[c] = g.off_axis[c];
+  }
+  flags[0] = g.info0;
+  flags[1] = g.info1;
+  return SCARF_OK;
+}
+
+size_t scarf_fim_workspace_bytes(const int npts[3], int npoi) {
+  if (!npts || npts[0] <= 0 || npts[1] <= 0 || npts[2] <= 0 || npoi < 0) return 0;
+  FimGrid g{};
+  for (int c = 0; c < 3; ++c) g.npts[c] = npts[c];
+  return fim_workspace_bytes(g, npoi);
+}
+
 int scarf_set_direct_sincos(int mode) {
   if (mode != SCARF_SINCOS_FAST && mode != SCARF_SINCOS_ACCURATE)
     return fail(SCARF_ERR_ARG, "direct-sum sincos mode %d (0 accurate, 1 fast)", mode);

@@ -69,3 +69,25 @@ def test_field_properties():
     f2, _, _ = fim.execute_structured(fs=[1, 1, 1], fe=[64, 64, 64], ds=50.0, acf=0, cl=[400.0] * 3, sigma=0.05,
                                       hurst=0.5, seed=1235, pad=1, rescale=1)
     assert abs(float(np.std(f2.astype(np.float64))) - 0.05) < 0.01
+
+
+def test_library_internal_grid_equals_the_oracle():
+    """The library's FIM grid (host code of the product) and the oracle's
+    restatement agree bit for bit over random domains, steps and lengths."""
+    import scarf3d_b200 as sb
+    rng = np.random.default_rng(17)
+    for _ in range(400):
+        ndim = int(rng.integers(2, 4))
+        nc = (rng.uniform(-5000.0, 5000.0, 3)).astype(np.float32)
+        fc = (nc + rng.uniform(10.0, 30000.0, 3)).astype(np.float32)
+        if ndim == 2:
+            nc[2] = fc[2] = 0.0
+        dh = np.float32(rng.uniform(5.0, 200.0))
+        cl = rng.uniform(50.0, 5000.0, ndim).astype(np.float32)
+        pad = int(rng.integers(0, 2))
+        a = sb.fim_internal_grid(ndim, nc, fc, dh, cl, pad)
+        b = fim.grid(ndim, nc, fc, dh, cl, pad)
+        assert a[0] == b[0]
+        assert np.array_equal(np.asarray(a[1]).view(np.uint32), np.asarray(b[1]).view(np.uint32))
+        assert np.array_equal(a[2], b[2])
+    assert sb.lib.scarf_fim_workspace_bytes(np.asarray([64, 64, 64], np.int32).ctypes.data, 2) > 64 * 64 * 33 * 8
