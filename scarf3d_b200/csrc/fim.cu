@@ -311,11 +311,17 @@ bool load_cufft() {
 
 std::mutex g_fim_mu;
 int g_fim_tables_dev = -1;
+unsigned long long g_fim_tables_ctx = 0;
 
+// The generator tables in this module's device and constant memory, uploaded
+// once per device context (a reset context has a new id; when the id cannot
+// be read they are uploaded on every call).
 cudaError_t ensure_fim_tables() {
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess || dev == g_fim_tables_dev) return e;
+  if (e != cudaSuccess) return e;
+  const unsigned long long ctx = current_context_id();
+  if (dev == g_fim_tables_dev && ctx != 0 && ctx == g_fim_tables_ctx) return cudaSuccess;
   static const std::vector<uint32_t> pw = device_pow_tables();
   e = cudaMemcpyToSymbol(g_fim_pow, pw.data(), sizeof(uint32_t) * pw.size());
   if (e != cudaSuccess) return e;
@@ -335,6 +341,7 @@ cudaError_t ensure_fim_tables() {
   if ((e = cudaMemcpyToSymbol(c_lane, lane, sizeof(lane))) != cudaSuccess) return e;
   if ((e = cudaMemcpyToSymbol(c_step, step, sizeof(step))) != cudaSuccess) return e;
   g_fim_tables_dev = dev;
+  g_fim_tables_ctx = current_context_id();
   return cudaSuccess;
 }
 

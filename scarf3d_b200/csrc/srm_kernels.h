@@ -10,6 +10,10 @@
 
 namespace scarf {
 
+// Process-unique id of the current CUDA context (0 when it cannot be read),
+// for caches of per-context state (cuda_context.cpp).
+unsigned long long current_context_id();
+
 // Statistics records written by the summation kernels when asked for: one
 // (count, mean, M2) triple (FP64) per epilogue warp and work item of the
 // tensor-core form, or per block of the direct form, merged in record order by

@@ -29,7 +29,6 @@
 // The plan (kernel form, row tile, column axis) follows the same rule as
 // scarf_srm_tc_structured, tuned plans included, so both entry points run the
 // same plan and scarf_srm_tc_workspace_bytes gives the scratch this one needs.
-#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -55,35 +54,6 @@ struct ScratchSlot {
   void* ptr;
 };
 ScratchSlot g_noalloc_slot[kMaxDevices] = {};
-
-using CtxGetCurrentFn = CUresult (*)(CUcontext*);
-using CtxGetIdFn = CUresult (*)(CUcontext, unsigned long long*);
-
-// Unique id of the current context (0 when it cannot be read). The driver
-// routines are fetched through the runtime, so the library does not link
-// libcuda itself.
-unsigned long long current_context_id() {
-  static CtxGetCurrentFn get_current = nullptr;
-  static CtxGetIdFn get_id = nullptr;
-  static std::once_flag once;
-  std::call_once(once, [] {
-    void* f = nullptr;
-    cudaDriverEntryPointQueryResult q{};
-    if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &f, 12000, cudaEnableDefault, &q) == cudaSuccess &&
-        q == cudaDriverEntryPointSuccess)
-      get_current = reinterpret_cast<CtxGetCurrentFn>(f);
-    f = nullptr;
-    if (cudaGetDriverEntryPointByVersion("cuCtxGetId", &f, 12000, cudaEnableDefault, &q) == cudaSuccess &&
-        q == cudaDriverEntryPointSuccess)
-      get_id = reinterpret_cast<CtxGetIdFn>(f);
-  });
-  if (!get_current || !get_id) return 0;
-  CUcontext ctx = nullptr;
-  unsigned long long id = 0;
-  if (get_current(&ctx) != CUDA_SUCCESS || !ctx) return 0;
-  if (get_id(ctx, &id) != CUDA_SUCCESS) return 0;
-  return id;
-}
 
 // Device address of g_noalloc_scratch in the current context. In host code
 // the symbol itself is only a host-side stand-in and must never be passed to
