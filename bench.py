@@ -302,7 +302,7 @@ def run_batched(args, nfields=256):
     hosts = [torch.empty(o.numel(), dtype=torch.float32, pin_memory=True) for o in outs]
     batch.set_host_outputs([h.data_ptr() for h in hosts])
     torch.cuda.synchronize()
-    # (a) One step alone (latency): sample, upload, launch, copy out.
+    # One step at a time: sample, upload, launch, copy out (median of 3).
     lat = []
     for _ in range(3):
         t0 = time.perf_counter()
@@ -314,30 +314,6 @@ def run_batched(args, nfields=256):
         lat.append(time.perf_counter() - t0)
     t_e2e = float(np.median(lat))
     e2e_ok = all(torch.equal(h, o.cpu()) for h, o in zip(hosts, outs))
-    # (b) Steady state: each step's sampling (its GPU scans on a side stream,
-    # its host walks on the host) runs while the previous step's launch
-    # computes; host tables double-buffered so a step never overwrites tables
-    # still being uploaded. Every step still samples, uploads, launches and
-    # copies all of its fields out inside the timed region.
-    h_tabs_b = torch.empty(int(offs[-1]), dtype=torch.float32, pin_memory=True)
-    views_b = [h_tabs_b[int(offs[i]):int(offs[i + 1])].numpy() for i in range(nfields)]
-    side = torch.cuda.Stream()
-    bufs = [(h_tabs, views), (h_tabs_b, views_b)]
-    k_pipe = max(3, min(args.steps, 6))
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    sb.sample_device_batch(params, setups, side.cuda_stream, out=bufs[0][1])
-    for step in range(k_pipe):
-        hb = bufs[step % 2][0]
-        stream.wait_stream(side)
-        d_tabs.copy_(hb, non_blocking=True)
-        graph.replay()
-        if step + 1 < k_pipe:
-            sb.sample_device_batch(params, setups, side.cuda_stream, out=bufs[(step + 1) % 2][1])
-        batch.wait(stream.cuda_stream)
-    torch.cuda.synchronize()
-    t_pipe = (time.perf_counter() - t0) / k_pipe
-    pipe_ok = all(torch.equal(h, o.cpu()) for h, o in zip(hosts[:8], outs[:8]))
     del graph
     sb.set_tc_variant(sb.TC_SINGLE)
     return {"fields": nfields, "work_pt_harm": work, "value": work / t_step, "unit": UNIT,
@@ -348,14 +324,11 @@ def run_batched(args, nfields=256):
                                             "rel_rms_median": float(np.median(errs)),
                                             "max_abs_over_std_max": float(np.max(maxabs)),
                                             "fields_over_1e-5": int(np.sum(np.asarray(errs) > 1e-5))},
-            "e2e": {"value": work / t_pipe, "unit": UNIT, "s_per_step": t_pipe, "steps": k_pipe,
-                    "mode": "steady state: each step's sampling overlaps the previous step's launch",
-                    "host_copy_matches_device": pipe_ok,
+            "e2e": {"value": work / t_e2e, "unit": UNIT, "s_per_step": t_e2e, "steps": len(lat),
+                    "host_copy_matches_device": e2e_ok,
+                    "tables_kept_equal": all(len(a) == len(b) for a, b in zip(tabs, tabs2)),
                     "h2d_bytes_per_step": int(h_tabs.numel() * 4),
-                    "d2h_bytes_per_step": int(sum(o.numel() * 4 for o in outs)),
-                    "single_step": {"value": work / t_e2e, "s_per_step": t_e2e,
-                                    "host_copy_matches_device": e2e_ok,
-                                    "tables_kept_equal": all(len(a) == len(b) for a, b in zip(tabs, tabs2))}},
+                    "d2h_bytes_per_step": int(sum(o.numel() * 4 for o in outs))},
             "workload": "256 fields, axes log-uniform 32..256 (x16), VK/Gaussian alternating, cl U[500,5000] m, "
                         "nharm U[2000,20000], ds 50 m, meta-seed 20240"}
 

@@ -234,25 +234,24 @@ __device__ __forceinline__ float map_value(const MapArgs& A, float px, float py,
   return A.delta[(a - 1) + static_cast<long long>(A.n1) * ((b - 1) + static_cast<long long>(A.n2) * (c - 1))];
 }
 
-__global__ void fim_map_kernel(const MapArgs A) {
+// Point sets: one thread per point.
+__global__ void fim_map_points_kernel(const MapArgs A) {
   const long long stride = static_cast<long long>(gridDim.x) * blockDim.x;
-  for (long long p = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x; p < A.n; p += stride) {
-    float px, py, pz;
-    if (A.x) {
-      px = __fsub_rn(A.x[p], A.o1);
-      py = __fsub_rn(A.y[p], A.o2);
-      pz = __fsub_rn(A.z[p], A.o3);
-    } else {
-      const long long plane = static_cast<long long>(A.e1) * A.e2;
-      const int k = static_cast<int>(p / plane);
-      const long long rem = p - k * plane;
-      const int j = static_cast<int>(rem / A.e1);
-      const int i = static_cast<int>(rem - static_cast<long long>(j) * A.e1);
-      px = __fsub_rn(__fmul_rn(static_cast<float>(A.f1 + i), A.ds), A.o1);
-      py = __fsub_rn(__fmul_rn(static_cast<float>(A.f2 + j), A.ds), A.o2);
-      pz = __fsub_rn(__fmul_rn(static_cast<float>(A.f3 + k), A.ds), A.o3);
-    }
-    A.field[p] = map_value(A, px, py, pz);
+  for (long long p = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x; p < A.n; p += stride)
+    A.field[p] = map_value(A, __fsub_rn(A.x[p], A.o1), __fsub_rn(A.y[p], A.o2), __fsub_rn(A.z[p], A.o3));
+}
+
+// Structured grids: blocks along x, rows (j, k) over blockIdx.y; each row's
+// y and z coordinates are computed once, x per thread.
+__global__ void fim_map_grid_kernel(const MapArgs A, int rows) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= A.e1) return;
+  const float px = __fsub_rn(__fmul_rn(static_cast<float>(A.f1 + i), A.ds), A.o1);
+  for (int row = blockIdx.y; row < rows; row += gridDim.y) {
+    const int k = row / A.e2, j = row - k * A.e2;
+    const float py = __fsub_rn(__fmul_rn(static_cast<float>(A.f2 + j), A.ds), A.o2);
+    const float pz = __fsub_rn(__fmul_rn(static_cast<float>(A.f3 + k), A.ds), A.o3);
+    A.field[static_cast<long long>(row) * A.e1 + i] = map_value(A, px, py, pz);
   }
 }
 
@@ -563,8 +562,14 @@ cudaError_t fim_run(const FimInputs& in, const FimGrid& g, void* d_work, float* 
     M.x = in.d_x, M.y = in.d_y, M.z = in.d_z;
     M.n = in.npts;
   }
-  fim_map_kernel<<<blocks_for(M.n, 256), 256, 0, st>>>(M);
-  if ((e = cudaGetLastError()) != cudaSuccess) return failed("fim_map_kernel", e);
+  if (in.structured) {
+    const int rows = M.e2 * (in.fe[2] - in.fs[2] + 1);
+    const dim3 grid((M.e1 + 127) / 128, static_cast<unsigned>(std::min(rows, 65535)));
+    fim_map_grid_kernel<<<grid, 128, 0, st>>>(M, rows);
+  } else {
+    fim_map_points_kernel<<<blocks_for(M.n, 256), 256, 0, st>>>(M);
+  }
+  if ((e = cudaGetLastError()) != cudaSuccess) return failed("fim_map kernels", e);
   cudaEventRecord(ev[4], st);
   if ((e = cudaEventSynchronize(ev[4])) != cudaSuccess) return failed("FIM mapping", e);
   float ms[4] = {0, 0, 0, 0};

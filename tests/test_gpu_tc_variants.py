@@ -190,7 +190,7 @@ def test_harmonic_split_matches_unsplit_and_fp64(variant, split, monkeypatch):
     b = _run(variant, s, case["fs"], case["n"], case["ds"], tab)
     assert np.all(np.isfinite(a))
     assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
-    assert rel_rms(a, base) <= 2e-6
+    assert rel_rms(a, base) <= 1e-5  # two tensor-core sums, each within ~4e-6 of FP64
     ref64 = oracle.sum_structured(oracle.setup(case["op"]), case["fs"], case["n"], case["ds"], tab, f64=True)
     assert rel_rms(a, ref64) <= 1e-5
 
