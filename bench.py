@@ -347,7 +347,7 @@ CONFIG2 = dict(name="plain_unstructured_2e6pts_20x20x10km_gs_cl1500/1500/500_nha
                sigma=0.1, nharm=10000, seed=7)
 CONFIG5 = dict(name="large_structured_2048x2048x512_ds10m_vk_h0.3_cl5000/5000/2000_nharm50000", n=[2048, 2048, 512],
                ds=10.0, acf=0, hurst=0.3, cl=[5000.0, 5000.0, 2000.0], sigma=0.08, nharm=50000, seed=1234)
-DIRECT_WARP_INSTR_PER_PTHARM = 1.19  # ncu: sm__inst_executed per point*harmonic of srm_direct_kernel
+DIRECT_WARP_INSTR_PER_PTHARM = 0.574  # ncu: sm__inst_executed per point*harmonic of srm_direct_kernel (fast sincos)
 FP32_FLOP_PER_PTHARM = 9             # phase 3 mul + 2 add, accumulate 2 mul + 2 add (plus one sincosf)
 
 

@@ -184,23 +184,56 @@ __global__ void fim_clear_imag_kernel(float2* spec, int n1h, long long rows, int
 }
 
 // Scaling of the transform's real output, with one statistics record per
-// block (count, mean, M2 of the scaled values, FP64).
-__global__ void __launch_bounds__(256) fim_scale_kernel(float* f, long long n, float scaling, Moments* rec) {
-  __shared__ Moments s_warp[8];
-  const long long p = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
-  double cnt = 0.0, s1 = 0.0, shift = 0.0;
-  if (p < n) {
-    const float v = __fmul_rn(f[p], scaling);
-    f[p] = v;
-    shift = v;
-    cnt = 1.0;
+// block (count, mean, M2 of the scaled values, FP64). A block covers
+// kScaleThreads * kScaleRun values as kScaleRun / 4 coalesced float4 sweeps;
+// each thread sums its values about its first one before the warp and block
+// merges (a fixed order, so the records are deterministic).
+constexpr int kScaleRun = 16;
+constexpr int kScaleThreads = 256;
+
+__global__ void __launch_bounds__(kScaleThreads) fim_scale_kernel(float* f, long long n, float scaling, Moments* rec) {
+  __shared__ Moments s_warp[kScaleThreads / 32];
+  const long long base = static_cast<long long>(blockIdx.x) * kScaleThreads * kScaleRun;
+  double cnt = 0.0, s1 = 0.0, s2 = 0.0, shift = 0.0;
+  bool have = false;
+  auto take = [&](float v) {
+    if (!have) {
+      shift = v;
+      have = true;
+    }
+    const double d = static_cast<double>(v) - shift;
+    s1 += d;
+    s2 = fma(d, d, s2);
+    cnt += 1.0;
+  };
+#pragma unroll
+  for (int q = 0; q < kScaleRun / 4; ++q) {
+    const long long p = base + (static_cast<long long>(q) * kScaleThreads + threadIdx.x) * 4;
+    if (p + 4 <= n) {
+      float4 v = *reinterpret_cast<const float4*>(f + p);
+      v.x = __fmul_rn(v.x, scaling);
+      v.y = __fmul_rn(v.y, scaling);
+      v.z = __fmul_rn(v.z, scaling);
+      v.w = __fmul_rn(v.w, scaling);
+      *reinterpret_cast<float4*>(f + p) = v;
+      take(v.x);
+      take(v.y);
+      take(v.z);
+      take(v.w);
+    } else {
+      for (long long e = p; e < n && e < p + 4; ++e) {
+        const float v = __fmul_rn(f[e], scaling);
+        f[e] = v;
+        take(v);
+      }
+    }
   }
-  Moments m = warp_moments(moments_from_shifted(cnt, shift, s1, 0.0));
-  if ((threadIdx.x & 31) == 0) s_warp[threadIdx.x >> 5] = m;
+  Moments mo = warp_moments(moments_from_shifted(cnt, shift, s1, s2));
+  if ((threadIdx.x & 31) == 0) s_warp[threadIdx.x >> 5] = mo;
   __syncthreads();
   if (threadIdx.x == 0) {
     Moments b = s_warp[0];
-    for (int w = 1; w < 8; ++w) b = moments_merge(b, s_warp[w]);
+    for (int w = 1; w < kScaleThreads / 32; ++w) b = moments_merge(b, s_warp[w]);
     rec[blockIdx.x] = b;
   }
 }
@@ -386,7 +419,7 @@ FimLayout fim_layout(const FimGrid& g, int npoi) {
   L.n1h = g.npts[0] / 2 + 1;
   L.rows = static_cast<long long>(g.npts[1]) * g.npts[2];
   L.real = static_cast<long long>(g.npts[0]) * L.rows;
-  L.nrec = (L.real + 255) / 256;
+  L.nrec = (L.real + kScaleThreads * kScaleRun - 1) / (kScaleThreads * kScaleRun);
   size_t off = 0;
   L.off_spec = off;
   off = align256(off + sizeof(float2) * static_cast<size_t>(L.n1h * L.rows));
@@ -507,7 +540,7 @@ cudaError_t fim_run(const FimInputs& in, const FimGrid& g, void* d_work, float* 
   const float dhn = in.ndim == 2 ? in.dh * in.dh : (in.dh * in.dh) * in.dh;
   const float scaling = 1.0f / std::sqrt(((static_cast<float>(n1) * static_cast<float>(n2)) * static_cast<float>(n3)) *
                                          dhn);
-  fim_scale_kernel<<<static_cast<unsigned>(L.nrec), 256, 0, st>>>(real, L.real, scaling, rec);
+  fim_scale_kernel<<<static_cast<unsigned>(L.nrec), kScaleThreads, 0, st>>>(real, L.real, scaling, rec);
   if ((e = cudaGetLastError()) != cudaSuccess) return failed("fim_scale_kernel", e);
   if ((e = launch_stats_records(rec, L.nrec, d_out, st)) != cudaSuccess) return failed("statistics", e);
   float mv[2];

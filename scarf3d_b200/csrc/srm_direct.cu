@@ -59,15 +59,23 @@ __device__ __forceinline__ void rotate(const DirectArgs& A, float x, float y, fl
 // phases here (|arg| < 1e4 rad) the reduced argument is within ~2.5e-7 of
 // exact, so each term is within ~6e-7 absolute, and fields agree with the
 // FP32 restatement (glibc sinf/cosf) to ~4e-7 of their standard deviation.
+// (Phases up to 2^22 * 2 pi = 2.6e7 rad; the FP32 phase itself carries an
+// error of several radians long before that.)
 constexpr float kInv2Pi = 0x1.45f306p-3f;
 constexpr float kTwoPi1 = 0x1.921fb6p+2f;
 constexpr float kTwoPi2 = -0x1.777a5cp-23f;
 constexpr float kTwoPi3 = -0x1.ee59dap-48f;
 
+// Nearest integer of t for |t| < 2^22 on the FMA pipe (round to nearest
+// even, as rintf): adding and subtracting 1.5 * 2^23 leaves the integer
+// part. rintf itself would issue on the SFU's pipe, which __sinf and __cosf
+// already saturate here.
+constexpr float kRoundMagic = 0x1.8p23f;
+
 template <bool kFast>
 __device__ __forceinline__ void phase_sincos(float arg, float* sn, float* cs) {
   if constexpr (kFast) {
-    const float j = rintf(__fmul_rn(arg, kInv2Pi));
+    const float j = __fsub_rn(__fadd_rn(__fmul_rn(arg, kInv2Pi), kRoundMagic), kRoundMagic);
     float r = fmaf(-j, kTwoPi1, arg);
     r = fmaf(-j, kTwoPi2, r);
     r = fmaf(-j, kTwoPi3, r);

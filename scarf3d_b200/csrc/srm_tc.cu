@@ -60,8 +60,9 @@ __host__ __device__ constexpr uint32_t swz64(uint32_t row, uint32_t chunk) {
 // Split of two FP32 values into hi and lo 16-bit operands (hi = round(v),
 // lo = round(v - hi)), packed as two 2-byte elements: FP16 (the default) or
 // BF16 (the operand-precision setting; same layouts, same MMA kind).
-__device__ __forceinline__ void split_pair(float a, float b, bool bf16, uint32_t& hi, uint32_t& lo) {
-  if (bf16) {
+template <bool kBf16>
+__device__ __forceinline__ void split_pair(float a, float b, uint32_t& hi, uint32_t& lo) {
+  if constexpr (kBf16) {
     const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
     const float2 f = __bfloat1622float2(h);
     const __nv_bfloat162 l = __floats2bfloat162_rn(a - f.x, b - f.y);
@@ -73,6 +74,23 @@ __device__ __forceinline__ void split_pair(float a, float b, bool bf16, uint32_t
     const __half2 l = __floats2half2_rn(a - f.x, b - f.y);
     hi = *reinterpret_cast<const uint32_t*>(&h);
     lo = *reinterpret_cast<const uint32_t*>(&l);
+  }
+}
+
+// The A operand of kGenHarm harmonics for one row: the complex products
+// R_h(i) S_h(j) (the conjugate's imaginary part, as the MMA sums re cos -
+// im sin), split into hi/lo pairs. rt / stt: this row's R and S entries of
+// the first harmonic, strided by the tiles' widths.
+template <bool kBf16>
+__device__ __forceinline__ void gen_products(const float2* rt, const float2* stt, int ti, int tj, uint32_t* hv,
+                                             uint32_t* lv) {
+#pragma unroll
+  for (int u = 0; u < kGenHarm; ++u) {
+    const float2 x = rt[u * ti];
+    const float2 y = stt[u * tj];
+    const float re = x.x * y.x - x.y * y.y;
+    const float nim = -(x.x * y.y + x.y * y.x);
+    split_pair<kBf16>(re, nim, hv[u], lv[u]);
   }
 }
 
@@ -231,7 +249,7 @@ __global__ void tc_build_c(const TableJob j0, const TableJob* jobs) {
         cs32 = static_cast<float>(cs);
         sn32 = static_cast<float>(sn);
       }
-      split_pair(cs32, sn32, kBf16, hi[u], lo[u]);
+      split_pair<kBf16>(cs32, sn32, hi[u], lo[u]);
     }
     uint8_t* base = T.cimg + ((static_cast<size_t>(nb) * T.stages + k) * T.parts + part) *
                                  (2u * part_rows * kRowBytes);
@@ -359,7 +377,7 @@ __global__ void tc_build_c_factored(const TableJob j0, const TableJob* jobs) {
           cs32 = static_cast<float>(z.x);
           sn32 = static_cast<float>(z.y);
         }
-        split_pair(cs32, sn32, kBf16, hi[u], lo[u]);
+        split_pair<kBf16>(cs32, sn32, hi[u], lo[u]);
       }
       uint8_t* base = T.cimg + ((static_cast<size_t>(nb) * T.stages + k) * T.parts + part) *
                                    (2u * part_rows * kRowBytes);
@@ -474,7 +492,7 @@ __global__ void __launch_bounds__(32 * kBuilderWarps) tc_build_c_warps(const Tab
           cs32 = static_cast<float>(z.x);
           sn32 = static_cast<float>(z.y);
         }
-        split_pair(cs32, sn32, kBf16, hi[u], lo[u]);
+        split_pair<kBf16>(cs32, sn32, hi[u], lo[u]);
       }
       uint8_t* base = T.cimg + ((static_cast<size_t>(nb) * T.stages + k) * T.parts + part) *
                                    (2u * part_rows * kRowBytes);
@@ -709,14 +727,10 @@ __device__ __forceinline__ void generate_a_smem(const TcKernelArgs& A, uint8_t* 
   const float2* rt = reinterpret_cast<const float2*>(rs) + h0 * A.ti + ii;
   const float2* stt = reinterpret_cast<const float2*>(rs) + kStageHarm * A.ti + h0 * A.tj + jj;
   uint32_t hv[kGenHarm], lv[kGenHarm];
-#pragma unroll
-  for (int u = 0; u < kGenHarm; ++u) {
-    const float2 x = rt[u * A.ti];
-    const float2 y = stt[u * A.tj];
-    const float re = x.x * y.x - x.y * y.y;
-    const float nim = -(x.x * y.y + x.y * y.x);
-    split_pair(re, nim, A.bf16 != 0, hv[u], lv[u]);
-  }
+  if (A.bf16)
+    gen_products<true>(rt, stt, A.ti, A.tj, hv, lv);
+  else
+    gen_products<false>(rt, stt, A.ti, A.tj, hv, lv);
   uint8_t* a_hi = st + A.off_a;
   uint8_t* a_lo = a_hi + kATileBytes;
 #pragma unroll
@@ -1021,14 +1035,10 @@ __global__ void __launch_bounds__(kThreads, 1) srm_tc_kernel(const TcKernelArgs 
         const float2* rt = reinterpret_cast<const float2*>(st + A.off_r) + h0 * A.ti + ii;
         const float2* stt = reinterpret_cast<const float2*>(st + A.off_s) + h0 * A.tj + jj;
         uint32_t hv[kGenHarm], lv[kGenHarm];
-#pragma unroll
-        for (int u = 0; u < kGenHarm; ++u) {
-          const float2 x = rt[u * A.ti];
-          const float2 y = stt[u * A.tj];
-          const float re = x.x * y.x - x.y * y.y;
-          const float nim = -(x.x * y.y + x.y * y.x);
-          split_pair(re, nim, A.bf16 != 0, hv[u], lv[u]);
-        }
+        if (A.bf16)
+          gen_products<true>(rt, stt, A.ti, A.tj, hv, lv);
+        else
+          gen_products<false>(rt, stt, A.ti, A.tj, hv, lv);
         if constexpr (kTmemA) {
           // Harmonic h = column h of the stage's hi half (16 + h: lo half).
           // The slot's previous MMAs completed before its bulk copies were
@@ -1807,7 +1817,8 @@ cudaError_t launch_tc_structured(const scarf_srm_setup& s, const int fs[3], cons
   TcKernelArgs A{};
   A.f0 = make_field(s, p, T, d_field);
   A.bf16 = p.bf16;
-  A.f0.band = tc_item_band(p, nsm);
+  // Slab copies need whole column tiles to finish early: natural order then.
+  A.f0.band = (slabs && slabs->nslabs > 0) ? p.bix : tc_item_band(p, nsm);
   const long long npts = static_cast<long long>(n[0]) * n[1] * n[2];
   if (p.split > 1) {
     // Statistics and slab signals need the final values in the kernel.
