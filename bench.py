@@ -884,6 +884,54 @@ def run_b200(args, w):
         dist.destroy_process_group()
 
 
+def run_precision_grid(args, w):
+    """The operand-precision comparison on the grid and harmonic count given
+    (every point against FP64): one line of JSON."""
+    import torch
+
+    import oracle
+    import scarf3d_b200 as sb
+    from oracle import gpu_fp64
+
+    n = [w["nx"], w["ny"], w["nz"]]
+    ds = w["ds"]
+    fs = [1, 1, 1]
+    ds32 = np.float32(ds)
+    nc = [0.0, 0.0, 0.0]
+    fc = [float(np.float32(n[c] - 1) * ds32) for c in range(3)]
+    kw = dict(acf=w["acf"], nharm=w["nharm"], seed=w["seed"], hurst=w["hurst"], sigma=w["sigma"], ds=ds, cl=w["cl"])
+    p = sb.make_params(nc=nc, fc=fc, **kw)
+    s = sb.compute_setup(p)
+    tab, _ = sb.sample(p, s)
+    nh = len(tab)
+    so = oracle.setup(oracle.params(nc=nc, fc=fc, **kw))
+    d_tab = torch.from_numpy(tab.reshape(-1).copy()).cuda()
+    field = torch.empty(int(np.prod(n)), dtype=torch.float32, device="cuda")
+    sptr = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    sb.check(sb.lib.scarf_set_kernel_timing(1))
+    rows = []
+    for otype, terms in ((0, 3), (1, 3), (0, 2)):
+        sb.set_tc_precision(otype, terms)
+        try:
+            wb = sb.tc_workspace_bytes(3, n, nh)
+            work = torch.empty(wb, dtype=torch.uint8, device="cuda")
+
+            def launch():
+                sb.check(sb.lib.scarf_srm_tc_structured(ctypes.byref(s), _i3(fs), _i3(n), ds,
+                                                        ctypes.c_void_p(d_tab.data_ptr()), nh,
+                                                        ctypes.c_void_p(field.data_ptr()),
+                                                        ctypes.c_void_p(work.data_ptr()), wb, sptr))
+            ms = _kernel_times(launch, max(1, args.steps))
+            torch.cuda.synchronize()
+            r = gpu_fp64.compare_structured(field, so, fs, n, ds, tab)
+            rows.append({"operands": ["fp16", "bf16"][otype], "terms": terms, "kernel_ms": float(np.mean(ms)),
+                         "rel_rms_vs_fp64": r["rel_rms"], "max_abs_over_std": r["max_abs"] / r["std_ref"]})
+            del work
+        finally:
+            sb.set_tc_precision(0, 3)
+    return {"grid": n, "nharm": w["nharm"], "harmonics_kept": nh, "precision_plans": rows}
+
+
 def run_profile_leg(args, w):
     """One leg alone, for ncu captures of its kernels (prints no bench line):
     tc = table builders + tensor-core sum (warm-up, then one launch) on the
@@ -899,6 +947,9 @@ def run_profile_leg(args, w):
     torch.cuda.set_device(0)
     if args.profile_leg == "batched":
         run_batched(args)
+        return
+    if args.profile_leg == "precision":
+        print(json.dumps(run_precision_grid(args, w)), flush=True)
         return
     n = [w["nx"], w["ny"], w["nz"]]
     ds = w["ds"]
@@ -947,12 +998,16 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--grid", type=int, nargs=3, default=None, help="override the grid (profiling of small cases)")
+    ap.add_argument("--ds", type=float, default=None)
+    ap.add_argument("--hurst", type=float, default=None)
+    ap.add_argument("--cl", type=float, nargs=3, default=None)
+    ap.add_argument("--sigma", type=float, default=None)
     ap.add_argument("--nharm", type=int, default=None)
     ap.add_argument("--no-batched", action="store_true", help="skip the 256-field batched measurement")
     ap.add_argument("--no-autotune", action="store_true", help="default plans instead of autotuned ones")
     ap.add_argument("--no-precision", action="store_true", help="skip the operand-precision comparison")
     ap.add_argument("--no-fim", action="store_true", help="skip the FIM (method 0) measurement")
-    ap.add_argument("--profile-leg", choices=["tc", "direct", "batched", "fim", "execute"], default=None,
+    ap.add_argument("--profile-leg", choices=["tc", "direct", "batched", "fim", "execute", "precision"], default=None,
                     help="run one leg alone for a profiler capture (no bench line)")
     ap.add_argument("--configs", default="1,2,5",
                     help="other configurations to measure (comma list of 1, 2, 5; empty to skip)")
@@ -962,6 +1017,9 @@ def main():
         w["nx"], w["ny"], w["nz"] = args.grid
     if args.nharm:
         w["nharm"] = args.nharm
+    for key in ("ds", "hurst", "cl", "sigma"):
+        if getattr(args, key) is not None:
+            w[key] = getattr(args, key) if key != "cl" else list(getattr(args, key))
     if args.profile_leg:
         run_profile_leg(args, w)
         return
