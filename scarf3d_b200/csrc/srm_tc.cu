@@ -77,20 +77,39 @@ __device__ __forceinline__ void split_pair(float a, float b, uint32_t& hi, uint3
   }
 }
 
+// Operand pair type of the A image: FP16 or BF16 hi/lo halves.
+template <bool kBf16>
+struct OperandPair {
+  using T2 = __half2;
+  static __device__ __forceinline__ T2 pack(float a, float b) { return __floats2half2_rn(a, b); }
+  static __device__ __forceinline__ float2 unpack(T2 v) { return __half22float2(v); }
+};
+template <>
+struct OperandPair<true> {
+  using T2 = __nv_bfloat162;
+  static __device__ __forceinline__ T2 pack(float a, float b) { return __floats2bfloat162_rn(a, b); }
+  static __device__ __forceinline__ float2 unpack(T2 v) { return __bfloat1622float2(v); }
+};
+
 // The A operand of kGenHarm harmonics for one row: the complex products
 // R_h(i) S_h(j) (the conjugate's imaginary part, as the MMA sums re cos -
 // im sin), split into hi/lo pairs. rt / stt: this row's R and S entries of
-// the first harmonic, strided by the tiles' widths.
+// the first harmonic, strided by the tiles' widths. The operand type is a
+// compile-time choice: a run-time branch here costs the FP16 kernel ~4 %.
 template <bool kBf16>
-__device__ __forceinline__ void gen_products(const float2* rt, const float2* stt, int ti, int tj, uint32_t* hv,
-                                             uint32_t* lv) {
+__device__ __forceinline__ void gen_products(const float2* rt, const float2* stt, int ti, int tj,
+                                             typename OperandPair<kBf16>::T2* hv,
+                                             typename OperandPair<kBf16>::T2* lv) {
+  using Op = OperandPair<kBf16>;
 #pragma unroll
   for (int u = 0; u < kGenHarm; ++u) {
     const float2 x = rt[u * ti];
     const float2 y = stt[u * tj];
     const float re = x.x * y.x - x.y * y.y;
     const float nim = -(x.x * y.y + x.y * y.x);
-    split_pair<kBf16>(re, nim, hv[u], lv[u]);
+    hv[u] = Op::pack(re, nim);
+    const float2 hf = Op::unpack(hv[u]);
+    lv[u] = Op::pack(re - hf.x, nim - hf.y);
   }
 }
 
@@ -721,16 +740,14 @@ __device__ __forceinline__ void signal_field(const TcField& f, int lane) {
 // A operand of one stage into shared memory: row r of the tile (the
 // (ii, jj) point of the row block), kGenHarm harmonics from h0, FP16 hi and lo
 // images in the 64-B-swizzled K-major layout.
+template <bool kBf16>
 __device__ __forceinline__ void generate_a_smem(const TcKernelArgs& A, uint8_t* st, const uint8_t* rs, int r, int ii,
                                                 int jj, int h0) {
   // rs: the stage's R tile [16][ti] followed by its S tile [16][tj] (float2)
   const float2* rt = reinterpret_cast<const float2*>(rs) + h0 * A.ti + ii;
   const float2* stt = reinterpret_cast<const float2*>(rs) + kStageHarm * A.ti + h0 * A.tj + jj;
-  uint32_t hv[kGenHarm], lv[kGenHarm];
-  if (A.bf16)
-    gen_products<true>(rt, stt, A.ti, A.tj, hv, lv);
-  else
-    gen_products<false>(rt, stt, A.ti, A.tj, hv, lv);
+  typename OperandPair<kBf16>::T2 hv[kGenHarm], lv[kGenHarm];
+  gen_products<kBf16>(rt, stt, A.ti, A.tj, hv, lv);
   uint8_t* a_hi = st + A.off_a;
   uint8_t* a_lo = a_hi + kATileBytes;
 #pragma unroll
@@ -758,7 +775,7 @@ constexpr uint32_t kTmemAStageCols = 32;
 // (tcgen05.st from the generator registers, MMA in its TMEM-A form). The
 // TMEM-A form takes the A tile's writes and its three operand reads per
 // stage off the shared-memory port, which is the pipeline's bottleneck.
-template <bool kTmemA>
+template <bool kTmemA, bool kBf16>
 __global__ void __launch_bounds__(kThreads, 1) srm_tc_kernel(const TcKernelArgs A) {
   constexpr uint32_t kMasterCol = kTmemA ? kMaxNTmemA : kMaxNSmemA;
   extern __shared__ uint8_t smem_raw[];
@@ -1034,11 +1051,8 @@ __global__ void __launch_bounds__(kThreads, 1) srm_tc_kernel(const TcKernelArgs 
         uint8_t* st = smem + s * A.stage_bytes;
         const float2* rt = reinterpret_cast<const float2*>(st + A.off_r) + h0 * A.ti + ii;
         const float2* stt = reinterpret_cast<const float2*>(st + A.off_s) + h0 * A.tj + jj;
-        uint32_t hv[kGenHarm], lv[kGenHarm];
-        if (A.bf16)
-          gen_products<true>(rt, stt, A.ti, A.tj, hv, lv);
-        else
-          gen_products<false>(rt, stt, A.ti, A.tj, hv, lv);
+        typename OperandPair<kBf16>::T2 hv[kGenHarm], lv[kGenHarm];
+        gen_products<kBf16>(rt, stt, A.ti, A.tj, hv, lv);
         if constexpr (kTmemA) {
           // Harmonic h = column h of the stage's hi half (16 + h: lo half).
           // The slot's previous MMAs completed before its bulk copies were
@@ -1100,6 +1114,7 @@ __global__ void __launch_bounds__(kThreads, 1) srm_tc_kernel(const TcKernelArgs 
 //   empty[s]     both: the pair MMAs of stage s completed (multicast commit).
 //   accf         both: a chunk is accumulated (multicast commit).
 //   acce         even CTA: the epilogues of both CTAs drained the chunk.
+template <bool kBf16>
 __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1) srm_tc_pair_kernel(const TcKernelArgs A) {
   constexpr uint32_t kMasterCol = kMaxNSmemA;
   extern __shared__ uint8_t smem_raw[];
@@ -1461,7 +1476,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1) srm_tc_
           ok = false;
           break;
         }
-        generate_a_smem(A, smem + s * A.stage_bytes, smem + A.rs_base + rr * A.rs_bytes, r, ii, jj, h0);
+        generate_a_smem<kBf16>(A, smem + s * A.stage_bytes, smem + A.rs_base + rr * A.rs_bytes, r, ii, jj, h0);
         __syncwarp();
         if (lane == 0) {
           mbar_arrive(&agen[s]);
@@ -1621,17 +1636,25 @@ size_t compute_layout(TcKernelArgs& A, int ti, int tj, int ntile_max, bool tmem_
 
 // The kernel's dynamic shared-memory limit, raised once per device so that
 // launches themselves make no attribute calls.
+template <bool kBf16>
+cudaError_t set_smem_attributes() {
+  cudaError_t e = cudaFuncSetAttribute(srm_tc_kernel<false, kBf16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       kMaxDynSmem);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(srm_tc_kernel<true, kBf16>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(srm_tc_pair_kernel<kBf16>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
+  return e;
+}
+
 cudaError_t ensure_smem_attribute() {
   static bool done[64] = {};
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
   if (dev >= 0 && dev < 64 && done[dev]) return cudaSuccess;
-  e = cudaFuncSetAttribute(srm_tc_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
-  if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(srm_tc_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
-  if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(srm_tc_pair_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
+  e = set_smem_attributes<false>();
+  if (e == cudaSuccess) e = set_smem_attributes<true>();
   if (e == cudaSuccess && dev >= 0 && dev < 64) done[dev] = true;
   return e;
 }
@@ -1644,15 +1667,23 @@ int device_sms() {
 }
 
 // Persistent launch: one CTA (or CTA pair) per SM (pair), at most one per item.
-void launch_tc_kernel(const TcKernelArgs& A, bool tmem_a, bool pair, int nsm, size_t smem, cudaStream_t stream) {
+template <bool kBf16>
+void launch_tc_kernel_typed(const TcKernelArgs& A, bool tmem_a, bool pair, int nsm, size_t smem, cudaStream_t stream) {
   if (pair) {
     const int pairs = std::max(1, std::min(A.num_items, nsm / 2));
-    srm_tc_pair_kernel<<<2 * pairs, kThreads, smem, stream>>>(A);
+    srm_tc_pair_kernel<kBf16><<<2 * pairs, kThreads, smem, stream>>>(A);
   } else if (tmem_a) {
-    srm_tc_kernel<true><<<std::min(A.num_items, nsm), kThreads, smem, stream>>>(A);
+    srm_tc_kernel<true, kBf16><<<std::min(A.num_items, nsm), kThreads, smem, stream>>>(A);
   } else {
-    srm_tc_kernel<false><<<std::min(A.num_items, nsm), kThreads, smem, stream>>>(A);
+    srm_tc_kernel<false, kBf16><<<std::min(A.num_items, nsm), kThreads, smem, stream>>>(A);
   }
+}
+
+void launch_tc_kernel(const TcKernelArgs& A, bool tmem_a, bool pair, int nsm, size_t smem, cudaStream_t stream) {
+  if (A.bf16)
+    launch_tc_kernel_typed<true>(A, tmem_a, pair, nsm, smem, stream);
+  else
+    launch_tc_kernel_typed<false>(A, tmem_a, pair, nsm, smem, stream);
 }
 
 }  // namespace
