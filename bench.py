@@ -946,7 +946,7 @@ def run_profile_leg(args, w):
 
     torch.cuda.set_device(0)
     if args.profile_leg == "batched":
-        run_batched(args)
+        print(json.dumps(run_batched(args)), flush=True)
         return
     if args.profile_leg == "precision":
         print(json.dumps(run_precision_grid(args, w)), flush=True)

@@ -213,6 +213,13 @@ int scarf_srm_sample_device_batch(int nfields, const scarf_srm_params *p, const 
                                   float *const *tables, int *n_kept, long long *pairs_used, long long *host_decided,
                                   void *stream);
 
+/* The device scan's certain-reject table of one field (256 entries): a pair
+ * whose second raw draw y2 is >= thr[y1 >> 23] (y1 the first raw draw) fails
+ * the rejection test r2 < d(u) whatever the spectrum's FP32 rounding, and is
+ * dropped before the spectrum is evaluated. 0xFFFFFFFF: never dropped early.
+ * Exposed so that the bound can be checked on the host. */
+int scarf_srm_sampler_reject_table(const scarf_srm_params *p, const scarf_srm_setup *s, unsigned int thr[256]);
+
 /* Where scarf_execute draws its harmonics: SCARF_SAMPLER_AUTO (device,
  * unless a uniform source was installed), _HOST or _DEVICE. */
 #define SCARF_SAMPLER_AUTO 0

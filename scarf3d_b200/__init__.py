@@ -41,7 +41,7 @@ EXPORTED_SYMBOLS = (
     "scarf_set_output_overlap",
     "scarf_execute_ex",
     "scarf_srm_compute_setup", "scarf_srm_sample", "scarf_srm_sample_device", "scarf_srm_sample_device_batch",
-    "scarf_set_sampler",
+    "scarf_srm_sampler_reject_table", "scarf_set_sampler",
     "scarf_set_sampler_pass_pairs",
     "scarf_srm_direct_structured",
     "scarf_srm_direct_points", "scarf_srm_tc_workspace_bytes", "scarf_srm_tc_structured",
@@ -147,6 +147,7 @@ def _load() -> ctypes.CDLL:
                                             ctypes.POINTER(c_ll), ctypes.POINTER(c_ll), c_void_p]),
         "scarf_srm_sample_device_batch": (c_int, [c_int, c_void_p, c_void_p, c_void_p, ip, c_void_p,
                                                   ctypes.POINTER(c_ll), c_void_p]),
+        "scarf_srm_sampler_reject_table": (c_int, [ctypes.POINTER(SrmParams), ctypes.POINTER(SrmSetup), c_void_p]),
         "scarf_set_sampler": (c_int, [c_int]),
         "scarf_set_sampler_pass_pairs": (c_int, [c_ll]),
         "scarf_srm_direct_structured": (c_int, [ctypes.POINTER(SrmSetup), ip, ip, c_float, c_void_p, c_int,
@@ -361,6 +362,14 @@ def sample_device(p: SrmParams, s: SrmSetup, stream_handle: int | None = None):
                                       ctypes.byref(kept), ctypes.byref(used), ctypes.byref(open_),
                                       ctypes.c_void_p(stream_handle or 0)))
     return tab[: kept.value].copy(), used.value, open_.value
+
+
+def sampler_reject_table(p: SrmParams, s: SrmSetup):
+    """The device scan's certain-reject thresholds on the second raw draw,
+    one per bin y1 >> 23 of the first (256 uint32; 0xFFFFFFFF = never)."""
+    thr = np.zeros(256, np.uint32)
+    check(lib.scarf_srm_sampler_reject_table(ctypes.byref(p), ctypes.byref(s), thr.ctypes.data_as(ctypes.c_void_p)))
+    return thr
 
 
 def sample_device_batch(params, setups, stream_handle: int | None = None, out=None):

@@ -111,8 +111,7 @@ __global__ void __launch_bounds__(256) fim_spectrum_kernel(const SpecArgs A) {
     for (int i = lane; i < A.n1h; i += 32) {
       const uint32_t x = static_cast<uint32_t>(s.r0);
       const uint32_t y = x == 0 ? 0u
-                                : mulmod32(mulmod32(sp[x & 2047u], sp[kPow0 + ((x >> 11) & 2047u)]),
-                                           sp[kPow0 + kPow1 + (x >> 22)]);
+                                : mulmod3(sp[x & 2047u], sp[kPow0 + ((x >> 11) & 2047u)], sp[kPow0 + kPow1 + (x >> 22)]);
       const float u = to_u01(y);
       const float kx = __fmul_rn(static_cast<float>(i), A.dk1);  // i <= n1/2 on the half grid
       const float kr = __fsqrt_rn(__fadd_rn(__fadd_rn(__fmul_rn(kx, kx), kyy), kzz));

@@ -1059,6 +1059,13 @@ int scarf_srm_sample_device_batch(int nfields, const scarf_srm_params* p, const 
   return SCARF_OK;
 }
 
+int scarf_srm_sampler_reject_table(const scarf_srm_params* p, const scarf_srm_setup* s, unsigned int thr[256]) {
+  static_assert(kRejectBins == 256, "the header declares 256 bins");
+  if (!p || !s || !thr) return fail(SCARF_ERR_ARG, "NULL argument");
+  sampler_reject_thresholds(*s, p->acf, kSamplerMargin, thr);
+  return SCARF_OK;
+}
+
 int scarf_srm_sample(const scarf_srm_params* p, const scarf_srm_setup* s, float* table, int* n_kept,
                      long long* pairs_used) {
   if (!p || !s || !table) return fail(SCARF_ERR_ARG, "NULL argument");

@@ -570,7 +570,7 @@ struct DevBuf {
 struct DeviceSamplerState {
   int device = -1;
   bool tables = false;
-  DevBuf counts, offsets, entries, slots, batch_args, batch_tbeg;
+  DevBuf counts, offsets, entries, slots, batch_args, batch_tbeg, reject;
   SampleEntry* host_entries = nullptr;  // page-locked staging of candidate entries
   long long host_entries_cap = 0;
   cudaStream_t side = nullptr;        // gathers and copies beside the scans
@@ -591,6 +591,47 @@ bool host_accept(const scarf_srm_setup& s, int acf, float r1, float r2) {
 
 }  // namespace
 
+void sampler_reject_thresholds(const scarf_srm_setup& s, int acf, float margin, uint32_t* thr) {
+  const int pw = s.ndim - 1;
+  const double nu = s.nu;
+  auto F = [&](double x) {
+    const double psd = acf == 0 ? std::pow(1.0 + x * x, -nu) : std::exp(-0.25 * x * x);
+    return (pw == 2 ? x * x : x) * psd * static_cast<double>(s.cnst);
+  };
+  double peak = 0.0;
+  if (acf == 0) {
+    const double den = 2.0 * nu - pw;
+    peak = den > 0.0 ? std::sqrt(pw / den) : HUGE_VAL;  // (den <= 0: increasing)
+  } else {
+    peak = std::sqrt(2.0 * pw);
+  }
+  // u as the scan computes it from r1, in FP32 without contraction.
+  const float w = s.kmax - s.kmin;
+  auto u_of = [&](uint32_t y) { return Yarn2::to_u01(y) * w + s.kmin; };
+  for (int b = 0; b < kRejectBins; ++b) {
+    const uint32_t y0 = static_cast<uint32_t>(b) << kRejectShift;
+    const uint32_t y1 = static_cast<uint32_t>(std::min<uint64_t>((static_cast<uint64_t>(b) + 1) << kRejectShift,
+                                                                 Yarn2::kMod) - 1);
+    const double a = u_of(y0), c = u_of(y1);
+    const double x = std::min(std::max(peak, a), c);
+    // relative room for the FP32 spectrum (expf's argument error grows with
+    // |arg| to ~1e-5 before it underflows), absolute room for its subnormals
+    const double bound = F(x) * (1.0 + static_cast<double>(margin)) * (1.0 + 1e-4) + 1e-30;
+    // smallest raw y with to_u01(y) >= bound (to_u01 is non-decreasing)
+    uint32_t t = 0xFFFFFFFFu;
+    if (!(bound > 1.0) && std::isfinite(bound)) {
+      uint32_t lo = 0, hi = static_cast<uint32_t>(Yarn2::kMod);  // to_u01(m) = 1 >= bound
+      while (lo < hi) {
+        const uint32_t mid = lo + (hi - lo) / 2;
+        if (static_cast<double>(Yarn2::to_u01(mid)) >= bound) hi = mid;
+        else lo = mid + 1;
+      }
+      t = lo;
+    }
+    thr[b] = t;
+  }
+}
+
 void set_device_sampler_pass_cap(long long pairs) {
   std::lock_guard<std::mutex> lk(g_dev_sampler_mu);
   g_pass_pairs_cap = pairs > 0 ? pairs : 0;
@@ -610,9 +651,7 @@ SamplerArgs make_sampler_args(const scarf_srm_params& p, const scarf_srm_setup& 
   A.nu = s.nu;
   A.ndim = s.ndim;
   A.acf = p.acf;
-  // Device and host spectra differ by a few ulps at most; 2e-5 relative is a
-  // wide bound around the decision r2 < d.
-  A.margin = 2e-5f;
+  A.margin = kSamplerMargin;
   return A;
 }
 
@@ -629,7 +668,7 @@ long long first_pass_pairs(const scarf_srm_params& p, double acc) {
 void release_sampler_device_memory() {
   std::lock_guard<std::mutex> lk(g_dev_sampler_mu);
   DeviceSamplerState& D = g_dev_sampler;
-  for (DevBuf* b : {&D.counts, &D.offsets, &D.entries, &D.slots, &D.batch_args, &D.batch_tbeg}) b->release();
+  for (DevBuf* b : {&D.counts, &D.offsets, &D.entries, &D.slots, &D.batch_args, &D.batch_tbeg, &D.reject}) b->release();
 }
 
 namespace {
@@ -640,7 +679,7 @@ bool ensure_sampler_device(DeviceSamplerState& D) {
   if (cudaGetDevice(&dev) != cudaSuccess) return false;
   if (D.device != dev) {
     // the previous device's buffers (freed through unified addressing)
-    for (DevBuf* b : {&D.counts, &D.offsets, &D.entries, &D.slots, &D.batch_args, &D.batch_tbeg}) b->release();
+    for (DevBuf* b : {&D.counts, &D.offsets, &D.entries, &D.slots, &D.batch_args, &D.batch_tbeg, &D.reject}) b->release();
     if (D.host_entries) cudaFreeHost(D.host_entries);
     D = DeviceSamplerState();
     D.device = dev;
@@ -823,7 +862,16 @@ int srm_sample_device_batch(int nfields, const scarf_srm_params* p, const scarf_
   if (D.counts.ensure(sizeof(int) * T) != cudaSuccess || D.offsets.ensure(sizeof(long long) * T) != cudaSuccess ||
       D.slots.ensure(sizeof(unsigned long long) * sbeg[nfields]) != cudaSuccess ||
       D.batch_args.ensure(sizeof(SamplerArgs) * nfields) != cudaSuccess ||
-      D.batch_tbeg.ensure(sizeof(long long) * (nfields + 1)) != cudaSuccess)
+      D.batch_tbeg.ensure(sizeof(long long) * (nfields + 1)) != cudaSuccess ||
+      D.reject.ensure(sizeof(uint32_t) * kRejectBins * nfields) != cudaSuccess)
+    return err;
+  // Certain-reject thresholds of every field, uploaded before the scans.
+  std::vector<uint32_t> reject(static_cast<size_t>(kRejectBins) * nfields);
+  parallel_tasks(nfields, host_threads(), [&](int f) {
+    sampler_reject_thresholds(s[f], p[f].acf, args[f].margin, reject.data() + static_cast<size_t>(f) * kRejectBins);
+  });
+  if (cudaMemcpyAsync(D.reject.p, reject.data(), sizeof(uint32_t) * reject.size(), cudaMemcpyHostToDevice, stream) !=
+      cudaSuccess)
     return err;
   int* d_counts = static_cast<int*>(D.counts.p);
   long long* d_offsets = static_cast<long long*>(D.offsets.p);
@@ -833,6 +881,7 @@ int srm_sample_device_batch(int nfields, const scarf_srm_params* p, const scarf_
     args[f].offsets = nullptr;
     args[f].out = nullptr;
     args[f].keys = d_slots + sbeg[f];
+    args[f].reject = static_cast<const unsigned int*>(D.reject.p) + static_cast<size_t>(f) * kRejectBins;
   }
   // Groups of consecutive fields, balanced by their first-pass pairs. Each
   // group's scan is its own launch on `stream`; while later groups scan, the
@@ -861,6 +910,7 @@ int srm_sample_device_batch(int nfields, const scarf_srm_params* p, const scarf_
     D.side = nullptr;
     return err;
   }
+
   while (static_cast<int>(D.events.size()) < G) {
     cudaEvent_t e = nullptr;
     if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) return err;
@@ -873,6 +923,9 @@ int srm_sample_device_batch(int nfields, const scarf_srm_params* p, const scarf_
     return err;
   const SamplerArgs* d_args = static_cast<const SamplerArgs*>(D.batch_args.p);
   const long long* d_tbeg = static_cast<const long long*>(D.batch_tbeg.p);
+  // One launch per group on the caller's stream (scans of consecutive groups
+  // run on two streams measured slower: the groups then finish later and
+  // the host stages behind them start later).
   for (int g = 0; g < G; ++g) {
     const int f0 = gbeg[g], f1 = gbeg[g + 1];
     if (f1 > f0 &&

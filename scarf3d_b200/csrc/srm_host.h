@@ -93,6 +93,21 @@ int srm_sample_device(const scarf_srm_params& p, const scarf_srm_setup& s, float
 // infeasible; -2 - nfields on a CUDA error.
 int srm_sample_device_batch(int nfields, const scarf_srm_params* p, const scarf_srm_setup* s, float* const* tables,
                             int* kept, long long* pairs_used, void* stream, long long* uncertain);
+// Certain-reject thresholds of the device scan, one per bin of the first
+// draw's raw output (bin = y1 >> kRejectShift, kRejectBins entries; both
+// constants in srm_kernels.h beside SamplerArgs): a pair whose second raw draw
+// y2 is at least thr[bin] fails the decision r2 < d(u) (1 + margin) for every
+// u that the bin's r1 values give, so the scan drops it without evaluating
+// the spectrum. thr[bin] bounds the spectrum's exact maximum over the bin's u
+// interval (it is unimodal: x^(ndim-1) psd(x) peaks at x^2 = (ndim-1) /
+// (2 nu - ndim + 1) for von Karman, 2 (ndim-1) for Gaussian) with 1e-4
+// relative and 1e-30 absolute room for the device's FP32 evaluation;
+// 0xFFFFFFFF = never.
+void sampler_reject_thresholds(const scarf_srm_setup& s, int acf, float margin, uint32_t* thr);
+// Relative band around the decision r2 < d in which the device leaves a pair
+// to the host: device and host spectra differ by a few ulps at most.
+constexpr float kSamplerMargin = 2e-5f;
+
 // Upper bound on the pairs tested per device pass (0 = sized from the
 // acceptance rate); smaller passes are chained until every harmonic is drawn.
 void set_device_sampler_pass_cap(long long pairs);

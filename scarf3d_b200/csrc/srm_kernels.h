@@ -167,8 +167,13 @@ struct SampleEntry {
   int pad;
   float r[8];   // pairs q, q+1, q+2, q+3
 };
+// Bins of the scan's certain-reject test: the first draw's raw output
+// y1 < 2^31 falls in bin y1 >> kRejectShift.
+constexpr int kRejectShift = 23;
+constexpr int kRejectBins = 1 << (31 - kRejectShift);
 struct SamplerArgs {
   unsigned long long r0, r1;  // generator state after seeding (pair 0 next)
+  const unsigned int* reject; // [kRejectBins] certain-reject thresholds on y2 (NULL: none)
   long long q_begin, q_count;
   int pairs_per_thread;
   long long nthreads;

@@ -13,6 +13,13 @@
 // the pair and of the three pairs that follow it (angles, a, b), which is
 // everything the host walk needs.
 //
+// Most pairs are certain rejections that the raw draws already show: the
+// host gives each field a table of thresholds on y2 per bin of y1 (an upper
+// bound of the spectrum over the bin's u interval, with room for the FP32
+// evaluation), and a pair with y2 at or above its bin's threshold is dropped
+// before any floating-point work. Every other pair takes the full test, so
+// the decisions are those of the full test for every pair.
+//
 // Two passes over the same range: the first counts candidates per thread,
 // the host turns the counts into offsets, the second writes them.
 //
@@ -63,7 +70,8 @@ __device__ __forceinline__ int classify(const SamplerArgs& A, float r1, float r2
 // thread's own slot keys + t * cap while counting them all (write = 2: one
 // scan instead of two; a count above cap tells the host to redo that field;
 // the gather launch rebuilds full entries from the keys).
-__device__ __forceinline__ void sample_range(const SamplerArgs& A, long long t, int write, const uint32_t* sp) {
+__device__ __forceinline__ void sample_range(const SamplerArgs& A, long long t, int write, const uint32_t* sp,
+                                             const uint32_t* thr) {
   const long long q0 = A.q_begin + t * A.pairs_per_thread;
   long long q1 = q0 + A.pairs_per_thread;
   if (q1 > A.q_begin + A.q_count) q1 = A.q_begin + A.q_count;
@@ -73,8 +81,11 @@ __device__ __forceinline__ void sample_range(const SamplerArgs& A, long long t, 
   long long slot = write == 1 ? A.offsets[t] : (write == 2 ? t * A.cap : 0);
   const long long slot_end = write == 2 ? slot + A.cap : (1ll << 62);
   for (long long q = q0; q < q1; ++q) {
-    const float r1 = to_u01(g.next());
-    const float r2 = to_u01(g.next());
+    const uint32_t y1 = g.next();
+    const uint32_t y2 = g.next();
+    if (thr && y2 >= thr[y1 >> kRejectShift]) continue;
+    const float r1 = to_u01(y1);
+    const float r2 = to_u01(y2);
     const int c = classify(A, r1, r2);
     if (c == 0) continue;
     ++count;
@@ -96,28 +107,49 @@ __device__ __forceinline__ void sample_range(const SamplerArgs& A, long long t, 
 
 __global__ void sampler_kernel(const SamplerArgs A) {
   __shared__ uint32_t sp[kPowWords];
+  __shared__ uint32_t sthr[kRejectBins];
+  if (A.reject)
+    for (int i = threadIdx.x; i < kRejectBins; i += blockDim.x) sthr[i] = A.reject[i];
   load_pow(sp);
   const long long t = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (t >= A.nthreads) return;
-  sample_range(A, t, A.write, sp);
+  sample_range(A, t, A.write, sp, A.reject ? sthr : nullptr);
 }
 
-// Passes of many fields in one launch: global thread t belongs to the field
-// f with tbeg[f] <= t < tbeg[f + 1] (binary search over the prefix).
-__global__ void sampler_batch_kernel(const SamplerArgs* fields, const long long* tbeg, int nfields,
-                                     long long total, int write) {
-  __shared__ uint32_t sp[kPowWords];
-  load_pow(sp);
-  const long long t = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (t >= total) return;
+// The field f with tbeg[f] <= t < tbeg[f + 1] (binary search over the prefix).
+__device__ __forceinline__ int field_of(const long long* tbeg, int nfields, long long t) {
   int lo = 0, hi = nfields - 1;
   while (lo < hi) {
     const int mid = (lo + hi + 1) >> 1;
     if (tbeg[mid] <= t) lo = mid;
     else hi = mid - 1;
   }
-  const SamplerArgs A = fields[lo];
-  sample_range(A, t - tbeg[lo], write, sp);
+  return lo;
+}
+
+// Passes of many fields in one launch: global thread t belongs to field
+// field_of(t). The block keeps the reject thresholds of its first thread's
+// field and of the next field in shared memory (a block spans at most those
+// two unless fields have fewer threads than a block; threads of any further
+// field read their field's table from global memory).
+__global__ void sampler_batch_kernel(const SamplerArgs* fields, const long long* tbeg, int nfields,
+                                     long long total, int write) {
+  __shared__ uint32_t sp[kPowWords];
+  __shared__ uint32_t sthr[2][kRejectBins];
+  const long long tb = static_cast<long long>(blockIdx.x) * blockDim.x;
+  const int f0 = field_of(tbeg, nfields, tb);
+  for (int i = threadIdx.x; i < 2 * kRejectBins; i += blockDim.x) {
+    const int f = f0 + i / kRejectBins;
+    const uint32_t* src = f < nfields ? fields[f].reject : nullptr;
+    sthr[i / kRejectBins][i % kRejectBins] = src ? src[i % kRejectBins] : 0xFFFFFFFFu;
+  }
+  load_pow(sp);
+  const long long t = tb + threadIdx.x;
+  if (t >= total) return;
+  const int f = field_of(tbeg, nfields, t);
+  const SamplerArgs A = fields[f];
+  const uint32_t* thr = f - f0 < 2 ? sthr[f - f0] : A.reject;
+  sample_range(A, t - tbeg[f], write, sp, thr);
 }
 
 // Compacts the per-thread slots of a write = 2 pass: thread t's min(count,
@@ -130,12 +162,7 @@ __global__ void sampler_gather_kernel(const SamplerArgs* fields, const long long
   load_pow(sp);
   const long long t = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (t >= total) return;
-  int lo = 0, hi = nfields - 1;
-  while (lo < hi) {
-    const int mid = (lo + hi + 1) >> 1;
-    if (tbeg[mid] <= t) lo = mid;
-    else hi = mid - 1;
-  }
+  const int lo = field_of(tbeg, nfields, t);
   const SamplerArgs& A = fields[lo];
   const long long tl = t - tbeg[lo];
   const int n = min(A.counts[tl], A.cap);
