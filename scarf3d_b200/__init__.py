@@ -438,9 +438,9 @@ def set_direct_sincos(mode: int):
     check(lib.scarf_set_direct_sincos(int(mode)))
 
 
-def set_tc_precision(operand_type: int = 0, terms: int = 3):
+def set_tc_precision(operand_type: int = 1, terms: int = 3):
     """Operand split of the tensor-core form for plans made afterwards:
-    TC_FP16 (default) or TC_BF16 hi/lo parts, 3 (default) or 2 products."""
+    TC_BF16 (default) or TC_FP16 hi/lo parts, 3 (default) or 2 products."""
     check(lib.scarf_set_tc_precision(int(operand_type), int(terms)))
 
 

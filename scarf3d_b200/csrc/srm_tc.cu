@@ -10,10 +10,11 @@
 //   P_h(i,j) = R_h(i) S_h(j),  R_h(i) = (b - i a) e^{i (kx x_i + c)},  S_h(j) = e^{i ky y_j}.
 // Per-axis factors are computed in FP64 (phases reach ~1e4 rad) and rounded to
 // FP32. The A operand [128 rows x 2 nh] is generated in shared memory from the
-// R and S factor tiles (complex multiply, FP16 hi/lo split); the B operand
-// [cos; sin](kz z) is pre-split into FP16 hi/lo images in global memory and
-// staged by 1-D bulk copies. Three tcgen05 kind::f16 products (hi*hi, hi*lo,
-// lo*hi) accumulate in FP32 in tensor memory.
+// R and S factor tiles (complex multiply, 16-bit hi/lo split: BF16 by
+// default, FP16 on request); the B operand [cos; sin](kz z) is pre-split into
+// hi/lo images of the same type in global memory and staged by 1-D bulk
+// copies. Three tcgen05 kind::f16 products (hi*hi, hi*lo, lo*hi) accumulate
+// in FP32 in tensor memory.
 //
 // Work distribution: one persistent CTA per SM pulls work items (one 128-row
 // x <=256-column output tile of one field) from a device work queue (an
@@ -738,7 +739,7 @@ __device__ __forceinline__ void signal_field(const TcField& f, int lane) {
 }
 
 // A operand of one stage into shared memory: row r of the tile (the
-// (ii, jj) point of the row block), kGenHarm harmonics from h0, FP16 hi and lo
+// (ii, jj) point of the row block), kGenHarm harmonics from h0, 16-bit hi and lo
 // images in the 64-B-swizzled K-major layout.
 template <bool kBf16>
 __device__ __forceinline__ void generate_a_smem(const TcKernelArgs& A, uint8_t* st, const uint8_t* rs, int r, int ii,
@@ -1528,7 +1529,7 @@ int ilog2(int v) {
 constexpr int kDefaultChunkStages = 32;
 int g_chunk_stages = kDefaultChunkStages;
 int g_variant = kTcVariantSingle;
-int g_prec_bf16 = 0, g_prec_terms = 3;  // operand precision of plans made from now on
+int g_prec_bf16 = 1, g_prec_terms = 3;  // operand precision of plans made from now on (BF16 x 3 by default)
 
 TableJob make_job(const scarf_srm_setup& s, const int fs[3], float ds, const float* d_table, int nh,
                   const TcPlan& p, void* d_work) {
