@@ -1198,9 +1198,13 @@ struct scarf_tc_batch {
   int* flags = nullptr;      // host-mapped, one per field
   int* flags_dev = nullptr;  // their device address
   cudaStream_t copy_stream = nullptr;
+  scarf::BuilderFork fork;   // the C-image builder's stream beside the R/S builder
   ~scarf_tc_batch() {
     if (flags) cudaFreeHost(flags);
     if (copy_stream) cudaStreamDestroy(copy_stream);
+    if (fork.side) cudaStreamDestroy(fork.side);
+    if (fork.fork) cudaEventDestroy(fork.fork);
+    if (fork.join) cudaEventDestroy(fork.join);
   }
 };
 
@@ -1261,10 +1265,14 @@ int scarf_srm_tc_batch_create(const scarf_tc_field* fields, int nfields, void* d
     b->setups[f] = *fields[f].setup;
     b->in[f].s = &b->setups[f];
   }
-  const cudaError_t e = tc_batch_upload(b->in.data(), b->plan, d_work);
+  cudaError_t e = tc_batch_upload(b->in.data(), b->plan, d_work);
+  // Created here, outside any stream capture, for every later launch.
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->fork.side, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->fork.fork, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->fork.join, cudaEventDisableTiming);
   if (e != cudaSuccess) {
     delete b;
-    return cuda_fail(e, "tc_batch_upload");
+    return cuda_fail(e, "scarf_srm_tc_batch_create");
   }
   *batch = b;
   return SCARF_OK;
@@ -1301,7 +1309,7 @@ int scarf_srm_tc_batch_launch(const scarf_tc_batch* batch, void* stream) {
     if (rc) return rc;
   }
   SCARF_CUDA(tc_batch_launch(batch->plan, batch->d_work, static_cast<cudaStream_t>(stream), kernel_ev0(),
-                             kernel_ev1()));
+                             kernel_ev1(), &batch->fork));
   return SCARF_OK;
 }
 

@@ -156,9 +156,17 @@ size_t tc_batch_plan(const TcBatchInput* in, int nfields, TcBatchPlan* out);
 // once all of its items are stored.
 cudaError_t tc_batch_upload(const TcBatchInput* in, const TcBatchPlan& plan, void* d_work,
                             int* done_flags_dev = nullptr);
+// A second stream and two events with which the C-image builder runs beside
+// the R/S builder (fork after the stream's prior work, join before the
+// persistent kernel); all null: both builders in order on the stream.
+struct BuilderFork {
+  cudaStream_t side = nullptr;
+  cudaEvent_t fork = nullptr, join = nullptr;
+};
 // Enqueue only: status/queue reset, table builds, persistent kernel.
 cudaError_t tc_batch_launch(const TcBatchPlan& plan, void* d_work, cudaStream_t stream,
-                            cudaEvent_t ev_main0 = nullptr, cudaEvent_t ev_main1 = nullptr);
+                            cudaEvent_t ev_main0 = nullptr, cudaEvent_t ev_main1 = nullptr,
+                            const BuilderFork* fork = nullptr);
 
 // ---- device side of the harmonic sampler (srm_sampler.cu) ----
 struct SampleEntry {

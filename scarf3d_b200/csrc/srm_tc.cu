@@ -540,8 +540,15 @@ size_t factor_smem_c(const TcPlan& p) {
 // needs. The factored builders walk harmonics one block at a time, each
 // step latency-bound (a sincos and two barriers), so they get many small
 // blocks: ~64 per SM over all fields.
+// With `fork`, the C-image builder runs on fork->side beside the R/S builder
+// (the two are independent: R/S are issue-bound FP64 work, C writes its
+// images at a good share of HBM bandwidth) and `stream` joins it afterwards.
 void launch_table_builders(const TableJob& T, const TableJob* jobs, int nfields, int max_stages, size_t smem_rs,
-                           size_t smem_c, int nsm, cudaStream_t stream, bool bf16) {
+                           size_t smem_c, int nsm, cudaStream_t stream, bool bf16, const BuilderFork* fork = nullptr) {
+  const bool forked = fork && fork->side && fork->fork && fork->join &&
+                      cudaEventRecord(fork->fork, stream) == cudaSuccess &&
+                      cudaStreamWaitEvent(fork->side, fork->fork, 0) == cudaSuccess;
+  const cudaStream_t cs = forked ? fork->side : stream;
   const int per_field = std::max(1, nsm * 64 / std::max(1, nfields));
   const int grid_old = std::max(1, std::min(64, nsm * 8 / std::max(1, nfields)));
   // Builder form: warps while each warp's factor tables fit (default), else
@@ -570,19 +577,23 @@ void launch_table_builders(const TableJob& T, const TableJob* jobs, int nfields,
   const dim3 g_old(jobs ? grid_old : nsm * 8, nfields);
   if (forced == 0 && smem_c <= warps_limit) {
     if (bf16)
-      tc_build_c_warps<true><<<g_warps, 32 * kBuilderWarps, kBuilderWarps * smem_c, stream>>>(T, jobs);
+      tc_build_c_warps<true><<<g_warps, 32 * kBuilderWarps, kBuilderWarps * smem_c, cs>>>(T, jobs);
     else
-      tc_build_c_warps<false><<<g_warps, 32 * kBuilderWarps, kBuilderWarps * smem_c, stream>>>(T, jobs);
+      tc_build_c_warps<false><<<g_warps, 32 * kBuilderWarps, kBuilderWarps * smem_c, cs>>>(T, jobs);
   } else if (forced <= 1 && smem_c <= static_cast<size_t>(kFactorSmem)) {
     if (bf16)
-      tc_build_c_factored<true><<<g_fact, 128, smem_c, stream>>>(T, jobs);
+      tc_build_c_factored<true><<<g_fact, 128, smem_c, cs>>>(T, jobs);
     else
-      tc_build_c_factored<false><<<g_fact, 128, smem_c, stream>>>(T, jobs);
+      tc_build_c_factored<false><<<g_fact, 128, smem_c, cs>>>(T, jobs);
   } else {
     if (bf16)
-      tc_build_c<true><<<g_old, 256, 0, stream>>>(T, jobs);
+      tc_build_c<true><<<g_old, 256, 0, cs>>>(T, jobs);
     else
-      tc_build_c<false><<<g_old, 256, 0, stream>>>(T, jobs);
+      tc_build_c<false><<<g_old, 256, 0, cs>>>(T, jobs);
+  }
+  if (forked) {
+    cudaEventRecord(fork->join, cs);
+    cudaStreamWaitEvent(stream, fork->join, 0);
   }
 }
 
@@ -1970,7 +1981,7 @@ cudaError_t tc_batch_upload(const TcBatchInput* in, const TcBatchPlan& bp, void*
 }
 
 cudaError_t tc_batch_launch(const TcBatchPlan& bp, void* d_work, cudaStream_t stream, cudaEvent_t ev_main0,
-                            cudaEvent_t ev_main1) {
+                            cudaEvent_t ev_main1, const BuilderFork* fork) {
   uint8_t* work = static_cast<uint8_t*>(d_work);
   const int nsm = device_sms();
   const TableJob* jobs = reinterpret_cast<const TableJob*>(work + bp.off_jobs);
@@ -1981,7 +1992,7 @@ cudaError_t tc_batch_launch(const TcBatchPlan& bp, void* d_work, cudaStream_t st
   e = cudaMemsetAsync(work + bp.off_done, 0, sizeof(int) * bp.nfields, stream);  // field completion counts
   if (e != cudaSuccess) return e;
   launch_table_builders(none, jobs, bp.nfields, bp.max_stages, bp.smem_rs, bp.smem_c, nsm, stream,
-                        bp.nfields > 0 && bp.plans[0].bf16 != 0);
+                        bp.nfields > 0 && bp.plans[0].bf16 != 0, fork);
   e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   TcKernelArgs A{};
