@@ -329,7 +329,7 @@ def run_batched(args, nfields=256):
                     "tables_kept_equal": all(len(a) == len(b) for a, b in zip(tabs, tabs2)),
                     "h2d_bytes_per_step": int(h_tabs.numel() * 4),
                     "d2h_bytes_per_step": int(sum(o.numel() * 4 for o in outs))},
-            "workload": "256 fields, axes log-uniform 32..256 (x16), VK/Gaussian alternating, cl U[500,5000] m, "
+            "workload": f"{nfields} fields, axes log-uniform 32..256 (x16), VK/Gaussian alternating, cl U[500,5000] m, "
                         "nharm U[2000,20000], ds 50 m, meta-seed 20240"}
 
 
@@ -946,7 +946,7 @@ def run_profile_leg(args, w):
 
     torch.cuda.set_device(0)
     if args.profile_leg == "batched":
-        print(json.dumps(run_batched(args)), flush=True)
+        print(json.dumps(run_batched(args, nfields=args.fields)), flush=True)
         return
     if args.profile_leg == "precision":
         print(json.dumps(run_precision_grid(args, w)), flush=True)
@@ -1004,6 +1004,8 @@ def main():
     ap.add_argument("--sigma", type=float, default=None)
     ap.add_argument("--nharm", type=int, default=None)
     ap.add_argument("--no-batched", action="store_true", help="skip the 256-field batched measurement")
+    ap.add_argument("--fields", type=int, default=256,
+                    help="fields of the batched profile leg (the first N of the 256-field workload)")
     ap.add_argument("--no-autotune", action="store_true", help="default plans instead of autotuned ones")
     ap.add_argument("--no-precision", action="store_true", help="skip the operand-precision comparison")
     ap.add_argument("--no-fim", action="store_true", help="skip the FIM (method 0) measurement")

@@ -191,6 +191,37 @@ size_t scarf_fim_workspace_bytes(const int npts[3], int npoi);
  * reference fills it (stats[4] host seconds, stats[5] device seconds). */
 int scarf_execute_ex(int seed, float *field, float stats[8], int flags);
 
+/* ---- contexts (no counterpart in the reference) ---------------------------
+ * A context is one independent library instance: the object that an
+ * initialize call sets up (scarflib.f90:87 keeps one for the whole process),
+ * the scarf_set_* settings that shape an execute (nharm, form, stream, host
+ * threads, sampler, uniform source, kernel timing, output overlap) and the
+ * device buffers of its execute path. Every thread starts on the process-wide
+ * default context, on which the reference-compatible API acts; a thread that
+ * makes another context current runs every entry point of this header and of
+ * scarf3d.h on it. Entry points are serialised inside the library, so any
+ * thread may call them; contexts let several meshes stay initialised at once
+ * (one per context) and give each thread its own. The kernel-form settings
+ * (scarf_set_tc_variant, _precision, _chunk, _autotune, scarf_set_direct_sincos)
+ * stay process-wide. */
+struct scarf_opt;
+typedef struct scarf_ctx scarf_ctx;
+scarf_ctx *scarf_ctx_create(void);
+/* Finalises the context and frees its device buffers; NULL and the default
+ * context are ignored. A calling thread that had it current returns to the
+ * default; no other thread may still have it current. */
+void scarf_ctx_destroy(scarf_ctx *ctx);
+/* Makes ctx the calling thread's current context (NULL: the default). */
+int scarf_ctx_make_current(scarf_ctx *ctx);
+/* scarf_cart_initialize, scarf_nocart_initialize, scarf_execute_ex and
+ * scarf_finalize on an explicit context, with a status. */
+int scarf_ctx_cart_initialize(scarf_ctx *ctx, int nd, const int fs[], const int fe[], float ds, int acf,
+                              const float cl[], float sigma, const struct scarf_opt *opt);
+int scarf_ctx_nocart_initialize(scarf_ctx *ctx, int nd, int npts, const float *x, const float *y, const float *z,
+                                float dh, int acf, const float cl[], float sigma, const struct scarf_opt *opt);
+int scarf_ctx_execute(scarf_ctx *ctx, int seed, float *field, float stats[8], int flags);
+int scarf_ctx_finalize(scarf_ctx *ctx);
+
 /* ---- building blocks ----------------------------------------------------- */
 int scarf_srm_compute_setup(const scarf_srm_params *p, scarf_srm_setup *s);
 /* table: nharm rows {v1,v2,v3,a,b} (FP32); *n_kept = rows written. */

@@ -9,6 +9,7 @@ from __future__ import annotations
 
 import ctypes
 import os
+import threading
 from pathlib import Path
 
 import numpy as np
@@ -39,7 +40,8 @@ EXPORTED_SYMBOLS = (
     "scarf_selftest_wait_limit", "scarf_set_tc_chunk", "scarf_set_tc_variant", "scarf_set_tc_precision",
     "scarf_set_direct_sincos", "scarf_fim_internal_grid", "scarf_fim_workspace_bytes",
     "scarf_set_output_overlap",
-    "scarf_execute_ex",
+    "scarf_execute_ex", "scarf_ctx_create", "scarf_ctx_destroy", "scarf_ctx_make_current",
+    "scarf_ctx_cart_initialize", "scarf_ctx_nocart_initialize", "scarf_ctx_execute", "scarf_ctx_finalize",
     "scarf_srm_compute_setup", "scarf_srm_sample", "scarf_srm_sample_device", "scarf_srm_sample_device_batch",
     "scarf_srm_sampler_reject_table", "scarf_set_sampler",
     "scarf_set_sampler_pass_pairs",
@@ -140,6 +142,15 @@ def _load() -> ctypes.CDLL:
         "scarf_fim_workspace_bytes": (ctypes.c_size_t, [c_void_p, c_int]),
         "scarf_set_output_overlap": (c_int, [c_int]),
         "scarf_execute_ex": (c_int, [c_int, c_void_p, fp, c_int]),
+        "scarf_ctx_create": (c_void_p, []),
+        "scarf_ctx_destroy": (None, [c_void_p]),
+        "scarf_ctx_make_current": (c_int, [c_void_p]),
+        "scarf_ctx_cart_initialize": (c_int, [c_void_p, c_int, ip, ip, c_float, c_int, fp, c_float,
+                                              ctypes.POINTER(ScarfOpt)]),
+        "scarf_ctx_nocart_initialize": (c_int, [c_void_p, c_int, c_int, fp, fp, fp, c_float, c_int, fp, c_float,
+                                                ctypes.POINTER(ScarfOpt)]),
+        "scarf_ctx_execute": (c_int, [c_void_p, c_int, c_void_p, fp, c_int]),
+        "scarf_ctx_finalize": (c_int, [c_void_p]),
         "scarf_srm_compute_setup": (c_int, [ctypes.POINTER(SrmParams), ctypes.POINTER(SrmSetup)]),
         "scarf_srm_sample": (c_int, [ctypes.POINTER(SrmParams), ctypes.POINTER(SrmSetup), c_void_p, ip,
                                      ctypes.POINTER(c_ll)]),
@@ -212,10 +223,71 @@ def _fptr(a):
 # --------------------------------------------------------------------------
 # Reference-style interface (scarflib.f90 generic procedures)
 # --------------------------------------------------------------------------
-class _State:
-    keep: list = []
-    n: tuple | None = None
-    structured = True
+class _MeshState:
+    """Python-side companions of one context's mesh: the arrays the library
+    borrows until finalize, and the field extent."""
+
+    def __init__(self):
+        self.keep: list = []
+        self.n: tuple | None = None
+        self.structured = True
+
+
+_DEFAULT_MESH = _MeshState()
+_tls = threading.local()
+
+
+def _cur() -> _MeshState:
+    """The calling thread's current context's mesh state (the default
+    context's outside `with Context()`)."""
+    return getattr(_tls, "mesh", _DEFAULT_MESH)
+
+
+class Context:
+    """One independent library instance (scarf_ctx): an initialised mesh, the
+    execute settings (nharm, form, stream, sampler, ...) and the device buffers
+    of its execute path. Several contexts hold different meshes at once.
+    Inside `with ctx:` the calling thread's current context is ctx, so
+    scarf_initialize, scarf_execute, scarf_finalize, set_nharm and the other
+    per-context settings act on it."""
+
+    def __init__(self):
+        self._h = lib.scarf_ctx_create()
+        if not self._h:
+            raise ScarfError(SCARF_ERR_NOMEM, last_error())
+        self._mesh = _MeshState()
+        self._mesh._ctx_handle = self._h
+
+    def __enter__(self):
+        if not self._h:
+            raise ScarfError(SCARF_ERR_STATE, "context is closed")
+        check(lib.scarf_ctx_make_current(ctypes.c_void_p(self._h)))
+        stack = getattr(_tls, "stack", None)
+        if stack is None:
+            stack = _tls.stack = []
+        stack.append(_cur())
+        _tls.mesh = self._mesh
+        return self
+
+    def __exit__(self, *exc):
+        outer_mesh = _tls.stack.pop()
+        _tls.mesh = outer_mesh
+        outer = getattr(outer_mesh, "_ctx_handle", None)
+        lib.scarf_ctx_make_current(ctypes.c_void_p(outer) if outer else None)
+        return False
+
+    def close(self):
+        if self._h:
+            lib.scarf_ctx_destroy(ctypes.c_void_p(self._h))
+            self._h = None
+            self._mesh = _MeshState()
+            self._mesh._ctx_handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def scarf_initialize(*, fs=None, fe=None, ds=None, x=None, y=None, z=None, dh=None, acf, cl, sigma,
@@ -256,8 +328,8 @@ def scarf_initialize(*, fs=None, fe=None, ds=None, x=None, y=None, z=None, dh=No
         lib.scarf_cart_initialize(nd, _iptr(fs), _iptr(fe), float(ds), int(acf),
                                   clv.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), float(sigma),
                                   ctypes.byref(opt))
-        _State.structured = True
-        _State.n = tuple(int(e) - int(s) + 1 for s, e in zip(fs, fe))
+        _cur().structured = True
+        _cur().n = tuple(int(e) - int(s) + 1 for s, e in zip(fs, fe))
     else:
         if ds is not None:
             opt.ds = float(ds)
@@ -269,23 +341,23 @@ def scarf_initialize(*, fs=None, fe=None, ds=None, x=None, y=None, z=None, dh=No
                                     ys.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), fpz, float(dh), int(acf),
                                     clv.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), float(sigma),
                                     ctypes.byref(opt))
-        _State.structured = False
-        _State.n = (len(xs),)
+        _cur().structured = False
+        _cur().n = (len(xs),)
     err = last_error()
     if err:
         raise ScarfError(SCARF_ERR_ARG, err)
-    _State.keep = keep  # the library borrows these until scarf_finalize
+    _cur().keep = keep  # the library borrows these until scarf_finalize
 
 
 def scarf_execute(seed: int, field=None, *, flags: int = 0):
     """Run the SRM; returns (field, stats[8]). `field` may be a NumPy array
     (host) or an object exposing a CUDA device pointer via `data_ptr()`
     (torch tensor), float32, column-major extent n0 x n1 x n2 / npts."""
-    if _State.n is None:
+    if _cur().n is None:
         raise ScarfError(SCARF_ERR_STATE, "scarf_execute before scarf_initialize")
     stats = np.zeros(8, np.float32)
     if field is None:
-        field = np.zeros(int(np.prod(_State.n)), np.float32)
+        field = np.zeros(int(np.prod(_cur().n)), np.float32)
     if hasattr(field, "data_ptr"):
         ptr = field.data_ptr()
         flags |= FIELD_ON_DEVICE if field.is_cuda else 0
@@ -300,8 +372,8 @@ def scarf_execute(seed: int, field=None, *, flags: int = 0):
 
 def scarf_finalize():
     lib.scarf_finalize()
-    _State.keep = []
-    _State.n = None
+    _cur().keep = []
+    _cur().n = None
 
 
 def scarf_io(npts, field, filename: str, nwriters=None):

@@ -80,8 +80,6 @@ struct Config {
   bool kernel_timing = false;
   int overlap_items = kDefaultSlabItems;  // work items per slab copied out while the kernel runs; 0 = off
 };
-Config g_cfg;
-float g_last_kernel_ms = 0.0f;
 
 // ------------------------------------------- reference-style global object --
 struct Object {
@@ -100,8 +98,7 @@ struct Object {
   const float* poi = nullptr;                            // borrowed, [nd x npoi]
   int npoi = 0;
 };
-Object g_obj;
-std::mutex g_mu;
+std::mutex g_mu;  // every entry point that touches a context holds it
 
 // --------------------------------------------------- per-device resources --
 struct DeviceBuf {
@@ -168,42 +165,70 @@ struct Resources {
     device = -1;
   }
 };
-Resources g_res;
+}  // namespace
+}  // namespace scarf
+
+// One library instance: the reference's global object, the settings and the
+// device resources of its execute path. The legacy entry points act on the
+// calling thread's current context (the process-wide default unless
+// scarf_ctx_make_current chose another), so several meshes can be initialised
+// at once, one per context (scarflib.f90:87 allows one).
+struct scarf_ctx {
+  scarf::Config cfg;
+  scarf::Object obj;
+  scarf::Resources res;
+  float last_kernel_ms = 0.0f;
+};
+
+namespace scarf {
+namespace {
+scarf_ctx g_default_ctx;
+thread_local scarf_ctx* t_ctx = &g_default_ctx;
+
+// Makes `c` the calling thread's current context for one entry point's call.
+class CtxScope {
+ public:
+  explicit CtxScope(scarf_ctx* c) : prev_(t_ctx) { t_ctx = c; }
+  ~CtxScope() { t_ctx = prev_; }
+
+ private:
+  scarf_ctx* prev_;
+};
 
 int ensure_resources() {
   int dev = 0;
   SCARF_CUDA(cudaGetDevice(&dev));
-  if (g_res.device != dev) {
-    g_res.release();
-    g_res.device = dev;
+  if (t_ctx->res.device != dev) {
+    t_ctx->res.release();
+    t_ctx->res.device = dev;
   }
-  SCARF_CUDA(g_res.status.ensure(256));
-  SCARF_CUDA(g_res.stats.ensure(stats_partials_bytes(0) + 256));
-  if (!g_res.ev0) SCARF_CUDA(cudaEventCreate(&g_res.ev0));
-  if (!g_res.ev1) SCARF_CUDA(cudaEventCreate(&g_res.ev1));
-  if (!g_res.evk0) SCARF_CUDA(cudaEventCreate(&g_res.evk0));
-  if (!g_res.evk1) SCARF_CUDA(cudaEventCreate(&g_res.evk1));
+  SCARF_CUDA(t_ctx->res.status.ensure(256));
+  SCARF_CUDA(t_ctx->res.stats.ensure(stats_partials_bytes(0) + 256));
+  if (!t_ctx->res.ev0) SCARF_CUDA(cudaEventCreate(&t_ctx->res.ev0));
+  if (!t_ctx->res.ev1) SCARF_CUDA(cudaEventCreate(&t_ctx->res.ev1));
+  if (!t_ctx->res.evk0) SCARF_CUDA(cudaEventCreate(&t_ctx->res.evk0));
+  if (!t_ctx->res.evk1) SCARF_CUDA(cudaEventCreate(&t_ctx->res.evk1));
   return SCARF_OK;
 }
 
 // Slab flags (host-mapped) and device counters for at least n slabs, plus the
 // copy stream and its join event.
 int ensure_slab_resources(int n) {
-  if (!g_res.copy_stream) SCARF_CUDA(cudaStreamCreateWithFlags(&g_res.copy_stream, cudaStreamNonBlocking));
-  if (!g_res.evs) SCARF_CUDA(cudaEventCreateWithFlags(&g_res.evs, cudaEventDisableTiming));
-  if (n > g_res.slab_cap) {
-    if (g_res.slab_flags) cudaFreeHost(g_res.slab_flags);
-    g_res.slab_flags = g_res.slab_flags_dev = nullptr;
-    g_res.slab_cap = 0;
+  if (!t_ctx->res.copy_stream) SCARF_CUDA(cudaStreamCreateWithFlags(&t_ctx->res.copy_stream, cudaStreamNonBlocking));
+  if (!t_ctx->res.evs) SCARF_CUDA(cudaEventCreateWithFlags(&t_ctx->res.evs, cudaEventDisableTiming));
+  if (n > t_ctx->res.slab_cap) {
+    if (t_ctx->res.slab_flags) cudaFreeHost(t_ctx->res.slab_flags);
+    t_ctx->res.slab_flags = t_ctx->res.slab_flags_dev = nullptr;
+    t_ctx->res.slab_cap = 0;
     void* h = nullptr;
     SCARF_CUDA(cudaHostAlloc(&h, sizeof(int) * n, cudaHostAllocMapped));
-    g_res.slab_flags = static_cast<int*>(h);
+    t_ctx->res.slab_flags = static_cast<int*>(h);
     void* d = nullptr;
     SCARF_CUDA(cudaHostGetDevicePointer(&d, h, 0));
-    g_res.slab_flags_dev = static_cast<int*>(d);
-    g_res.slab_cap = n;
+    t_ctx->res.slab_flags_dev = static_cast<int*>(d);
+    t_ctx->res.slab_cap = n;
   }
-  SCARF_CUDA(g_res.slab_cnt.ensure(sizeof(int) * n));
+  SCARF_CUDA(t_ctx->res.slab_cnt.ensure(sizeof(int) * n));
   return SCARF_OK;
 }
 
@@ -239,15 +264,15 @@ bool is_pageable(const void* p) {
 
 int ensure_bounce(size_t slot_bytes) {
   slot_bytes = (slot_bytes + 4095) / 4096 * 4096;
-  if (g_res.bounce && g_res.bounce_slot >= slot_bytes) return SCARF_OK;
-  if (g_res.bounce) cudaFreeHost(g_res.bounce);
-  g_res.bounce = nullptr;
-  g_res.bounce_slot = 0;
+  if (t_ctx->res.bounce && t_ctx->res.bounce_slot >= slot_bytes) return SCARF_OK;
+  if (t_ctx->res.bounce) cudaFreeHost(t_ctx->res.bounce);
+  t_ctx->res.bounce = nullptr;
+  t_ctx->res.bounce_slot = 0;
   void* h = nullptr;
   SCARF_CUDA(cudaHostAlloc(&h, slot_bytes * kBounceSlots, cudaHostAllocDefault));
-  g_res.bounce = static_cast<char*>(h);
-  g_res.bounce_slot = slot_bytes;
-  for (auto& e : g_res.bounce_ev)
+  t_ctx->res.bounce = static_cast<char*>(h);
+  t_ctx->res.bounce_slot = slot_bytes;
+  for (auto& e : t_ctx->res.bounce_ev)
     if (!e) SCARF_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
   return SCARF_OK;
 }
@@ -260,7 +285,7 @@ class BounceCopier {
   explicit BounceCopier(cudaStream_t cs) : cs_(cs) {}
   ~BounceCopier() { finish(); }
   int issue(char* dst, size_t dpitch, const char* src, size_t spitch, size_t width, size_t height) {
-    const size_t cap = g_res.bounce_slot;
+    const size_t cap = t_ctx->res.bounce_slot;
     const size_t rows_per = std::max<size_t>(1, cap / std::max<size_t>(width, 1));
     if (width > cap) {  // one row longer than a slot: split the row
       for (size_t r = 0; r < height; ++r)
@@ -298,9 +323,9 @@ class BounceCopier {
     next_ = (next_ + 1) % kBounceSlots;
     int rc = complete(slot);
     if (rc) return rc;
-    char* buf = g_res.bounce + static_cast<size_t>(slot) * g_res.bounce_slot;
+    char* buf = t_ctx->res.bounce + static_cast<size_t>(slot) * t_ctx->res.bounce_slot;
     SCARF_CUDA(cudaMemcpy2DAsync(buf, width, src, spitch, width, height, cudaMemcpyDeviceToHost, cs_));
-    SCARF_CUDA(cudaEventRecord(g_res.bounce_ev[slot], cs_));
+    SCARF_CUDA(cudaEventRecord(t_ctx->res.bounce_ev[slot], cs_));
     pend_[slot] = Pending{true, dst, dpitch, width, height};
     return SCARF_OK;
   }
@@ -308,8 +333,8 @@ class BounceCopier {
     Pending& q = pend_[slot];
     if (!q.busy) return SCARF_OK;
     q.busy = false;
-    SCARF_CUDA(cudaEventSynchronize(g_res.bounce_ev[slot]));
-    const char* buf = g_res.bounce + static_cast<size_t>(slot) * g_res.bounce_slot;
+    SCARF_CUDA(cudaEventSynchronize(t_ctx->res.bounce_ev[slot]));
+    const char* buf = t_ctx->res.bounce + static_cast<size_t>(slot) * t_ctx->res.bounce_slot;
     constexpr size_t kPiece = size_t(1) << 20;
     const size_t per_row = (q.width + kPiece - 1) / kPiece;
     const Pending w = q;
@@ -333,8 +358,8 @@ int copy_slabs_out(const TcPlan& plan, const TcSlabSignal& sig, const float* d_f
     const int rc = ensure_bounce(std::min(kBounceSlotCap, std::max<size_t>(slab_bytes, 1 << 20)));
     if (rc) return rc;
   }
-  BounceCopier bc(g_res.copy_stream);
-  volatile int* flags = g_res.slab_flags;
+  BounceCopier bc(t_ctx->res.copy_stream);
+  volatile int* flags = t_ctx->res.slab_flags;
   const size_t plane = static_cast<size_t>(plan.n1) * plan.n2;
   bool idle = false;
   for (int q = 0; q < sig.nslabs; ++q) {
@@ -356,7 +381,7 @@ int copy_slabs_out(const TcPlan& plan, const TcSlabSignal& sig, const float* d_f
       continue;
     }
     SCARF_CUDA(cudaMemcpy2DAsync(field + off, plane * sizeof(float), d_field + off, plane * sizeof(float), width,
-                                 e.z1 - e.z0, cudaMemcpyDeviceToHost, g_res.copy_stream));
+                                 e.z1 - e.z0, cudaMemcpyDeviceToHost, t_ctx->res.copy_stream));
   }
   return bc.finish();
 }
@@ -372,7 +397,7 @@ int copy_field_out(float* field, const float* d_field, long long npts, cudaStrea
   int rc = ensure_bounce(std::min(kBounceSlotCap, std::max<size_t>(bytes / kBounceSlots, 1 << 20)));
   if (rc) return rc;
   BounceCopier bc(st);
-  const size_t row = g_res.bounce_slot;
+  const size_t row = t_ctx->res.bounce_slot;
   const size_t rows = bytes / row, rest = bytes - rows * row;
   char* dst = reinterpret_cast<char*>(field);
   const char* src = reinterpret_cast<const char*>(d_field);
@@ -383,12 +408,12 @@ int copy_field_out(float* field, const float* d_field, long long npts, cudaStrea
 }
 
 // Events bracketing the dominant kernel of the next launch, when enabled.
-cudaEvent_t kernel_ev0() { return g_cfg.kernel_timing ? g_res.evk0 : nullptr; }
-cudaEvent_t kernel_ev1() { return g_cfg.kernel_timing ? g_res.evk1 : nullptr; }
+cudaEvent_t kernel_ev0() { return t_ctx->cfg.kernel_timing ? t_ctx->res.evk0 : nullptr; }
+cudaEvent_t kernel_ev1() { return t_ctx->cfg.kernel_timing ? t_ctx->res.evk1 : nullptr; }
 void collect_kernel_time() {
-  if (!g_cfg.kernel_timing) return;
+  if (!t_ctx->cfg.kernel_timing) return;
   float ms = 0.0f;
-  if (cudaEventElapsedTime(&ms, g_res.evk0, g_res.evk1) == cudaSuccess) g_last_kernel_ms = ms;
+  if (cudaEventElapsedTime(&ms, t_ctx->res.evk0, t_ctx->res.evk1) == cudaSuccess) t_ctx->last_kernel_ms = ms;
   cudaGetLastError();
 }
 
@@ -415,22 +440,22 @@ double now_s() {
 
 scarf_srm_params params_from_object(int seed) {
   scarf_srm_params p{};
-  p.acf = g_obj.acf;
-  p.nharm = g_cfg.nharm;
+  p.acf = t_ctx->obj.acf;
+  p.nharm = t_ctx->cfg.nharm;
   p.seed = seed;
-  p.rescale = g_obj.rescale;
-  p.hurst = g_obj.hurst;
-  p.sigma = g_obj.sigma;
-  p.ds = g_obj.ds;
-  p.dh = g_obj.dh;
+  p.rescale = t_ctx->obj.rescale;
+  p.hurst = t_ctx->obj.hurst;
+  p.sigma = t_ctx->obj.sigma;
+  p.ds = t_ctx->obj.ds;
+  p.dh = t_ctx->obj.dh;
   for (int c = 0; c < 3; ++c) {
-    p.cl[c] = g_obj.cl[c];
-    p.nc[c] = g_obj.nc[c];
-    p.fc[c] = g_obj.fc[c];
+    p.cl[c] = t_ctx->obj.cl[c];
+    p.nc[c] = t_ctx->obj.nc[c];
+    p.fc[c] = t_ctx->obj.fc[c];
   }
-  p.alpha = g_obj.alpha;
-  p.beta = g_obj.beta;
-  p.gamma = g_obj.gamma;
+  p.alpha = t_ctx->obj.alpha;
+  p.beta = t_ctx->obj.beta;
+  p.gamma = t_ctx->obj.gamma;
   return p;
 }
 
@@ -442,44 +467,44 @@ scarf_srm_params params_from_object(int seed) {
 // SCARF_TAPER_UNSTRUCTURED is set: initialize_unstructured drops the POIs
 // (scarflib.f90:273,283), for either method.
 int fim_execute_impl(int seed, float* field, float stats[8], int flags) {
-  cudaStream_t st = g_cfg.stream;
+  cudaStream_t st = t_ctx->cfg.stream;
   FimInputs in{};
-  in.ndim = g_obj.cl[2] > 0.0f ? 3 : 2;  // scarflib_fim.f90:770-774
-  in.acf = g_obj.acf;
-  in.pad = g_obj.pad;
-  in.rescale = g_obj.rescale;
+  in.ndim = t_ctx->obj.cl[2] > 0.0f ? 3 : 2;  // scarflib_fim.f90:770-774
+  in.acf = t_ctx->obj.acf;
+  in.pad = t_ctx->obj.pad;
+  in.rescale = t_ctx->obj.rescale;
   in.seed = seed;
-  in.ds = g_obj.ds;
-  in.dh = g_obj.dh;
-  in.sigma = g_obj.sigma;
-  in.hurst = g_obj.hurst;
-  in.mute = g_obj.mute;
-  in.taper = g_obj.taper;
+  in.ds = t_ctx->obj.ds;
+  in.dh = t_ctx->obj.dh;
+  in.sigma = t_ctx->obj.sigma;
+  in.hurst = t_ctx->obj.hurst;
+  in.mute = t_ctx->obj.mute;
+  in.taper = t_ctx->obj.taper;
   for (int c = 0; c < 3; ++c) {
-    in.cl[c] = g_obj.cl[c];
-    in.nc[c] = g_obj.nc[c];
-    in.fc[c] = g_obj.fc[c];
+    in.cl[c] = t_ctx->obj.cl[c];
+    in.nc[c] = t_ctx->obj.nc[c];
+    in.fc[c] = t_ctx->obj.fc[c];
   }
   if (in.acf != 0 && in.acf != 1) return fail(SCARF_ERR_ARG, "FIM: acf must be 0 (von Karman) or 1 (Gaussian)");
-  in.structured = g_obj.structured ? 1 : 0;
+  in.structured = t_ctx->obj.structured ? 1 : 0;
   long long npts;
-  if (g_obj.structured) {
+  if (t_ctx->obj.structured) {
     npts = 1;
     for (int c = 0; c < 3; ++c) {
-      in.fs[c] = g_obj.fs[c];
-      in.fe[c] = g_obj.fe[c];
-      npts *= g_obj.fe[c] - g_obj.fs[c] + 1;
+      in.fs[c] = t_ctx->obj.fs[c];
+      in.fe[c] = t_ctx->obj.fe[c];
+      npts *= t_ctx->obj.fe[c] - t_ctx->obj.fs[c] + 1;
     }
   } else {
-    npts = g_obj.npts;
+    npts = t_ctx->obj.npts;
   }
   if (npts <= 0) return fail(SCARF_ERR_ARG, "empty point set");
   in.npts = npts;
-  const bool taper_ok = g_obj.structured || (flags & SCARF_TAPER_UNSTRUCTURED);
-  if (taper_ok && g_obj.poi && g_obj.npoi > 0) {
-    in.poi = g_obj.poi;
-    in.npoi = g_obj.npoi;
-    in.poi_stride = g_obj.nd;
+  const bool taper_ok = t_ctx->obj.structured || (flags & SCARF_TAPER_UNSTRUCTURED);
+  if (taper_ok && t_ctx->obj.poi && t_ctx->obj.npoi > 0) {
+    in.poi = t_ctx->obj.poi;
+    in.npoi = t_ctx->obj.npoi;
+    in.poi_stride = t_ctx->obj.nd;
   }
   FimGrid g{};
   fim_grid(in, &g);
@@ -488,23 +513,23 @@ int fim_execute_impl(int seed, float* field, float stats[8], int flags) {
   const bool on_device = (flags & SCARF_FIELD_ON_DEVICE) || is_device_pointer(field);
   float* d_field = field;
   if (!on_device) {
-    SCARF_CUDA(g_res.field.ensure(sizeof(float) * npts));
-    d_field = static_cast<float*>(g_res.field.p);
+    SCARF_CUDA(t_ctx->res.field.ensure(sizeof(float) * npts));
+    d_field = static_cast<float*>(t_ctx->res.field.p);
   }
-  if (!g_obj.structured) {
+  if (!t_ctx->obj.structured) {
     const size_t stride = (static_cast<size_t>(npts) + 3) / 4 * 4;
-    SCARF_CUDA(g_res.coords.ensure(sizeof(float) * 3 * stride));
-    float* c = static_cast<float*>(g_res.coords.p);
-    SCARF_CUDA(cudaMemcpyAsync(c, g_obj.x, sizeof(float) * npts, cudaMemcpyDefault, st));
-    SCARF_CUDA(cudaMemcpyAsync(c + stride, g_obj.y, sizeof(float) * npts, cudaMemcpyDefault, st));
-    SCARF_CUDA(cudaMemcpyAsync(c + 2 * stride, g_obj.z, sizeof(float) * npts, cudaMemcpyDefault, st));
+    SCARF_CUDA(t_ctx->res.coords.ensure(sizeof(float) * 3 * stride));
+    float* c = static_cast<float*>(t_ctx->res.coords.p);
+    SCARF_CUDA(cudaMemcpyAsync(c, t_ctx->obj.x, sizeof(float) * npts, cudaMemcpyDefault, st));
+    SCARF_CUDA(cudaMemcpyAsync(c + stride, t_ctx->obj.y, sizeof(float) * npts, cudaMemcpyDefault, st));
+    SCARF_CUDA(cudaMemcpyAsync(c + 2 * stride, t_ctx->obj.z, sizeof(float) * npts, cudaMemcpyDefault, st));
     in.d_x = c;
     in.d_y = c + stride;
     in.d_z = c + 2 * stride;
   }
-  SCARF_CUDA(g_res.work.ensure(fim_workspace_bytes(g, in.npoi)));
+  SCARF_CUDA(t_ctx->res.work.ensure(fim_workspace_bytes(g, in.npoi)));
   const char* what = "";
-  const cudaError_t e = fim_run(in, g, g_res.work.p, d_field, stats, st, &what);
+  const cudaError_t e = fim_run(in, g, t_ctx->res.work.p, d_field, stats, st, &what);
   if (e != cudaSuccess) return fail(SCARF_ERR_CUDA, "FIM: %s: %s", what, cudaGetErrorString(e));
   if (!on_device) {
     const int rc = copy_field_out(field, d_field, npts, st);
@@ -517,15 +542,15 @@ int fim_execute_impl(int seed, float* field, float stats[8], int flags) {
 // The whole SRM execute (scarflib_srm.f90:505-929 / :105-499) for the global
 // object. field: host or device memory of the local block / point set.
 int execute_impl(int seed, float* field, float stats[8], int flags) {
-  if (!g_obj.ready) return fail(SCARF_ERR_STATE, "scarf_execute called before scarf_*_initialize");
+  if (!t_ctx->obj.ready) return fail(SCARF_ERR_STATE, "scarf_execute called before scarf_*_initialize");
   if (!field || !stats) return fail(SCARF_ERR_ARG, "field and stats must not be NULL");
   int rc = ensure_resources();
   if (rc) return rc;
   scarf::take_device_alloc_failure();
-  cudaStream_t st = g_cfg.stream;
+  cudaStream_t st = t_ctx->cfg.stream;
   for (int i = 0; i < 8; ++i) stats[i] = 0.0f;
-  if (g_obj.method == 0) return fim_execute_impl(seed, field, stats, flags);
-  if (g_obj.method != 1) return fail(SCARF_ERR_UNSUPPORTED, "method must be 0 (FIM) or 1 (SRM)");
+  if (t_ctx->obj.method == 0) return fim_execute_impl(seed, field, stats, flags);
+  if (t_ctx->obj.method != 1) return fail(SCARF_ERR_UNSUPPORTED, "method must be 0 (FIM) or 1 (SRM)");
 
   // Host: setup scalars and harmonic table.
   const double th0 = now_s();
@@ -534,11 +559,11 @@ int execute_impl(int seed, float* field, float stats[8], int flags) {
   rc = srm_setup(p, &s);
   if (rc) return fail(rc, "invalid SRM parameters (acf %d, nharm %d)", p.acf, p.nharm);
   std::vector<float> table(5 * static_cast<size_t>(p.nharm));
-  const int threads = g_cfg.threads > 0 ? g_cfg.threads : host_threads();
+  const int threads = t_ctx->cfg.threads > 0 ? t_ctx->cfg.threads : host_threads();
   long long pairs = 0;
-  const bool on_gpu = !g_cfg.src.srng && g_cfg.sampler != SCARF_SAMPLER_HOST;
+  const bool on_gpu = !t_ctx->cfg.src.srng && t_ctx->cfg.sampler != SCARF_SAMPLER_HOST;
   const int nh = on_gpu ? srm_sample_device(p, s, table.data(), &pairs, st, nullptr)
-                        : srm_sample(p, s, &g_cfg.src, threads, table.data(), &pairs);
+                        : srm_sample(p, s, &t_ctx->cfg.src, threads, table.data(), &pairs);
   if (nh == -2) return sampler_fail("device sampler");
   if (nh < 0)
     return fail(SCARF_ERR_ARG,
@@ -550,23 +575,23 @@ int execute_impl(int seed, float* field, float stats[8], int flags) {
   // Device work.
   long long npts;
   int n[3] = {1, 1, 1};
-  if (g_obj.structured) {
-    for (int c = 0; c < 3; ++c) n[c] = g_obj.fe[c] - g_obj.fs[c] + 1;
+  if (t_ctx->obj.structured) {
+    for (int c = 0; c < 3; ++c) n[c] = t_ctx->obj.fe[c] - t_ctx->obj.fs[c] + 1;
     npts = static_cast<long long>(n[0]) * n[1] * n[2];
   } else {
-    npts = g_obj.npts;
+    npts = t_ctx->obj.npts;
   }
   if (npts <= 0) return fail(SCARF_ERR_ARG, "empty point set");
   const bool on_device = (flags & SCARF_FIELD_ON_DEVICE) || is_device_pointer(field);
-  SCARF_CUDA(g_res.table.ensure(sizeof(float) * 5 * std::max(nh, 1)));
-  float* d_table = static_cast<float*>(g_res.table.p);
-  int* d_status = static_cast<int*>(g_res.status.p);
+  SCARF_CUDA(t_ctx->res.table.ensure(sizeof(float) * 5 * std::max(nh, 1)));
+  float* d_table = static_cast<float*>(t_ctx->res.table.p);
+  int* d_status = static_cast<int*>(t_ctx->res.status.p);
   float* d_field = field;
   if (!on_device) {
-    SCARF_CUDA(g_res.field.ensure(sizeof(float) * npts));
-    d_field = static_cast<float*>(g_res.field.p);
+    SCARF_CUDA(t_ctx->res.field.ensure(sizeof(float) * npts));
+    d_field = static_cast<float*>(t_ctx->res.field.p);
   }
-  SCARF_CUDA(cudaEventRecord(g_res.ev0, st));
+  SCARF_CUDA(cudaEventRecord(t_ctx->res.ev0, st));
   SCARF_CUDA(cudaMemsetAsync(d_status, 0, sizeof(int), st));
   if (nh > 0)
     SCARF_CUDA(cudaMemcpyAsync(d_table, table.data(), sizeof(float) * 5 * nh, cudaMemcpyHostToDevice, st));
@@ -574,14 +599,14 @@ int execute_impl(int seed, float* field, float stats[8], int flags) {
   const float* dx = nullptr;
   const float* dy = nullptr;
   const float* dz = nullptr;
-  const bool taper_ok = g_obj.structured || (flags & SCARF_TAPER_UNSTRUCTURED);
-  const bool tapering = taper_ok && g_obj.poi && g_obj.npoi > 0;
+  const bool taper_ok = t_ctx->obj.structured || (flags & SCARF_TAPER_UNSTRUCTURED);
+  const bool tapering = taper_ok && t_ctx->obj.poi && t_ctx->obj.npoi > 0;
   // Set once slab copies into the caller's buffer are in flight: every exit
   // from here on first waits for them.
   struct CopyJoin {
     bool active = false;
     ~CopyJoin() {
-      if (active && g_res.copy_stream) cudaStreamSynchronize(g_res.copy_stream);
+      if (active && t_ctx->res.copy_stream) cudaStreamSynchronize(t_ctx->res.copy_stream);
     }
   } copy_join;
   bool copied_out = false;  // field already on its way to the host (slab copies)
@@ -591,35 +616,35 @@ int execute_impl(int seed, float* field, float stats[8], int flags) {
   long long nrec = 0;
   auto want_records = [&](long long count) -> int {
     if (count <= 0) return SCARF_OK;
-    SCARF_CUDA(g_res.statrec.ensure(sizeof(StatRecord) * static_cast<size_t>(count)));
-    d_rec = static_cast<StatRecord*>(g_res.statrec.p);
+    SCARF_CUDA(t_ctx->res.statrec.ensure(sizeof(StatRecord) * static_cast<size_t>(count)));
+    d_rec = static_cast<StatRecord*>(t_ctx->res.statrec.p);
     nrec = count;
     return SCARF_OK;
   };
-  if (g_obj.structured) {
-    const bool use_tc = (g_cfg.form != SCARF_FORM_DIRECT);
+  if (t_ctx->obj.structured) {
+    const bool use_tc = (t_ctx->cfg.form != SCARF_FORM_DIRECT);
     TcPlan plan{};
     TcChoice tuned{};
     const bool have_tuned = use_tc && nh > 0 && tc_tuned_choice(s.ndim, n, true, &tuned);
     const bool planned = have_tuned ? tc_make_plan(s.ndim, n, nh, &plan, tuned.tile_j, false, tuned.variant)
                                     : tc_make_plan(s.ndim, n, nh, &plan);
     if (use_tc && nh > 0 && planned) {
-      SCARF_CUDA(g_res.work.ensure(plan.bytes));
+      SCARF_CUDA(t_ctx->res.work.ensure(plan.bytes));
       // Without rescale or taper the field is final when the kernel stores
       // it: copy it out slab by slab while the kernel still runs.
       TcSlabSignal sig;
-      const bool overlap = g_cfg.overlap_items > 0 && !on_device && p.rescale != 1 && !tapering;
+      const bool overlap = t_ctx->cfg.overlap_items > 0 && !on_device && p.rescale != 1 && !tapering;
       if (overlap) {
-        tc_slab_layout(plan, g_cfg.overlap_items, &sig);
+        tc_slab_layout(plan, t_ctx->cfg.overlap_items, &sig);
         rc = ensure_slab_resources(sig.nslabs);
         if (rc) return rc;
-        std::memset(g_res.slab_flags, 0, sizeof(int) * sig.nslabs);
-        sig.d_cnt = static_cast<int*>(g_res.slab_cnt.p);
-        sig.flag_dev = g_res.slab_flags_dev;
+        std::memset(t_ctx->res.slab_flags, 0, sizeof(int) * sig.nslabs);
+        sig.d_cnt = static_cast<int*>(t_ctx->res.slab_cnt.p);
+        sig.flag_dev = t_ctx->res.slab_flags_dev;
       }
       rc = want_records(tc_stat_records(plan));
       if (rc) return rc;
-      SCARF_CUDA(launch_tc_structured(s, g_obj.fs, n, p.ds, d_table, nh, d_field, g_res.work.p, plan, d_status, st,
+      SCARF_CUDA(launch_tc_structured(s, t_ctx->obj.fs, n, p.ds, d_table, nh, d_field, t_ctx->res.work.p, plan, d_status, st,
                                       kernel_ev0(), kernel_ev1(), overlap ? &sig : nullptr, d_rec));
       if (overlap) {
         copy_join.active = true;
@@ -631,20 +656,20 @@ int execute_impl(int seed, float* field, float stats[8], int flags) {
       rc = want_records(direct_stat_records(npts));
       if (rc) return rc;
       if (kernel_ev0()) SCARF_CUDA(cudaEventRecord(kernel_ev0(), st));
-      SCARF_CUDA(launch_direct_structured(s, g_obj.fs, n, p.ds, d_table, nh, d_field, d_status, st, d_rec));
+      SCARF_CUDA(launch_direct_structured(s, t_ctx->obj.fs, n, p.ds, d_table, nh, d_field, d_status, st, d_rec));
       if (kernel_ev1()) SCARF_CUDA(cudaEventRecord(kernel_ev1(), st));
     } else {
       SCARF_CUDA(cudaMemsetAsync(d_field, 0, sizeof(float) * npts, st));
     }
   } else {
-    SCARF_CUDA(g_res.coords.ensure(sizeof(float) * 3 * npts + 64));
-    float* c = static_cast<float*>(g_res.coords.p);
+    SCARF_CUDA(t_ctx->res.coords.ensure(sizeof(float) * 3 * npts + 64));
+    float* c = static_cast<float*>(t_ctx->res.coords.p);
     const size_t stride = (static_cast<size_t>(npts) + 3) / 4 * 4;  // keep each array 16-B aligned
-    SCARF_CUDA(g_res.coords.ensure(sizeof(float) * 3 * stride));
-    c = static_cast<float*>(g_res.coords.p);
-    SCARF_CUDA(cudaMemcpyAsync(c, g_obj.x, sizeof(float) * npts, cudaMemcpyDefault, st));
-    SCARF_CUDA(cudaMemcpyAsync(c + stride, g_obj.y, sizeof(float) * npts, cudaMemcpyDefault, st));
-    SCARF_CUDA(cudaMemcpyAsync(c + 2 * stride, g_obj.z, sizeof(float) * npts, cudaMemcpyDefault, st));
+    SCARF_CUDA(t_ctx->res.coords.ensure(sizeof(float) * 3 * stride));
+    c = static_cast<float*>(t_ctx->res.coords.p);
+    SCARF_CUDA(cudaMemcpyAsync(c, t_ctx->obj.x, sizeof(float) * npts, cudaMemcpyDefault, st));
+    SCARF_CUDA(cudaMemcpyAsync(c + stride, t_ctx->obj.y, sizeof(float) * npts, cudaMemcpyDefault, st));
+    SCARF_CUDA(cudaMemcpyAsync(c + 2 * stride, t_ctx->obj.z, sizeof(float) * npts, cudaMemcpyDefault, st));
     dx = c;
     dy = c + stride;
     dz = c + 2 * stride;
@@ -664,8 +689,8 @@ int execute_impl(int seed, float* field, float stats[8], int flags) {
   // kernel merges them (a field without harmonics takes the two FP64 passes
   // instead). The sum's status word comes back with them in one
   // synchronisation (after a failed sum the statistics are dropped).
-  double* d_part = static_cast<double*>(g_res.stats.p);
-  float* d_out = reinterpret_cast<float*>(static_cast<char*>(g_res.stats.p) + stats_partials_bytes(0));
+  double* d_part = static_cast<double*>(t_ctx->res.stats.p);
+  float* d_out = reinterpret_cast<float*>(static_cast<char*>(t_ctx->res.stats.p) + stats_partials_bytes(0));
   if (d_rec)
     SCARF_CUDA(launch_stats_records(d_rec, nrec, d_out, st));
   else
@@ -695,21 +720,21 @@ int execute_impl(int seed, float* field, float stats[8], int flags) {
       stats[3] = 0.0f;
     }
     if (tapering) {
-      poi3.assign(3 * static_cast<size_t>(g_obj.npoi), 0.0f);
-      for (int q = 0; q < g_obj.npoi; ++q)
-        for (int c = 0; c < s.ndim; ++c) poi3[3 * q + c] = g_obj.poi[g_obj.nd * q + c];
-      SCARF_CUDA(g_res.poi.ensure(sizeof(float) * poi3.size()));
-      SCARF_CUDA(cudaMemcpyAsync(g_res.poi.p, poi3.data(), sizeof(float) * poi3.size(), cudaMemcpyHostToDevice, st));
-      fa.d_poi = static_cast<const float*>(g_res.poi.p);
-      fa.npoi = g_obj.npoi;
-      fa.mute = g_obj.mute;
-      fa.taper = g_obj.taper;
-      if (g_obj.structured) {
+      poi3.assign(3 * static_cast<size_t>(t_ctx->obj.npoi), 0.0f);
+      for (int q = 0; q < t_ctx->obj.npoi; ++q)
+        for (int c = 0; c < s.ndim; ++c) poi3[3 * q + c] = t_ctx->obj.poi[t_ctx->obj.nd * q + c];
+      SCARF_CUDA(t_ctx->res.poi.ensure(sizeof(float) * poi3.size()));
+      SCARF_CUDA(cudaMemcpyAsync(t_ctx->res.poi.p, poi3.data(), sizeof(float) * poi3.size(), cudaMemcpyHostToDevice, st));
+      fa.d_poi = static_cast<const float*>(t_ctx->res.poi.p);
+      fa.npoi = t_ctx->obj.npoi;
+      fa.mute = t_ctx->obj.mute;
+      fa.taper = t_ctx->obj.taper;
+      if (t_ctx->obj.structured) {
         fa.n0 = n[0];
         fa.n1 = n[1];
-        fa.o0 = g_obj.fs[0] - 1;
-        fa.o1 = g_obj.fs[1] - 1;
-        fa.o2 = g_obj.fs[2] - 1;
+        fa.o0 = t_ctx->obj.fs[0] - 1;
+        fa.o1 = t_ctx->obj.fs[1] - 1;
+        fa.o2 = t_ctx->obj.fs[2] - 1;
         fa.dh = p.ds;
       } else {
         fa.d_x = dx;
@@ -721,12 +746,12 @@ int execute_impl(int seed, float* field, float stats[8], int flags) {
   }
   if (copied_out) {
     // Device time ends with the last slab copy.
-    SCARF_CUDA(cudaEventRecord(g_res.evs, st));
-    SCARF_CUDA(cudaStreamWaitEvent(g_res.copy_stream, g_res.evs, 0));
-    SCARF_CUDA(cudaEventRecord(g_res.ev1, g_res.copy_stream));
-    SCARF_CUDA(cudaStreamSynchronize(g_res.copy_stream));
+    SCARF_CUDA(cudaEventRecord(t_ctx->res.evs, st));
+    SCARF_CUDA(cudaStreamWaitEvent(t_ctx->res.copy_stream, t_ctx->res.evs, 0));
+    SCARF_CUDA(cudaEventRecord(t_ctx->res.ev1, t_ctx->res.copy_stream));
+    SCARF_CUDA(cudaStreamSynchronize(t_ctx->res.copy_stream));
   } else {
-    SCARF_CUDA(cudaEventRecord(g_res.ev1, st));
+    SCARF_CUDA(cudaEventRecord(t_ctx->res.ev1, st));
     if (!on_device) {
       rc = copy_field_out(field, d_field, npts, st);
       if (rc) return rc;
@@ -734,15 +759,15 @@ int execute_impl(int seed, float* field, float stats[8], int flags) {
   }
   SCARF_CUDA(cudaStreamSynchronize(st));
   float ms = 0.0f;
-  cudaEventElapsedTime(&ms, g_res.ev0, g_res.ev1);
+  cudaEventElapsedTime(&ms, t_ctx->res.ev0, t_ctx->res.ev1);
   stats[4] = static_cast<float>(t_host);
   stats[5] = ms * 1e-3f;
   return SCARF_OK;
 }
 
 void finalize_impl() {
-  g_obj = Object();
-  g_res.release();
+  t_ctx->obj = Object();
+  t_ctx->res.release();
 }
 
 }  // namespace
@@ -764,14 +789,16 @@ void scarf_opt_init(struct scarf_opt* var) {
   std::memset(var, 0, sizeof(*var));
 }
 
-void scarf_cart_initialize(const int nd, const int fs[], const int fe[], const real ds, const int acf,
-                           const real cl[], const real sigma, struct scarf_opt* var) {
-  std::lock_guard<std::mutex> lk(g_mu);
-  if ((nd != 2 && nd != 3) || !fs || !fe || !cl) {
-    fail(SCARF_ERR_ARG, "scarf_cart_initialize: nd must be 2 or 3 and fs, fe, cl non-NULL");
-    return;
-  }
-  Object& o = g_obj;
+}  // extern "C"
+
+namespace {
+// The bodies of the initialize entry points, on the current context (the
+// caller holds g_mu).
+int cart_initialize_impl(const int nd, const int fs[], const int fe[], const real ds, const int acf,
+                         const real cl[], const real sigma, const struct scarf_opt* var) {
+  if ((nd != 2 && nd != 3) || !fs || !fe || !cl)
+    return fail(SCARF_ERR_ARG, "scarf_cart_initialize: nd must be 2 or 3 and fs, fe, cl non-NULL");
+  Object& o = t_ctx->obj;
   o = Object();
   o.structured = true;
   o.nd = nd;
@@ -811,17 +838,15 @@ void scarf_cart_initialize(const int nd, const int fs[], const int fe[], const r
   }
   o.ready = true;
   g_last_error.clear();
+  return SCARF_OK;
 }
 
-void scarf_nocart_initialize(const int nd, const int npts, const real* x, const real* y, const real* z,
-                             const real dh, const int acf, const real cl[], const real sigma,
-                             struct scarf_opt* var) {
-  std::lock_guard<std::mutex> lk(g_mu);
-  if ((nd != 2 && nd != 3) || npts <= 0 || !x || !y || !cl || (nd == 3 && !z)) {
-    fail(SCARF_ERR_ARG, "scarf_nocart_initialize: invalid nd/npts or NULL coordinates");
-    return;
-  }
-  Object& o = g_obj;
+int nocart_initialize_impl(const int nd, const int npts, const real* x, const real* y, const real* z,
+                           const real dh, const int acf, const real cl[], const real sigma,
+                           const struct scarf_opt* var) {
+  if ((nd != 2 && nd != 3) || npts <= 0 || !x || !y || !cl || (nd == 3 && !z))
+    return fail(SCARF_ERR_ARG, "scarf_nocart_initialize: invalid nd/npts or NULL coordinates");
+  Object& o = t_ctx->obj;
   o = Object();
   o.structured = false;
   o.nd = nd;
@@ -877,6 +902,23 @@ void scarf_nocart_initialize(const int nd, const int npts, const real* x, const 
   }
   o.ready = true;
   g_last_error.clear();
+  return SCARF_OK;
+}
+}  // namespace
+
+extern "C" {
+
+void scarf_cart_initialize(const int nd, const int fs[], const int fe[], const real ds, const int acf,
+                           const real cl[], const real sigma, struct scarf_opt* var) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  cart_initialize_impl(nd, fs, fe, ds, acf, cl, sigma, var);
+}
+
+void scarf_nocart_initialize(const int nd, const int npts, const real* x, const real* y, const real* z,
+                             const real dh, const int acf, const real cl[], const real sigma,
+                             struct scarf_opt* var) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  nocart_initialize_impl(nd, npts, x, y, z, dh, acf, cl, sigma, var);
 }
 
 void scarf_execute(const int seed, real* field, real stats[]) {
@@ -895,13 +937,13 @@ void scarf_finalize(void) {
 void scarf_io_one(const int nd, const int* npts, const real* field, const char fname[], const int* nwriters) {
   (void)nwriters;
   std::lock_guard<std::mutex> lk(g_mu);
-  if (!g_obj.ready || !g_obj.structured || !npts || !field || !fname) {
+  if (!t_ctx->obj.ready || !t_ctx->obj.structured || !npts || !field || !fname) {
     fail(SCARF_ERR_STATE, "scarf_io_one: needs an initialized structured mesh");
     return;
   }
   long long gn[3] = {npts[0], nd > 1 ? npts[1] : 1, nd > 2 ? npts[2] : 1};
   int n[3];
-  for (int c = 0; c < 3; ++c) n[c] = g_obj.fe[c] - g_obj.fs[c] + 1;
+  for (int c = 0; c < 3; ++c) n[c] = t_ctx->obj.fe[c] - t_ctx->obj.fs[c] + 1;
   const int fd = open(fname, O_CREAT | O_WRONLY, 0644);
   if (fd < 0) {
     fail(SCARF_ERR_ARG, "scarf_io_one: cannot open %s", fname);
@@ -909,7 +951,7 @@ void scarf_io_one(const int nd, const int* npts, const real* field, const char f
   }
   for (int k = 0; k < n[2]; ++k)
     for (int j = 0; j < n[1]; ++j) {
-      const long long gi = (g_obj.fs[0] - 1) + gn[0] * ((g_obj.fs[1] - 1 + j) + gn[1] * (g_obj.fs[2] - 1 + k));
+      const long long gi = (t_ctx->obj.fs[0] - 1) + gn[0] * ((t_ctx->obj.fs[1] - 1 + j) + gn[1] * (t_ctx->obj.fs[2] - 1 + k));
       const real* src = field + static_cast<long long>(n[0]) * (j + static_cast<long long>(n[1]) * k);
       if (pwrite(fd, src, sizeof(real) * n[0], static_cast<off_t>(gi * sizeof(real))) < 0) {
         fail(SCARF_ERR_ARG, "scarf_io_one: write failed");
@@ -924,17 +966,17 @@ void scarf_io_one(const int nd, const int* npts, const real* field, const char f
 // (scarflib_common.f90:527-646), written as a 2-D column-major FP32 array.
 void scarf_io_slice(const int* npts, const char axis[], const int plane, const real* field, const char fname[]) {
   std::lock_guard<std::mutex> lk(g_mu);
-  if (!g_obj.ready || !g_obj.structured || !npts || !axis || !field || !fname) {
+  if (!t_ctx->obj.ready || !t_ctx->obj.structured || !npts || !axis || !field || !fname) {
     fail(SCARF_ERR_STATE, "scarf_io_slice: needs an initialized structured mesh");
     return;
   }
   const int cut = axis[0] == 'x' ? 0 : axis[0] == 'y' ? 1 : axis[0] == 'z' ? 2 : -1;
   if (cut < 0) return;
-  if (plane < g_obj.fs[cut] || plane > g_obj.fe[cut]) return;
+  if (plane < t_ctx->obj.fs[cut] || plane > t_ctx->obj.fe[cut]) return;
   int n[3];
-  for (int c = 0; c < 3; ++c) n[c] = g_obj.fe[c] - g_obj.fs[c] + 1;
+  for (int c = 0; c < 3; ++c) n[c] = t_ctx->obj.fe[c] - t_ctx->obj.fs[c] + 1;
   const int d0 = cut == 0 ? 1 : 0, d1 = cut == 2 ? 1 : 2;
-  const int cidx = plane - g_obj.fs[cut];
+  const int cidx = plane - t_ctx->obj.fs[cut];
   const int fd = open(fname, O_CREAT | O_WRONLY, 0644);
   if (fd < 0) {
     fail(SCARF_ERR_ARG, "scarf_io_slice: cannot open %s", fname);
@@ -949,7 +991,7 @@ void scarf_io_slice(const int* npts, const char axis[], const int plane, const r
       idx[d1] = b;
       row[a] = field[idx[0] + static_cast<long long>(n[0]) * (idx[1] + static_cast<long long>(n[1]) * idx[2])];
     }
-    const long long gi = (g_obj.fs[d0] - 1) + static_cast<long long>(npts[d0]) * (g_obj.fs[d1] - 1 + b);
+    const long long gi = (t_ctx->obj.fs[d0] - 1) + static_cast<long long>(npts[d0]) * (t_ctx->obj.fs[d1] - 1 + b);
     if (pwrite(fd, row.data(), sizeof(real) * n[d0], static_cast<off_t>(gi * sizeof(real))) < 0) break;
   }
   close(fd);
@@ -963,16 +1005,16 @@ const char* scarf_last_error(void) { return g_last_error.c_str(); }
 int scarf_set_nharm(int nharm) {
   if (nharm <= 0) return fail(SCARF_ERR_ARG, "nharm must be positive");
   std::lock_guard<std::mutex> lk(g_mu);
-  g_cfg.nharm = nharm;
+  t_ctx->cfg.nharm = nharm;
   return SCARF_OK;
 }
 
-int scarf_get_nharm(void) { return g_cfg.nharm; }
+int scarf_get_nharm(void) { return t_ctx->cfg.nharm; }
 
 int scarf_set_form(int form) {
   if (form < SCARF_FORM_AUTO || form > SCARF_FORM_TC) return fail(SCARF_ERR_ARG, "unknown form %d", form);
   std::lock_guard<std::mutex> lk(g_mu);
-  g_cfg.form = form;
+  t_ctx->cfg.form = form;
   return SCARF_OK;
 }
 
@@ -980,27 +1022,80 @@ int scarf_set_uniform_source(void (*set_seed)(int), void (*srng)(float*)) {
   if ((set_seed == nullptr) != (srng == nullptr))
     return fail(SCARF_ERR_ARG, "set_seed and srng must both be given or both be NULL");
   std::lock_guard<std::mutex> lk(g_mu);
-  g_cfg.src.set_seed = set_seed;
-  g_cfg.src.srng = srng;
+  t_ctx->cfg.src.set_seed = set_seed;
+  t_ctx->cfg.src.srng = srng;
   return SCARF_OK;
 }
 
 int scarf_set_stream(void* stream) {
   std::lock_guard<std::mutex> lk(g_mu);
-  g_cfg.stream = static_cast<cudaStream_t>(stream);
+  t_ctx->cfg.stream = static_cast<cudaStream_t>(stream);
   return SCARF_OK;
 }
 
 int scarf_set_host_threads(int nthreads) {
   if (nthreads < 0) return fail(SCARF_ERR_ARG, "nthreads must be >= 0");
   std::lock_guard<std::mutex> lk(g_mu);
-  g_cfg.threads = nthreads;
+  t_ctx->cfg.threads = nthreads;
   return SCARF_OK;
 }
 
 int scarf_execute_ex(int seed, float* field, float stats[8], int flags) {
   std::lock_guard<std::mutex> lk(g_mu);
   return execute_impl(seed, field, stats, flags);
+}
+
+scarf_ctx* scarf_ctx_create(void) {
+  auto* c = new (std::nothrow) scarf_ctx();
+  if (!c) fail(SCARF_ERR_NOMEM, "out of host memory");
+  return c;
+}
+
+void scarf_ctx_destroy(scarf_ctx* ctx) {
+  if (!ctx || ctx == &g_default_ctx) return;
+  std::lock_guard<std::mutex> lk(g_mu);
+  {
+    CtxScope scope(ctx);
+    finalize_impl();
+  }
+  if (t_ctx == ctx) t_ctx = &g_default_ctx;
+  delete ctx;
+}
+
+int scarf_ctx_make_current(scarf_ctx* ctx) {
+  t_ctx = ctx ? ctx : &g_default_ctx;
+  return SCARF_OK;
+}
+
+int scarf_ctx_cart_initialize(scarf_ctx* ctx, int nd, const int fs[], const int fe[], float ds, int acf,
+                              const float cl[], float sigma, const struct scarf_opt* opt) {
+  if (!ctx) return fail(SCARF_ERR_ARG, "NULL context");
+  std::lock_guard<std::mutex> lk(g_mu);
+  CtxScope scope(ctx);
+  return cart_initialize_impl(nd, fs, fe, ds, acf, cl, sigma, opt);
+}
+
+int scarf_ctx_nocart_initialize(scarf_ctx* ctx, int nd, int npts, const float* x, const float* y, const float* z,
+                                float dh, int acf, const float cl[], float sigma, const struct scarf_opt* opt) {
+  if (!ctx) return fail(SCARF_ERR_ARG, "NULL context");
+  std::lock_guard<std::mutex> lk(g_mu);
+  CtxScope scope(ctx);
+  return nocart_initialize_impl(nd, npts, x, y, z, dh, acf, cl, sigma, opt);
+}
+
+int scarf_ctx_execute(scarf_ctx* ctx, int seed, float* field, float stats[8], int flags) {
+  if (!ctx) return fail(SCARF_ERR_ARG, "NULL context");
+  std::lock_guard<std::mutex> lk(g_mu);
+  CtxScope scope(ctx);
+  return execute_impl(seed, field, stats, flags);
+}
+
+int scarf_ctx_finalize(scarf_ctx* ctx) {
+  if (!ctx) return fail(SCARF_ERR_ARG, "NULL context");
+  std::lock_guard<std::mutex> lk(g_mu);
+  CtxScope scope(ctx);
+  finalize_impl();
+  return SCARF_OK;
 }
 
 int scarf_srm_compute_setup(const scarf_srm_params* p, scarf_srm_setup* s) {
@@ -1013,7 +1108,7 @@ int scarf_srm_compute_setup(const scarf_srm_params* p, scarf_srm_setup* s) {
 int scarf_set_sampler(int where) {
   if (where < SCARF_SAMPLER_AUTO || where > SCARF_SAMPLER_DEVICE) return fail(SCARF_ERR_ARG, "unknown sampler");
   std::lock_guard<std::mutex> lk(g_mu);
-  g_cfg.sampler = where;
+  t_ctx->cfg.sampler = where;
   return SCARF_OK;
 }
 
@@ -1072,9 +1167,9 @@ int scarf_srm_sample(const scarf_srm_params* p, const scarf_srm_setup* s, float*
   UniformSource src;
   {
     std::lock_guard<std::mutex> lk(g_mu);
-    src = g_cfg.src;
+    src = t_ctx->cfg.src;
   }
-  const int threads = g_cfg.threads > 0 ? g_cfg.threads : host_threads();
+  const int threads = t_ctx->cfg.threads > 0 ? t_ctx->cfg.threads : host_threads();
   long long used = 0;
   const int kept = srm_sample(*p, *s, &src, threads, table, &used);
   if (kept < 0)
@@ -1093,7 +1188,7 @@ int scarf_srm_direct_structured(const scarf_srm_setup* s, const int fs[3], const
   int rc = ensure_resources();
   if (rc) return rc;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  int* d_status = static_cast<int*>(g_res.status.p);
+  int* d_status = static_cast<int*>(t_ctx->res.status.p);
   SCARF_CUDA(cudaMemsetAsync(d_status, 0, sizeof(int), st));
   if (nh == 0) {
     SCARF_CUDA(cudaMemsetAsync(d_field, 0, sizeof(float) * n[0] * n[1] * n[2], st));
@@ -1115,7 +1210,7 @@ int scarf_srm_direct_points(const scarf_srm_setup* s, const float* d_x, const fl
   int rc = ensure_resources();
   if (rc) return rc;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  int* d_status = static_cast<int*>(g_res.status.p);
+  int* d_status = static_cast<int*>(t_ctx->res.status.p);
   SCARF_CUDA(cudaMemsetAsync(d_status, 0, sizeof(int), st));
   if (nh == 0) {
     SCARF_CUDA(cudaMemsetAsync(d_field, 0, sizeof(float) * npts, st));
@@ -1171,7 +1266,7 @@ int scarf_srm_tc_structured(const scarf_srm_setup* s, const int fs[3], const int
   if (work_bytes < p.bytes) return fail(SCARF_ERR_ARG, "workspace too small: %zu < %zu", work_bytes, p.bytes);
   if (reinterpret_cast<uintptr_t>(d_work) & 255u) return fail(SCARF_ERR_ARG, "workspace must be 256-byte aligned");
   std::lock_guard<std::mutex> lk(g_mu);
-  if (g_cfg.kernel_timing) {
+  if (t_ctx->cfg.kernel_timing) {
     const int rc = ensure_resources();
     if (rc) return rc;
   }
@@ -1304,7 +1399,7 @@ int scarf_srm_tc_batch_set_host_outputs(scarf_tc_batch* batch, float* const* hos
 
 int scarf_srm_tc_batch_launch(const scarf_tc_batch* batch, void* stream) {
   if (!batch) return fail(SCARF_ERR_ARG, "NULL batch");
-  if (g_cfg.kernel_timing) {
+  if (t_ctx->cfg.kernel_timing) {
     const int rc = ensure_resources();
     if (rc) return rc;
   }
@@ -1356,7 +1451,7 @@ void scarf_srm_tc_batch_destroy(scarf_tc_batch* batch) { delete batch; }
 
 int scarf_set_kernel_timing(int enable) {
   std::lock_guard<std::mutex> lk(g_mu);
-  g_cfg.kernel_timing = enable != 0;
+  t_ctx->cfg.kernel_timing = enable != 0;
   return SCARF_OK;
 }
 
@@ -1369,12 +1464,12 @@ size_t scarf_device_memory_in_use(void) { return scarf::device_memory_in_use(); 
 
 int scarf_release_device_memory(void) {
   std::lock_guard<std::mutex> lk(g_mu);
-  if (g_res.device >= 0) {
+  if (t_ctx->res.device >= 0) {
     int dev = 0;
     SCARF_CUDA(cudaGetDevice(&dev));
-    SCARF_CUDA(cudaSetDevice(g_res.device));
+    SCARF_CUDA(cudaSetDevice(t_ctx->res.device));
     SCARF_CUDA(cudaDeviceSynchronize());
-    g_res.release();
+    t_ctx->res.release();
     SCARF_CUDA(cudaSetDevice(dev));
   }
   scarf::release_sampler_device_memory();
@@ -1393,7 +1488,7 @@ int scarf_selftest_wait_limit(int blocks, int* device_status, double* waited_s) 
   int status = -1;
   unsigned long long waited = 0;
   bool timed_out = false;
-  SCARF_CUDA(scarf::run_wait_limit_probe(blocks, d, g_cfg.stream, &status, &waited, &timed_out));
+  SCARF_CUDA(scarf::run_wait_limit_probe(blocks, d, t_ctx->cfg.stream, &status, &waited, &timed_out));
   if (device_status) *device_status = status;
   if (waited_s) *waited_s = static_cast<double>(waited) * 1e-9;
   if (!timed_out)
@@ -1402,7 +1497,7 @@ int scarf_selftest_wait_limit(int blocks, int* device_status, double* waited_s) 
   return SCARF_OK;
 }
 
-float scarf_last_kernel_ms(void) { return g_last_kernel_ms; }
+float scarf_last_kernel_ms(void) { return t_ctx->last_kernel_ms; }
 
 int scarf_set_tc_chunk(int harmonics) {
   if (harmonics < 0) return fail(SCARF_ERR_ARG, "chunk must be >= 0");
@@ -1414,7 +1509,7 @@ int scarf_set_tc_chunk(int harmonics) {
 int scarf_set_output_overlap(int items_per_slab) {
   if (items_per_slab < 0) return fail(SCARF_ERR_ARG, "items_per_slab must be >= 0");
   std::lock_guard<std::mutex> lk(g_mu);
-  g_cfg.overlap_items = items_per_slab == 1 ? kDefaultSlabItems : items_per_slab;
+  t_ctx->cfg.overlap_items = items_per_slab == 1 ? kDefaultSlabItems : items_per_slab;
   return SCARF_OK;
 }
 
