@@ -858,7 +858,9 @@ def run_b200(args, w):
                          "peak_kind": peak_kind, "peak_sustained": peak_sustained,
                          "frac_of_sustained": achieved / peak_sustained,
                          "kernel": "srm_tc_kernel", "kernel_ms": k_avg_s * 1e3,
-                         "flop_per_launch": flops_launch},
+                         "flop_per_launch": flops_launch,
+                         # the field's one store per point, as HBM write bandwidth over the launch
+                         "output_store": {"bytes": npts * 4, "gbs": npts * 4 / k_avg_s / 1e9}},
             "direct_sum": {"value": direct_rate, "unit": UNIT, "harmonics_timed": nh,
                            "kernel_ms": float(np.mean(d_ms)), "tc_over_direct": value / direct_rate,
                            "roofline": _direct_roofline(direct_rate, clocks.get("sm_max_mhz")),
