@@ -92,3 +92,47 @@ def test_destroying_the_current_context_returns_to_the_default():
     sb.lib.scarf_ctx_destroy(ctypes.c_void_p(h))
     assert sb.lib.scarf_get_nharm() == 10000
     sb.lib.scarf_ctx_destroy(None)  # ignored
+
+
+def test_contexts_from_a_c_program(tmp_path):
+    """The context entry points as a C caller links them: two meshes kept at
+    once, status codes, and the default context untouched."""
+    import subprocess
+    from pathlib import Path
+    root = Path(__file__).resolve().parent.parent
+    pkg = root / "scarf3d_b200"
+    src = tmp_path / "ctx.c"
+    src.write_text(r"""
+#include <stdio.h>
+#include "scarf3d.h"
+#include "scarf3d_b200.h"
+int main(void) {
+  const int fs[3] = {1, 1, 1}, fa[3] = {8, 6, 4}, fb[3] = {4, 4, 4};
+  const float cl[3] = {500.f, 500.f, 500.f};
+  struct scarf_opt opt;
+  scarf_opt_init(&opt);
+  opt.method = 1;
+  opt.hurst = 0.5f;
+  scarf_ctx *a = scarf_ctx_create(), *b = scarf_ctx_create();
+  if (!a || !b) return 1;
+  if (scarf_ctx_cart_initialize(a, 3, fs, fa, 50.f, 0, cl, 0.1f, &opt) != SCARF_OK) return 2;
+  if (scarf_ctx_cart_initialize(b, 3, fs, fb, 25.f, 1, cl, 0.1f, &opt) != SCARF_OK) return 3;
+  scarf_ctx_make_current(a);
+  if (scarf_set_nharm(321) != SCARF_OK || scarf_get_nharm() != 321) return 4;
+  scarf_ctx_make_current(NULL);
+  if (scarf_get_nharm() != 10000) return 5;
+  float field[8], stats[8];
+  if (scarf_execute_ex(1, field, stats, 0) != SCARF_ERR_STATE) return 6;  /* default: no mesh */
+  if (scarf_ctx_finalize(b) != SCARF_OK) return 7;
+  if (scarf_ctx_execute(b, 1, field, stats, 0) != SCARF_ERR_STATE) return 8;  /* b finalised */
+  scarf_ctx_destroy(a);
+  scarf_ctx_destroy(b);
+  printf("ok\n");
+  return 0;
+}
+""")
+    exe = tmp_path / "ctx"
+    subprocess.run(["gcc", "-std=c11", f"-I{root / 'include'}", str(src), f"-L{pkg}", "-lscarf3d_b200",
+                    f"-Wl,-rpath,{pkg}", "-o", str(exe)], check=True)
+    r = subprocess.run([str(exe)], capture_output=True, text=True)
+    assert r.returncode == 0 and r.stdout.strip() == "ok", (r.returncode, r.stdout, r.stderr)
