@@ -5,7 +5,8 @@
 // (scarflib_srm.f90:794-809 structured, :397-406 points, :843-851 scaling).
 // The rotated coordinates P are loop invariant in the reference, so they are
 // computed once per point; the harmonic table streams through shared memory
-// in tiles moved by 1-D bulk (TMA) copies, double-buffered on mbarriers.
+// in tiles moved by 1-D bulk (TMA) copies, double-buffered on mbarriers,
+// and every thread reads four table rows at a time with five 16-byte loads.
 #include <cuda_runtime.h>
 
 #include "common.cuh"
@@ -16,7 +17,7 @@ namespace {
 
 constexpr int kTile = 256;           // harmonics per shared-memory tile
 constexpr int kRow = 5;              // floats per table row {v1,v2,v3,a,b}
-constexpr int kPts = 4;              // points per thread (one float4 store)
+constexpr int kPts = 8;              // points per thread (two float4 stores)
 constexpr int kThreads = 128;
 constexpr uint32_t kTileBytes = kTile * kRow * 4;  // 5120, multiple of 16
 
@@ -53,9 +54,12 @@ __device__ __forceinline__ void rotate(const DirectArgs& A, float x, float y, fl
 // Accurate (kFast = false): CUDA's sincosf, correctly rounded to ~1 ulp with
 // full range reduction. Fast (default): the phase reduced to [-pi, pi] by
 // Cody-Waite's method (Cody & Waite, "Software Manual for the Elementary
-// Functions", 1980) with 2 pi split into three floats (C1 + C2 + C3; the
-// residual is 4e-23), each product applied by one FMA, then the SFU's
-// __sinf/__cosf, whose absolute error on [-pi, pi] is about 2^-21.4. For the
+// Functions", 1980) with 2 pi split into two floats C1 + C2 (the residual,
+// 6.9e-15, times |j| < 2^22 stays below 3e-8), each product applied by one
+// FMA, then the SFU's __sinf/__cosf, whose absolute error on [-pi, pi] is
+// about 2^-21.4. C1 has 24 significant bits, so arg - j C1 is exact (a
+// multiple of 2^-21 below 2^2 in magnitude, or Sterbenz's case for |j| = 1);
+// only the C2 step rounds. For the
 // phases here (|arg| < 1e4 rad) the reduced argument is within ~2.5e-7 of
 // exact, so each term is within ~6e-7 absolute, and fields agree with the
 // FP32 restatement (glibc sinf/cosf) to ~4e-7 of their standard deviation.
@@ -64,21 +68,20 @@ __device__ __forceinline__ void rotate(const DirectArgs& A, float x, float y, fl
 constexpr float kInv2Pi = 0x1.45f306p-3f;
 constexpr float kTwoPi1 = 0x1.921fb6p+2f;
 constexpr float kTwoPi2 = -0x1.777a5cp-23f;
-constexpr float kTwoPi3 = -0x1.ee59dap-48f;
 
-// Nearest integer of t for |t| < 2^22 on the FMA pipe (round to nearest
-// even, as rintf): adding and subtracting 1.5 * 2^23 leaves the integer
-// part. rintf itself would issue on the SFU's pipe, which __sinf and __cosf
-// already saturate here.
+// Nearest integer of arg / (2 pi) for |arg / (2 pi)| < 2^22 on the FMA pipe:
+// one FMA adds 1.5 * 2^23 to the exact product (rounding it to an integer,
+// nearest even) and a subtraction removes it. rintf itself would issue on
+// the SFU's pipe, which __sinf and __cosf already saturate here. Near a
+// half-integer either neighbour may be chosen; both leave |r| <= pi + 3e-7.
 constexpr float kRoundMagic = 0x1.8p23f;
 
 template <bool kFast>
 __device__ __forceinline__ void phase_sincos(float arg, float* sn, float* cs) {
   if constexpr (kFast) {
-    const float j = __fsub_rn(__fadd_rn(__fmul_rn(arg, kInv2Pi), kRoundMagic), kRoundMagic);
+    const float j = __fsub_rn(__fmaf_rn(arg, kInv2Pi, kRoundMagic), kRoundMagic);
     float r = fmaf(-j, kTwoPi1, arg);
     r = fmaf(-j, kTwoPi2, r);
-    r = fmaf(-j, kTwoPi3, r);
     *sn = __sinf(r);
     *cs = __cosf(r);
   } else {
@@ -155,10 +158,7 @@ __global__ void __launch_bounds__(kThreads) srm_direct_kernel(const DirectArgs A
     }
     if (!__syncthreads_and(ok)) break;  // all threads agree before consuming
     const float* tb = s_tab[buf];
-#pragma unroll 2
-    for (int h = 0; h < rows; ++h) {
-      const float v1 = tb[h * kRow + 0], v2 = tb[h * kRow + 1], v3 = tb[h * kRow + 2];
-      const float a = tb[h * kRow + 3], b = tb[h * kRow + 4];
+    auto harmonic = [&](float v1, float v2, float v3, float a, float b) {
 #pragma unroll
       for (int q = 0; q < kPts; ++q) {
         const float arg = __fadd_rn(__fadd_rn(__fmul_rn(v1, P1[q]), __fmul_rn(v2, P2[q])), __fmul_rn(v3, P3[q]));
@@ -166,7 +166,18 @@ __global__ void __launch_bounds__(kThreads) srm_direct_kernel(const DirectArgs A
         phase_sincos<kFast>(arg, &sn, &cs);
         acc[q] = __fadd_rn(__fadd_rn(acc[q], __fmul_rn(a, sn)), __fmul_rn(b, cs));
       }
+    };
+    // Four rows (20 floats, 80 bytes from a 16-byte aligned tile) per step.
+    int h = 0;
+    for (; h + 4 <= rows; h += 4) {
+      const float4* g4 = reinterpret_cast<const float4*>(tb + h * kRow);
+      const float4 q0 = g4[0], q1 = g4[1], q2 = g4[2], q3 = g4[3], q4 = g4[4];
+      harmonic(q0.x, q0.y, q0.z, q0.w, q1.x);
+      harmonic(q1.y, q1.z, q1.w, q2.x, q2.y);
+      harmonic(q2.z, q2.w, q3.x, q3.y, q3.z);
+      harmonic(q3.w, q4.x, q4.y, q4.z, q4.w);
     }
+    for (; h < rows; ++h) harmonic(tb[h * kRow + 0], tb[h * kRow + 1], tb[h * kRow + 2], tb[h * kRow + 3], tb[h * kRow + 4]);
     __syncthreads();  // buffer `buf` fully consumed
     if (tid == 0 && aligned && t + 2 < nfull) {
       mbar_arrive_expect_tx(&s_full[buf], kTileBytes);
@@ -189,7 +200,9 @@ __global__ void __launch_bounds__(kThreads) srm_direct_kernel(const DirectArgs A
   for (int q = 0; q < kPts; ++q) out[q] = __fmul_rn(acc[q], A.scaling);
   float* dst = A.field + p0;
   if (p0 + kPts <= A.npts && (reinterpret_cast<uintptr_t>(dst) & 15u) == 0) {
-    *reinterpret_cast<float4*>(dst) = make_float4(out[0], out[1], out[2], out[3]);
+#pragma unroll
+    for (int q = 0; q < kPts; q += 4)
+      *reinterpret_cast<float4*>(dst + q) = make_float4(out[q], out[q + 1], out[q + 2], out[q + 3]);
   } else {
 #pragma unroll
     for (int q = 0; q < kPts; ++q)
