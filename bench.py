@@ -446,30 +446,37 @@ def _structured_leg(cfg, forms, steps, e2e_steps, peaks, clocks, cpu_full=False,
         del work
     del field
     torch.cuda.empty_cache()
-    # End to end: scarf_execute into a page-locked host field.
-    ef = e2e_form or forms[0]
+    # End to end: scarf_execute into a page-locked host field, with the
+    # named form and (when timed above) the tensor-core form as well.
     host = torch.empty(npts, dtype=torch.float32, pin_memory=True)
-    sb.set_nharm(cfg["nharm"])
-    sb.set_form(sb.FORM_TC if ef == "tc" else sb.FORM_DIRECT)
-    sb.set_stream(stream.cuda_stream)
-    sb.scarf_initialize(fs=fs, fe=fe, ds=ds, acf=cfg["acf"], cl=cfg["cl"], sigma=cfg["sigma"], method=1,
-                        hurst=cfg["hurst"], nc=np.asarray(nc, np.float32), fc=np.asarray(fc, np.float32))
-    stats = np.zeros(8, np.float32)
-    fptr = ctypes.c_void_p(host.data_ptr())
-    sp = stats.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
-    try:
-        sb.check(sb.lib.scarf_execute_ex(cfg["seed"], fptr, sp, 0))
-        t0 = time.perf_counter()
-        for _ in range(e2e_steps):
+
+    def e2e(form):
+        sb.set_nharm(cfg["nharm"])
+        sb.set_form(sb.FORM_TC if form == "tc" else sb.FORM_DIRECT)
+        sb.set_stream(stream.cuda_stream)
+        sb.scarf_initialize(fs=fs, fe=fe, ds=ds, acf=cfg["acf"], cl=cfg["cl"], sigma=cfg["sigma"], method=1,
+                            hurst=cfg["hurst"], nc=np.asarray(nc, np.float32), fc=np.asarray(fc, np.float32))
+        stats = np.zeros(8, np.float32)
+        fptr = ctypes.c_void_p(host.data_ptr())
+        sp = stats.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+        try:
             sb.check(sb.lib.scarf_execute_ex(cfg["seed"], fptr, sp, 0))
-        t_e2e = (time.perf_counter() - t0) / e2e_steps
-    finally:
-        sb.scarf_finalize()
-        sb.set_form(sb.FORM_AUTO)
-        sb.set_nharm(10000)
-    out["e2e"] = {"value": float(npts) * nh / t_e2e, "unit": UNIT, "form": ef, "ms_per_step": t_e2e * 1e3,
-                  "steps": e2e_steps, "host_memory": "page-locked", "h2d_bytes_per_step": int(nh * 20),
-                  "d2h_bytes_per_step": int(npts * 4 + 8), "stats_std_mean": [float(stats[2]), float(stats[3])]}
+            t0 = time.perf_counter()
+            for _ in range(e2e_steps):
+                sb.check(sb.lib.scarf_execute_ex(cfg["seed"], fptr, sp, 0))
+            t_e2e = (time.perf_counter() - t0) / e2e_steps
+        finally:
+            sb.scarf_finalize()
+            sb.set_form(sb.FORM_AUTO)
+            sb.set_nharm(10000)
+        return {"value": float(npts) * nh / t_e2e, "unit": UNIT, "form": form, "ms_per_step": t_e2e * 1e3,
+                "steps": e2e_steps, "host_memory": "page-locked", "h2d_bytes_per_step": int(nh * 20),
+                "d2h_bytes_per_step": int(npts * 4 + 8), "stats_std_mean": [float(stats[2]), float(stats[3])]}
+
+    ef = e2e_form or forms[0]
+    out["e2e"] = e2e(ef)
+    if ef != "tc" and "tc" in forms:
+        out["e2e_tc"] = e2e("tc")
     del host
     if cpu_full:
         nth = os.cpu_count() or 1
