@@ -347,8 +347,9 @@ CONFIG2 = dict(name="plain_unstructured_2e6pts_20x20x10km_gs_cl1500/1500/500_nha
                sigma=0.1, nharm=10000, seed=7)
 CONFIG5 = dict(name="large_structured_2048x2048x512_ds10m_vk_h0.3_cl5000/5000/2000_nharm50000", n=[2048, 2048, 512],
                ds=10.0, acf=0, hurst=0.3, cl=[5000.0, 5000.0, 2000.0], sigma=0.08, nharm=50000, seed=1234)
-DIRECT_WARP_INSTR_PER_PTHARM = 0.574  # ncu: sm__inst_executed per point*harmonic of srm_direct_kernel (fast sincos)
-FP32_FLOP_PER_PTHARM = 9             # phase 3 mul + 2 add, accumulate 2 mul + 2 add (plus one sincosf)
+DIRECT_WARP_INSTR_PER_PTHARM = 0.513  # ncu: sm__inst_executed per point*harmonic of srm_direct_kernel (fast sincos)
+DIRECT_MUFU_PER_PTHARM = 2            # __sinf and __cosf of the reduced phase
+FP32_FLOP_PER_PTHARM = 9             # phase 3 mul + 2 add, accumulate 2 mul + 2 add (plus the sin/cos)
 
 
 def _i3(v):
@@ -356,16 +357,22 @@ def _i3(v):
 
 
 def _direct_roofline(value, sm_max_mhz):
-    """Issue-bound roofline of the FP32 direct sum: warp instructions per
-    point*harmonic (ncu) against 148 SMs x 4 schedulers x the SM clock."""
+    """Roofline of the FP32 direct sum: its two SFU (XU pipe) operations per
+    point*harmonic against 148 SMs x 16 per clock, with the issue rate (warp
+    instructions per point*harmonic from ncu against 148 SMs x 4 schedulers)
+    beside it; both at the SM clock."""
     clk = (sm_max_mhz or 1965.0) * 1e6
-    achieved = value * DIRECT_WARP_INSTR_PER_PTHARM / 1e12
-    peak = 148 * 4 * clk / 1e12
+    achieved = value * DIRECT_MUFU_PER_PTHARM / 1e12
+    peak = 148 * 16 * clk / 1e12
+    issue = value * DIRECT_WARP_INSTR_PER_PTHARM / 1e12
+    issue_peak = 148 * 4 * clk / 1e12
     fp32 = value * FP32_FLOP_PER_PTHARM / 1e12
     fp32_peak = 148 * 128 * 2 * clk / 1e12
-    return {"bound": "issue", "achieved": achieved, "peak": peak, "unit": "T warp-instr/s", "frac": achieved / peak,
-            "instr_per_ptharm": DIRECT_WARP_INSTR_PER_PTHARM, "fp32_tflops": fp32, "fp32_peak_tflops": fp32_peak,
-            "fp32_frac": fp32 / fp32_peak, "kernel": "srm_direct_kernel", "traffic": None}
+    return {"bound": "sfu", "achieved": achieved, "peak": peak, "unit": "T MUFU-op/s", "frac": achieved / peak,
+            "issue": {"achieved": issue, "peak": issue_peak, "unit": "T warp-instr/s", "frac": issue / issue_peak,
+                      "instr_per_ptharm": DIRECT_WARP_INSTR_PER_PTHARM},
+            "fp32_tflops": fp32, "fp32_peak_tflops": fp32_peak, "fp32_frac": fp32 / fp32_peak,
+            "kernel": "srm_direct_kernel", "traffic": None}
 
 
 def _tc_roofline(value, peaks):
