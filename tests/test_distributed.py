@@ -1,8 +1,8 @@
 """Multi-rank host logic on the CPU (gloo, world size 2): every rank draws the
 same harmonics and evaluates its own z-slab; the global statistics are the
 Chan merge of the per-rank (variance, mean, count), gathered in rank order."""
+import datetime
 import os
-import socket
 
 import numpy as np
 import pytest
@@ -17,10 +17,11 @@ NX, NY, NZ = 20, 16, 13
 KW = dict(acf=0, nharm=150, seed=31, hurst=0.3, sigma=0.05, ds=50.0, cl=[2000.0, 2000.0, 1000.0], alpha=10.0)
 
 
-def _free_port():
-    with socket.socket() as s:
-        s.bind(("127.0.0.1", 0))
-        return s.getsockname()[1]
+# The ranks meet through a file store in the test's own directory: no port
+# to pick, so no port another process can take between the pick and the bind.
+def _init(rank, world, store, seconds):
+    dist.init_process_group("gloo", init_method=f"file://{store}", rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=seconds))
 
 
 def _global_corners():
@@ -41,9 +42,8 @@ def _slab_field(rank, world):
     return oracle.sum_structured(s, fs, n, KW["ds"], tab), n
 
 
-def _worker(rank, world, port, out):
-    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
-    dist.init_process_group("gloo", rank=rank, world_size=world)
+def _worker(rank, world, store, out):
+    _init(rank, world, store, 60)
     import oracle
     f, n = _slab_field(rank, world)
     var, mean = oracle.variance(f), oracle.mean(f)
@@ -74,12 +74,12 @@ def test_chan_merge_single_set_is_identity():
     assert v == np.float32(0.25) and m == np.float32(-0.5)
 
 
-def test_two_rank_slabs_reproduce_single_rank_field_and_stats():
+def test_two_rank_slabs_reproduce_single_rank_field_and_stats(tmp_path):
     import oracle
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
-    port = _free_port()
-    procs = [ctx.Process(target=_worker, args=(r, 2, port, q)) for r in range(2)]
+    store = str(tmp_path / "store")
+    procs = [ctx.Process(target=_worker, args=(r, 2, store, q)) for r in range(2)]
     for p in procs:
         p.start()
     gv, gm, whole = q.get(timeout=120)
@@ -92,13 +92,11 @@ def test_two_rank_slabs_reproduce_single_rank_field_and_stats():
     assert abs(gm - oracle.mean(full)) <= 1e-6 * np.sqrt(gv)
 
 
-def _leaving_worker(rank, world, port, out):
+def _leaving_worker(rank, world, store, out):
     # Rank 1 leaves between steps (after the group is up, before the merge);
     # rank 0 must get an error from its next collective, not wait for good.
-    import datetime
     import time
-    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
-    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=5))
+    _init(rank, world, store, 5)
     if rank == 1:
         os._exit(0)
     t0 = time.monotonic()
@@ -110,11 +108,11 @@ def _leaving_worker(rank, world, port, out):
     os._exit(0)
 
 
-def test_a_rank_that_leaves_makes_the_merge_fail_instead_of_hang():
+def test_a_rank_that_leaves_makes_the_merge_fail_instead_of_hang(tmp_path):
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
-    port = _free_port()
-    procs = [ctx.Process(target=_leaving_worker, args=(r, 2, port, q)) for r in range(2)]
+    store = str(tmp_path / "store")
+    procs = [ctx.Process(target=_leaving_worker, args=(r, 2, store, q)) for r in range(2)]
     for p in procs:
         p.start()
     res = q.get(timeout=120)
