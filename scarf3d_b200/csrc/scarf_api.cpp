@@ -97,7 +97,67 @@ struct Object {
   std::vector<float> z2d;                                // 2D meshes: z = 0 (:239-240)
   const float* poi = nullptr;                            // borrowed, [nd x npoi]
   int npoi = 0;
+  const void* pinned[3] = {nullptr, nullptr, nullptr};  // coordinate arrays this library page-locked
 };
+
+// The caller's coordinate arrays stay borrowed for the life of the mesh and
+// every execute reads them anew (as the reference's does), so the library
+// page-locks them there: each execute's upload is then an asynchronous copy
+// that runs while the harmonics are sampled. Arrays that share pages are
+// registered as one range; arrays that are managed or already page-locked
+// memory, or that cannot be registered, are copied as they are.
+void unpin_points(Object& o) {
+  bool any = false;
+  for (auto& p : o.pinned) {
+    if (p) cudaHostUnregister(const_cast<void*>(p));
+    any = any || p;
+    p = nullptr;
+  }
+  if (any) (void)cudaGetLastError();
+}
+
+void pin_points(Object& o) {
+  const float* arr[3] = {o.x, o.y, o.nd == 3 ? o.z : nullptr};
+  const uintptr_t bytes = sizeof(float) * static_cast<uintptr_t>(o.npts);
+  constexpr uintptr_t kPage = 4096;
+  // Byte ranges of the arrays not yet page-locked; ranges whose pages touch
+  // are registered as one (a second registration of a page fails).
+  struct Range { uintptr_t lo, hi; };
+  Range r[3];
+  int n = 0;
+  for (int c = 0; c < 3; ++c) {
+    if (!arr[c]) continue;
+    cudaPointerAttributes at{};
+    if (cudaPointerGetAttributes(&at, arr[c]) != cudaSuccess) {
+      (void)cudaGetLastError();
+      return;  // no usable device: nothing to gain
+    }
+    if (at.type != cudaMemoryTypeUnregistered) continue;  // device, managed or already page-locked
+    const uintptr_t lo = reinterpret_cast<uintptr_t>(arr[c]);
+    r[n++] = {lo, lo + bytes};
+  }
+  std::sort(r, r + n, [](const Range& a, const Range& b) { return a.lo < b.lo; });
+  int m = 0;
+  for (int i = 0; i < n; ++i) {
+    if (m > 0 && r[i].lo / kPage <= (r[m - 1].hi - 1) / kPage) {
+      r[m - 1].hi = std::max(r[m - 1].hi, r[i].hi);
+    } else {
+      r[m++] = r[i];
+    }
+  }
+  for (int i = 0; i < m; ++i) {
+    void* p = reinterpret_cast<void*>(r[i].lo);
+    if (cudaHostRegister(p, r[i].hi - r[i].lo, cudaHostRegisterDefault) == cudaSuccess)
+      o.pinned[i] = p;
+    else
+      (void)cudaGetLastError();
+  }
+}
+
+void reset_object(Object& o) {
+  unpin_points(o);
+  o = Object();
+}
 std::mutex g_mu;  // every entry point that touches a context holds it
 
 // --------------------------------------------------- per-device resources --
@@ -124,6 +184,7 @@ struct Resources {
   int device = -1;
   DeviceBuf status, stats, table, field, coords, work, slab_cnt, statrec, poi;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr, evk0 = nullptr, evk1 = nullptr, evs = nullptr;
+  cudaEvent_t evp = nullptr;  // the coordinates' upload on the copy stream
   cudaStream_t copy_stream = nullptr;  // non-blocking: runs beside the legacy stream too
   int* slab_flags = nullptr;           // host-mapped, written by the kernel
   int* slab_flags_dev = nullptr;
@@ -148,6 +209,8 @@ struct Resources {
     copy_stream = nullptr;
     if (evs) cudaEventDestroy(evs);
     evs = nullptr;
+    if (evp) cudaEventDestroy(evp);
+    evp = nullptr;
     if (evk0) cudaEventDestroy(evk0);
     if (evk1) cudaEventDestroy(evk1);
     evk0 = evk1 = nullptr;
@@ -539,6 +602,25 @@ int fim_execute_impl(int seed, float* field, float stats[8], int flags) {
   return SCARF_OK;
 }
 
+// Device copy of an unstructured mesh's coordinates (three arrays, each
+// 16-byte aligned), issued on the copy stream; res.evp marks its end.
+size_t coord_stride() { return (static_cast<size_t>(t_ctx->obj.npts) + 3) / 4 * 4; }
+
+int upload_points() {
+  const size_t npts = static_cast<size_t>(t_ctx->obj.npts);
+  const size_t stride = coord_stride();
+  SCARF_CUDA(t_ctx->res.coords.ensure(sizeof(float) * 3 * stride));
+  if (!t_ctx->res.copy_stream) SCARF_CUDA(cudaStreamCreateWithFlags(&t_ctx->res.copy_stream, cudaStreamNonBlocking));
+  if (!t_ctx->res.evp) SCARF_CUDA(cudaEventCreateWithFlags(&t_ctx->res.evp, cudaEventDisableTiming));
+  float* c = static_cast<float*>(t_ctx->res.coords.p);
+  cudaStream_t cs = t_ctx->res.copy_stream;
+  SCARF_CUDA(cudaMemcpyAsync(c, t_ctx->obj.x, sizeof(float) * npts, cudaMemcpyDefault, cs));
+  SCARF_CUDA(cudaMemcpyAsync(c + stride, t_ctx->obj.y, sizeof(float) * npts, cudaMemcpyDefault, cs));
+  SCARF_CUDA(cudaMemcpyAsync(c + 2 * stride, t_ctx->obj.z, sizeof(float) * npts, cudaMemcpyDefault, cs));
+  SCARF_CUDA(cudaEventRecord(t_ctx->res.evp, cs));
+  return SCARF_OK;
+}
+
 // The whole SRM execute (scarflib_srm.f90:505-929 / :105-499) for the global
 // object. field: host or device memory of the local block / point set.
 int execute_impl(int seed, float* field, float stats[8], int flags) {
@@ -551,6 +633,11 @@ int execute_impl(int seed, float* field, float stats[8], int flags) {
   for (int i = 0; i < 8; ++i) stats[i] = 0.0f;
   if (t_ctx->obj.method == 0) return fim_execute_impl(seed, field, stats, flags);
   if (t_ctx->obj.method != 1) return fail(SCARF_ERR_UNSUPPORTED, "method must be 0 (FIM) or 1 (SRM)");
+  // An unstructured mesh's coordinates go up while the harmonics are sampled.
+  if (!t_ctx->obj.structured) {
+    rc = upload_points();
+    if (rc) return rc;
+  }
 
   // Host: setup scalars and harmonic table.
   const double th0 = now_s();
@@ -662,14 +749,10 @@ int execute_impl(int seed, float* field, float stats[8], int flags) {
       SCARF_CUDA(cudaMemsetAsync(d_field, 0, sizeof(float) * npts, st));
     }
   } else {
-    SCARF_CUDA(t_ctx->res.coords.ensure(sizeof(float) * 3 * npts + 64));
-    float* c = static_cast<float*>(t_ctx->res.coords.p);
-    const size_t stride = (static_cast<size_t>(npts) + 3) / 4 * 4;  // keep each array 16-B aligned
-    SCARF_CUDA(t_ctx->res.coords.ensure(sizeof(float) * 3 * stride));
-    c = static_cast<float*>(t_ctx->res.coords.p);
-    SCARF_CUDA(cudaMemcpyAsync(c, t_ctx->obj.x, sizeof(float) * npts, cudaMemcpyDefault, st));
-    SCARF_CUDA(cudaMemcpyAsync(c + stride, t_ctx->obj.y, sizeof(float) * npts, cudaMemcpyDefault, st));
-    SCARF_CUDA(cudaMemcpyAsync(c + 2 * stride, t_ctx->obj.z, sizeof(float) * npts, cudaMemcpyDefault, st));
+    // The coordinates were issued on the copy stream before the sampling.
+    const float* c = static_cast<const float*>(t_ctx->res.coords.p);
+    const size_t stride = coord_stride();
+    SCARF_CUDA(cudaStreamWaitEvent(st, t_ctx->res.evp, 0));
     dx = c;
     dy = c + stride;
     dz = c + 2 * stride;
@@ -766,7 +849,7 @@ int execute_impl(int seed, float* field, float stats[8], int flags) {
 }
 
 void finalize_impl() {
-  t_ctx->obj = Object();
+  reset_object(t_ctx->obj);
   t_ctx->res.release();
 }
 
@@ -799,7 +882,7 @@ int cart_initialize_impl(const int nd, const int fs[], const int fe[], const rea
   if ((nd != 2 && nd != 3) || !fs || !fe || !cl)
     return fail(SCARF_ERR_ARG, "scarf_cart_initialize: nd must be 2 or 3 and fs, fe, cl non-NULL");
   Object& o = t_ctx->obj;
-  o = Object();
+  reset_object(o);
   o.structured = true;
   o.nd = nd;
   for (int c = 0; c < nd; ++c) {
@@ -847,7 +930,7 @@ int nocart_initialize_impl(const int nd, const int npts, const real* x, const re
   if ((nd != 2 && nd != 3) || npts <= 0 || !x || !y || !cl || (nd == 3 && !z))
     return fail(SCARF_ERR_ARG, "scarf_nocart_initialize: invalid nd/npts or NULL coordinates");
   Object& o = t_ctx->obj;
-  o = Object();
+  reset_object(o);
   o.structured = false;
   o.nd = nd;
   o.npts = npts;
@@ -900,6 +983,7 @@ int nocart_initialize_impl(const int nd, const int npts, const real* x, const re
     if (var->beta != 0) o.beta = var->beta;
     if (var->gamma != 0) o.gamma = var->gamma;
   }
+  pin_points(o);
   o.ready = true;
   g_last_error.clear();
   return SCARF_OK;
