@@ -17,7 +17,10 @@ namespace {
 
 constexpr int kTile = 256;           // harmonics per shared-memory tile
 constexpr int kRow = 5;              // floats per table row {v1,v2,v3,a,b}
-constexpr int kPts = 8;              // points per thread (two float4 stores)
+// Points per thread: 8 (two float4 stores) with the SFU sin/cos; 4 with
+// CUDA's sincosf, whose slow path needs the registers (8 would spill).
+template <bool kFast>
+constexpr int points_per_thread() { return kFast ? 8 : 4; }
 constexpr int kThreads = 128;
 constexpr uint32_t kTileBytes = kTile * kRow * 4;  // 5120, multiple of 16
 
@@ -91,6 +94,7 @@ __device__ __forceinline__ void phase_sincos(float arg, float* sn, float* cs) {
 
 template <bool kStructured, bool kFast>
 __global__ void __launch_bounds__(kThreads) srm_direct_kernel(const DirectArgs A) {
+  constexpr int kPts = points_per_thread<kFast>();
   __shared__ __align__(128) float s_tab[2][kTile * kRow];
   __shared__ __align__(8) uint64_t s_full[2];
 
@@ -241,8 +245,10 @@ int g_direct_fast = 1;
 void direct_set_sincos(int fast) { g_direct_fast = fast ? 1 : 0; }
 int direct_get_sincos() { return g_direct_fast; }
 
+int direct_points_per_thread() { return g_direct_fast ? points_per_thread<true>() : points_per_thread<false>(); }
+
 long long direct_stat_records(long long npts) {
-  const long long per_block = static_cast<long long>(kThreads) * kPts;
+  const long long per_block = static_cast<long long>(kThreads) * direct_points_per_thread();
   return (npts + per_block - 1) / per_block;
 }
 
@@ -265,7 +271,7 @@ cudaError_t launch_direct_structured(const scarf_srm_setup& s, const int fs[3], 
   A.off1 = fs[1] - 2;
   A.off2 = fs[2] - 2;
   A.stats = d_stats;
-  const long long per_block = static_cast<long long>(kThreads) * kPts;
+  const long long per_block = static_cast<long long>(kThreads) * direct_points_per_thread();
   const long long blocks = (A.npts + per_block - 1) / per_block;
   if (blocks <= 0) return cudaSuccess;
   if (g_direct_fast)
@@ -291,7 +297,7 @@ cudaError_t launch_direct_points(const scarf_srm_setup& s, const float* d_x, con
   A.y = d_y;
   A.z = d_z;
   A.stats = d_stats;
-  const long long per_block = static_cast<long long>(kThreads) * kPts;
+  const long long per_block = static_cast<long long>(kThreads) * direct_points_per_thread();
   const long long blocks = (npts + per_block - 1) / per_block;
   if (blocks <= 0) return cudaSuccess;
   if (g_direct_fast)
