@@ -147,7 +147,7 @@ void pin_points(Object& o) {
   }
   for (int i = 0; i < m; ++i) {
     void* p = reinterpret_cast<void*>(r[i].lo);
-    if (cudaHostRegister(p, r[i].hi - r[i].lo, cudaHostRegisterDefault) == cudaSuccess)
+    if (cudaHostRegister(p, r[i].hi - r[i].lo, cudaHostRegisterPortable) == cudaSuccess)
       o.pinned[i] = p;
     else
       (void)cudaGetLastError();
