@@ -522,6 +522,25 @@ scarf_srm_params params_from_object(int seed) {
   return p;
 }
 
+// Device copy of an unstructured mesh's coordinates (three arrays, each
+// 16-byte aligned), issued on the copy stream; res.evp marks its end.
+size_t coord_stride() { return (static_cast<size_t>(t_ctx->obj.npts) + 3) / 4 * 4; }
+
+int upload_points() {
+  const size_t npts = static_cast<size_t>(t_ctx->obj.npts);
+  const size_t stride = coord_stride();
+  SCARF_CUDA(t_ctx->res.coords.ensure(sizeof(float) * 3 * stride));
+  if (!t_ctx->res.copy_stream) SCARF_CUDA(cudaStreamCreateWithFlags(&t_ctx->res.copy_stream, cudaStreamNonBlocking));
+  if (!t_ctx->res.evp) SCARF_CUDA(cudaEventCreateWithFlags(&t_ctx->res.evp, cudaEventDisableTiming));
+  float* c = static_cast<float*>(t_ctx->res.coords.p);
+  cudaStream_t cs = t_ctx->res.copy_stream;
+  SCARF_CUDA(cudaMemcpyAsync(c, t_ctx->obj.x, sizeof(float) * npts, cudaMemcpyDefault, cs));
+  SCARF_CUDA(cudaMemcpyAsync(c + stride, t_ctx->obj.y, sizeof(float) * npts, cudaMemcpyDefault, cs));
+  SCARF_CUDA(cudaMemcpyAsync(c + 2 * stride, t_ctx->obj.z, sizeof(float) * npts, cudaMemcpyDefault, cs));
+  SCARF_CUDA(cudaEventRecord(t_ctx->res.evp, cs));
+  return SCARF_OK;
+}
+
 // FIM (method 0) for the global object: scarf3d_structured_fim /
 // scarf3d_unstructured_fim (scarflib_fim.f90:141-1104) on one device
 // (fim.cu). The internal grid covers nc..fc; statistics, rescale and taper
@@ -580,12 +599,11 @@ int fim_execute_impl(int seed, float* field, float stats[8], int flags) {
     d_field = static_cast<float*>(t_ctx->res.field.p);
   }
   if (!t_ctx->obj.structured) {
-    const size_t stride = (static_cast<size_t>(npts) + 3) / 4 * 4;
-    SCARF_CUDA(t_ctx->res.coords.ensure(sizeof(float) * 3 * stride));
-    float* c = static_cast<float*>(t_ctx->res.coords.p);
-    SCARF_CUDA(cudaMemcpyAsync(c, t_ctx->obj.x, sizeof(float) * npts, cudaMemcpyDefault, st));
-    SCARF_CUDA(cudaMemcpyAsync(c + stride, t_ctx->obj.y, sizeof(float) * npts, cudaMemcpyDefault, st));
-    SCARF_CUDA(cudaMemcpyAsync(c + 2 * stride, t_ctx->obj.z, sizeof(float) * npts, cudaMemcpyDefault, st));
+    const size_t stride = coord_stride();
+    const int rc = upload_points();
+    if (rc) return rc;
+    SCARF_CUDA(cudaStreamWaitEvent(st, t_ctx->res.evp, 0));
+    const float* c = static_cast<const float*>(t_ctx->res.coords.p);
     in.d_x = c;
     in.d_y = c + stride;
     in.d_z = c + 2 * stride;
@@ -599,25 +617,6 @@ int fim_execute_impl(int seed, float* field, float stats[8], int flags) {
     if (rc) return rc;
     SCARF_CUDA(cudaStreamSynchronize(st));
   }
-  return SCARF_OK;
-}
-
-// Device copy of an unstructured mesh's coordinates (three arrays, each
-// 16-byte aligned), issued on the copy stream; res.evp marks its end.
-size_t coord_stride() { return (static_cast<size_t>(t_ctx->obj.npts) + 3) / 4 * 4; }
-
-int upload_points() {
-  const size_t npts = static_cast<size_t>(t_ctx->obj.npts);
-  const size_t stride = coord_stride();
-  SCARF_CUDA(t_ctx->res.coords.ensure(sizeof(float) * 3 * stride));
-  if (!t_ctx->res.copy_stream) SCARF_CUDA(cudaStreamCreateWithFlags(&t_ctx->res.copy_stream, cudaStreamNonBlocking));
-  if (!t_ctx->res.evp) SCARF_CUDA(cudaEventCreateWithFlags(&t_ctx->res.evp, cudaEventDisableTiming));
-  float* c = static_cast<float*>(t_ctx->res.coords.p);
-  cudaStream_t cs = t_ctx->res.copy_stream;
-  SCARF_CUDA(cudaMemcpyAsync(c, t_ctx->obj.x, sizeof(float) * npts, cudaMemcpyDefault, cs));
-  SCARF_CUDA(cudaMemcpyAsync(c + stride, t_ctx->obj.y, sizeof(float) * npts, cudaMemcpyDefault, cs));
-  SCARF_CUDA(cudaMemcpyAsync(c + 2 * stride, t_ctx->obj.z, sizeof(float) * npts, cudaMemcpyDefault, cs));
-  SCARF_CUDA(cudaEventRecord(t_ctx->res.evp, cs));
   return SCARF_OK;
 }
 
