@@ -80,10 +80,12 @@ __device__ __forceinline__ void sample_range(const SamplerArgs& A, long long t, 
   int count = 0;
   long long slot = write == 1 ? A.offsets[t] : (write == 2 ? t * A.cap : 0);
   const long long slot_end = write == 2 ? slot + A.cap : (1ll << 62);
-  for (long long q = q0; q < q1; ++q) {
+  const int npairs = q1 > q0 ? static_cast<int>(q1 - q0) : 0;  // at most pairs_per_thread
+  for (int i = 0; i < npairs; ++i) {
     const uint32_t y1 = g.next();
     const uint32_t y2 = g.next();
     if (thr && y2 >= thr[y1 >> kRejectShift]) continue;
+    const long long q = q0 + i;
     const float r1 = to_u01(y1);
     const float r2 = to_u01(y2);
     const int c = classify(A, r1, r2);

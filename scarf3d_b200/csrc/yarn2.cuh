@@ -70,8 +70,9 @@ struct Gen {
     const uint32_t u = sub_m(static_cast<uint32_t>(f & kMod) + static_cast<uint32_t>(f >> 31));
     r1 = r0;
     r0 = u;
-    if (u == 0) return 0u;
-    return mulmod3(sp[u & 2047u], sp[kPow0 + ((u >> 11) & 2047u)], sp[kPow0 + kPow1 + (u >> 22)]);
+    // The state 0 outputs 0; the power is formed regardless (no branch).
+    const uint32_t y = mulmod3(sp[u & 2047u], sp[kPow0 + ((u >> 11) & 2047u)], sp[kPow0 + kPow1 + (u >> 22)]);
+    return u == 0 ? 0u : y;
   }
   __device__ __forceinline__ void jump(uint64_t n) {
     uint64_t m00 = kA1, m01 = kA2, m10 = 1, m11 = 0;
