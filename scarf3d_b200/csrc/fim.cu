@@ -344,6 +344,42 @@ std::mutex g_fim_mu;
 int g_fim_tables_dev = -1;
 unsigned long long g_fim_tables_ctx = 0;
 
+// The two cuFFT plans of the last internal grid transformed on each device,
+// kept across calls: building a plan (kernel selection and the allocation of
+// its work area) takes far longer than the transforms. Plans belong to the
+// device context they were made in; after a reset (a new context id) the old
+// handles are dropped, not destroyed. Guarded by g_fim_mu.
+struct FimPlans {
+  unsigned long long ctx = 0;
+  int n1 = 0, n2 = 0, n3 = 0, three = -1;
+  cufftHandle yz = 0, x = 0;
+};
+constexpr int kPlanDevices = 64;
+FimPlans g_fim_plans[kPlanDevices];
+
+void destroy_plans(FimPlans& p) {
+  if (p.yz) g_cufft.destroy(p.yz);
+  if (p.x) g_cufft.destroy(p.x);
+  p = FimPlans();
+}
+
+}  // namespace
+
+// Frees the cached cuFFT plans (and their work areas) of the current device.
+void release_fim_plans() {
+  std::lock_guard<std::mutex> lk(g_fim_mu);
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev >= kPlanDevices) {
+    (void)cudaGetLastError();
+    return;
+  }
+  FimPlans& P = g_fim_plans[dev];
+  if (P.yz && P.ctx == current_context_id() && g_cufft.ok) destroy_plans(P);
+  P = FimPlans();
+}
+
+namespace {
+
 // The generator tables in this module's device and constant memory, uploaded
 // once per device context (a reset context has a new id; when the id cannot
 // be read they are uploaded on every call).
@@ -506,26 +542,48 @@ cudaError_t fim_run(const FimInputs& in, const FimGrid& g, void* d_work, float* 
   cudaEventRecord(ev[2], st);
   // 3. inverse transform: c2c along z and y (x bins as the batch), the
   // unused imaginary parts of x bins 0 and n1/2 cleared, c2r along x.
-  cufftHandle p_yz = 0, p_x = 0;
-  struct PlanGuard {
-    cufftHandle* a;
-    cufftHandle* b;
-    ~PlanGuard() {
-      if (*a) g_cufft.destroy(*a);
-      if (*b) g_cufft.destroy(*b);
-    }
-  } pg{&p_yz, &p_x};
   const int n1h = static_cast<int>(L.n1h);
-  {
+  const bool three = in.ndim == 3 && n3 > 1;
+  // The plans: this device's cached pair when the grid matches, else new
+  // ones (cached for the next call; on devices beyond the cache, freed on
+  // return).
+  int dev = 0;
+  if ((e = cudaGetDevice(&dev)) != cudaSuccess) return failed("cudaGetDevice", e);
+  const unsigned long long ctx = current_context_id();
+  const bool cacheable = dev < kPlanDevices && ctx != 0;
+  FimPlans local;
+  FimPlans& P = cacheable ? g_fim_plans[dev] : local;
+  struct LocalGuard {
+    FimPlans* p;
+    ~LocalGuard() { destroy_plans(*p); }
+  } lg{&local};
+  if (cacheable && P.ctx != ctx) P = FimPlans();  // handles of a reset context are dropped
+  if (P.yz && !(P.n1 == n1 && P.n2 == n2 && P.n3 == n3 && P.three == (three ? 1 : 0))) destroy_plans(P);
+  if (!P.yz) {
+    FimPlans fresh;
+    struct FreshGuard {
+      FimPlans* p;
+      bool keep = false;
+      ~FreshGuard() {
+        if (!keep) destroy_plans(*p);
+      }
+    } fg{&fresh};
     int dims3[2] = {n3, n2}, dims2[1] = {n2};
-    const bool three = in.ndim == 3 && n3 > 1;
     int* dims = three ? dims3 : dims2;
     const int rank = three ? 2 : 1;
-    if (g_cufft.plan_many(&p_yz, rank, dims, dims, n1h, 1, dims, n1h, 1, CUFFT_C2C, n1h) != CUFFT_SUCCESS)
+    if (g_cufft.plan_many(&fresh.yz, rank, dims, dims, n1h, 1, dims, n1h, 1, CUFFT_C2C, n1h) != CUFFT_SUCCESS)
       return failed("cufftPlanMany (z, y)", cudaErrorUnknown);
     int dx[1] = {n1}, ex[1] = {n1h}, ox[1] = {n1};
-    if (g_cufft.plan_many(&p_x, 1, dx, ex, 1, n1h, ox, 1, n1, CUFFT_C2R, static_cast<int>(L.rows)) != CUFFT_SUCCESS)
+    if (g_cufft.plan_many(&fresh.x, 1, dx, ex, 1, n1h, ox, 1, n1, CUFFT_C2R, static_cast<int>(L.rows)) !=
+        CUFFT_SUCCESS)
       return failed("cufftPlanMany (x)", cudaErrorUnknown);
+    fresh.ctx = ctx;
+    fresh.n1 = n1, fresh.n2 = n2, fresh.n3 = n3, fresh.three = three ? 1 : 0;
+    P = fresh;
+    fg.keep = true;
+  }
+  const cufftHandle p_yz = P.yz, p_x = P.x;
+  {
     if (g_cufft.set_stream(p_yz, st) != CUFFT_SUCCESS || g_cufft.set_stream(p_x, st) != CUFFT_SUCCESS)
       return failed("cufftSetStream", cudaErrorUnknown);
     cufftComplex* c = reinterpret_cast<cufftComplex*>(spec);

@@ -1556,6 +1556,7 @@ int scarf_release_device_memory(void) {
     SCARF_CUDA(cudaSetDevice(dev));
   }
   scarf::release_sampler_device_memory();
+  scarf::release_fim_plans();
   return SCARF_OK;
 }
 

@@ -268,5 +268,7 @@ size_t fim_workspace_bytes(const FimGrid& g, int npoi);
 // failure *what names the failing step. Synchronises `st`.
 cudaError_t fim_run(const FimInputs& in, const FimGrid& g, void* d_work, float* d_field, float stats[8],
                     cudaStream_t st, const char** what);
+// Frees the FIM's cached cuFFT plans of the current device.
+void release_fim_plans();
 
 }  // namespace scarf

@@ -99,3 +99,19 @@ def test_fim_is_deterministic_and_seeded():
     d, _, _, _ = _execute_structured(dict(c, seed=c["seed"] + 1))
     assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
     assert rel_rms(a, d) > 0.5
+
+
+def test_cached_transform_plans_follow_the_grid():
+    """The cuFFT plans kept from one call to the next are rebuilt when the
+    internal grid changes and after scarf_release_device_memory: grids run in
+    turn (A, B, A, release, A) give A's field bit for bit every time."""
+    a, b = STRUCTURED[0], STRUCTURED[1]
+    ref, st_ref, _, _ = _execute_structured(a)
+    other, _, _, _ = _execute_structured(b)
+    assert other.size != ref.size
+    again, st_again, _, _ = _execute_structured(a)
+    assert np.array_equal(again.view(np.uint32), ref.view(np.uint32))
+    assert np.array_equal(st_again[:4], st_ref[:4])
+    sb.check(sb.lib.scarf_release_device_memory())
+    after, _, _, _ = _execute_structured(a)
+    assert np.array_equal(after.view(np.uint32), ref.view(np.uint32))
