@@ -342,7 +342,8 @@ int scarf_srm_tc_batch_autotune(const scarf_tc_field *fields, int nfields, void 
  * library holds until exit; a grid and harmonic count whose
  * scarf_srm_tc_workspace_bytes() exceeds it returns SCARF_ERR_ARG. The plan
  * is the one scarf_srm_tc_structured runs (tuned plans included). The first
- * call in each device context looks up the array's device address. Every
+ * call in each device context looks up the array's device address; make that
+ * first call on a device before any stream capture begins there. Every
  * call reads its status word back and synchronises `stream`. All calls on a
  * device share the array: calls that overlap on the GPU race and must be
  * serialised. */
