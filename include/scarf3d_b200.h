@@ -93,7 +93,9 @@ int scarf_set_device_memory_cap(size_t bytes);
 /* Device bytes the library holds now. */
 size_t scarf_device_memory_in_use(void);
 /* Frees the device buffers the library keeps between calls (they are
- * allocated again on demand); waits for the library's device work first. */
+ * allocated again on demand), and the FIM's cuFFT plans of the current
+ * device (kept between calls; their work areas are cuFFT's own allocations,
+ * outside the cap); waits for the library's device work first. */
 int scarf_release_device_memory(void);
 /* Self-test of the bounded waits inside every pipeline kernel: `blocks`
  * blocks (1..1024) wait on an mbarrier that nothing arrives on, through the
