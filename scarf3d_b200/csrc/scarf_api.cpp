@@ -366,6 +366,19 @@ class BounceCopier {
     }
     return SCARF_OK;
   }
+  // Moves every slot whose copy has already landed (oldest first) into the
+  // caller's array, so that little is left for finish() once the last
+  // region is issued.
+  int poll() {
+    for (int k = 0; k < kBounceSlots; ++k) {
+      const int slot = (next_ + k) % kBounceSlots;
+      if (!pend_[slot].busy) continue;
+      if (cudaEventQuery(t_ctx->res.bounce_ev[slot]) != cudaSuccess) break;  // later copies queue behind it
+      const int rc = complete(slot);
+      if (rc) return rc;
+    }
+    return SCARF_OK;
+  }
   int finish() {
     int rc = SCARF_OK;
     for (int k = 0; k < kBounceSlots; ++k) {
@@ -430,6 +443,11 @@ int copy_slabs_out(const TcPlan& plan, const TcSlabSignal& sig, const float* d_f
       if ((spins & 1023u) == 1023u && cudaStreamQuery(st) != cudaErrorNotReady) {
         cudaGetLastError();
         idle = true;
+      }
+      if (bounce && (spins & 255u) == 255u) {
+        // While the next slab computes, empty the slots that have landed.
+        const int rc = bc.poll();
+        if (rc) return rc;
       }
       cpu_relax();
     }
