@@ -573,6 +573,11 @@ struct DeviceSamplerState {
   DevBuf counts, offsets, entries, slots, batch_args, batch_tbeg, reject;
   SampleEntry* host_entries = nullptr;  // page-locked staging of candidate entries
   long long host_entries_cap = 0;
+  // Two sets of the same for a batch's groups: one group's gather fills one
+  // while the host walks the previous group's entries in the other.
+  DevBuf gentries[2];
+  SampleEntry* ghost[2] = {nullptr, nullptr};
+  long long ghost_cap[2] = {0, 0};
   cudaStream_t side = nullptr;        // gathers and copies beside the scans
   std::vector<cudaEvent_t> events;    // end of each group's scan
 };
@@ -668,7 +673,9 @@ long long first_pass_pairs(const scarf_srm_params& p, double acc) {
 void release_sampler_device_memory() {
   std::lock_guard<std::mutex> lk(g_dev_sampler_mu);
   DeviceSamplerState& D = g_dev_sampler;
-  for (DevBuf* b : {&D.counts, &D.offsets, &D.entries, &D.slots, &D.batch_args, &D.batch_tbeg, &D.reject}) b->release();
+  for (DevBuf* b : {&D.counts, &D.offsets, &D.entries, &D.slots, &D.batch_args, &D.batch_tbeg, &D.reject,
+                    &D.gentries[0], &D.gentries[1]})
+    b->release();
 }
 
 namespace {
@@ -679,8 +686,12 @@ bool ensure_sampler_device(DeviceSamplerState& D) {
   if (cudaGetDevice(&dev) != cudaSuccess) return false;
   if (D.device != dev) {
     // the previous device's buffers (freed through unified addressing)
-    for (DevBuf* b : {&D.counts, &D.offsets, &D.entries, &D.slots, &D.batch_args, &D.batch_tbeg, &D.reject}) b->release();
+    for (DevBuf* b : {&D.counts, &D.offsets, &D.entries, &D.slots, &D.batch_args, &D.batch_tbeg, &D.reject,
+                      &D.gentries[0], &D.gentries[1]})
+      b->release();
     if (D.host_entries) cudaFreeHost(D.host_entries);
+    for (SampleEntry* h : D.ghost)
+      if (h) cudaFreeHost(h);
     D = DeviceSamplerState();
     D.device = dev;
   }
@@ -965,6 +976,34 @@ int srm_sample_device_batch(int nfields, const scarf_srm_params* p, const scarf_
       }
     });
   };
+  // Walks of a group whose entries sit in staging set `b` (complete once the
+  // side stream has passed the group's copy), then the table rows of the
+  // fields it finished.
+  auto walk_group = [&](int g, int b, const std::vector<long long>& ebeg) {
+    const int f0 = gbeg[g], f1 = gbeg[g + 1];
+    for (int f = f0; f < f1; ++f) {
+      DeviceWalk& w = walks[f];
+      w.ent = overflow[f] ? nullptr : D.ghost[b] + ebeg[f - f0];
+      w.nent = overflow[f] ? 0 : static_cast<size_t>(ebeg[f - f0 + 1] - ebeg[f - f0]);
+      if (overflow[f]) w.pass_end = 0;
+    }
+    parallel_tasks(f1 - f0, host_threads(), [&](int i) { done[f0 + i] = walks[f0 + i].walk() ? 1 : 0; });
+    std::vector<int> finished;
+    for (int f = f0; f < f1; ++f) {
+      // the staging set belongs to a later group now
+      walks[f].ent = nullptr;
+      walks[f].nent = 0;
+      walks[f].ei = 0;
+      if (done[f]) finished.push_back(f);
+    }
+    fill_rows(finished);
+  };
+  // Group g: its counts (which also waits for the previous group's gather
+  // and copy on the side stream), then its gather into the staging set the
+  // previous non-empty group did not use; the previous group is walked
+  // while that gather runs.
+  int prev = -1, prev_b = 1;
+  std::vector<long long> prev_ebeg;
   for (int g = 0; g < G; ++g) {
     const int f0 = gbeg[g], f1 = gbeg[g + 1];
     if (f1 == f0) continue;
@@ -984,47 +1023,36 @@ int srm_sample_device_batch(int nfields, const scarf_srm_params* p, const scarf_
       }
       ebeg[f - f0 + 1] = total;
     }
+    const int b = prev_b ^ 1;
     if (total > 0) {
-      // The previous group's gather and copy have finished (side stream
-      // synchronised) and its walks are done, so both buffers may be reused.
-      if (D.entries.ensure(sizeof(SampleEntry) * total) != cudaSuccess) return err;
-      if (D.host_entries_cap < total) {
-        if (D.host_entries) cudaFreeHost(D.host_entries);
-        D.host_entries = nullptr;
-        D.host_entries_cap = 0;
+      // Set b was last read by the walks of the group before the previous
+      // one, which are done.
+      if (D.gentries[b].ensure(sizeof(SampleEntry) * total) != cudaSuccess) return err;
+      if (D.ghost_cap[b] < total) {
+        if (D.ghost[b]) cudaFreeHost(D.ghost[b]);
+        D.ghost[b] = nullptr;
+        D.ghost_cap[b] = 0;
         void* h = nullptr;
         if (cudaHostAlloc(&h, sizeof(SampleEntry) * total, cudaHostAllocDefault) != cudaSuccess) return err;
-        D.host_entries = static_cast<SampleEntry*>(h);
-        D.host_entries_cap = total;
+        D.ghost[b] = static_cast<SampleEntry*>(h);
+        D.ghost_cap[b] = total;
       }
       if (cudaMemcpyAsync(d_offsets + t0, offsets.data() + t0, sizeof(long long) * Tg, cudaMemcpyHostToDevice,
                           D.side) != cudaSuccess ||
           launch_sampler_gather(d_args + f0, d_tbeg + f0 + g, f1 - f0, Tg, d_offsets + t0,
-                                static_cast<SampleEntry*>(D.entries.p), D.side) != cudaSuccess ||
-          cudaMemcpyAsync(D.host_entries, D.entries.p, sizeof(SampleEntry) * total, cudaMemcpyDeviceToHost,
-                          D.side) != cudaSuccess ||
-          cudaStreamSynchronize(D.side) != cudaSuccess)
+                                static_cast<SampleEntry*>(D.gentries[b].p), D.side) != cudaSuccess ||
+          cudaMemcpyAsync(D.ghost[b], D.gentries[b].p, sizeof(SampleEntry) * total, cudaMemcpyDeviceToHost,
+                          D.side) != cudaSuccess)
         return err;
     }
-    // Walks over the group's first passes, fields spread over host threads
-    // (each walk is independent). An overflowed field starts over later with
-    // its own passes (empty first pass).
-    for (int f = f0; f < f1; ++f) {
-      DeviceWalk& w = walks[f];
-      w.ent = overflow[f] ? nullptr : D.host_entries + ebeg[f - f0];
-      w.nent = overflow[f] ? 0 : static_cast<size_t>(ebeg[f - f0 + 1] - ebeg[f - f0]);
-      if (overflow[f]) w.pass_end = 0;
-    }
-    parallel_tasks(f1 - f0, host_threads(), [&](int i) { done[f0 + i] = walks[f0 + i].walk() ? 1 : 0; });
-    std::vector<int> finished;
-    for (int f = f0; f < f1; ++f) {
-      // the staging buffer belongs to the next group now
-      walks[f].ent = nullptr;
-      walks[f].nent = 0;
-      walks[f].ei = 0;
-      if (done[f]) finished.push_back(f);
-    }
-    fill_rows(finished);
+    if (prev >= 0) walk_group(prev, prev_b, prev_ebeg);
+    prev = g;
+    prev_b = b;
+    prev_ebeg.swap(ebeg);
+  }
+  if (prev >= 0) {
+    if (cudaStreamSynchronize(D.side) != cudaSuccess) return err;
+    walk_group(prev, prev_b, prev_ebeg);
   }
   // Fields whose first pass ran short (or overflowed) continue with their own
   // device passes, one field at a time, once every group's scan is done.
